@@ -1,0 +1,95 @@
+"""ctypes binding of oracle/_ref/libcolaref.so -- TEST INFRASTRUCTURE.
+
+The library is the reference's own C code (unchanged) linked against the
+project's shims; see oracle/Makefile.  The functions bound here are the
+reference's public hot-path entry points (pm.h:6-11, cola.h:7-18,
+lpt.h:6-8, power.h:4-6, move.h:7, comm.h:8, msg.h:4-9, timer.h:4-10).
+"""
+import ctypes
+import os
+import subprocess
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_ref", "libcolaref.so")
+
+_lib = None
+
+
+def build(ref_dir="/root/reference"):
+    """Compile the reference (needs its sources; they are not on GPU hosts)."""
+    if not os.path.isdir(ref_dir):
+        return os.path.exists(LIB_PATH)
+    subprocess.run(["make", "-s", "-C", HERE, "REF=" + ref_dir], check=True)
+    return True
+
+
+def load():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        build()
+    lib = ctypes.CDLL(LIB_PATH)
+    P = ctypes.c_void_p
+    f, d, i = ctypes.c_float, ctypes.c_double, ctypes.c_int
+    sz = ctypes.c_size_t
+    sig = {
+        "msg_init": (None, []),
+        "msg_set_loglevel": (None, [i]),
+        "timer_set_category": (None, [i]),
+        "timer_print": (None, []),
+        "comm_init": (None, [i, i, f]),
+        "power_init": (None, [ctypes.c_char_p, d, d, d, d]),
+        "PowerSpec": (d, [d]),
+        "GrowthFactor": (d, [d, d]),
+        "lpt_init": (None, [i, P, sz]),
+        "lpt_set_displacement": (i, [d, d, i, d, P]),
+        "lpt_get_local_nx": (i, []),
+        "pm_init": (None, [i, i, f, f, P, sz, P, sz]),
+        "pm_calculate_forces": (None, [P]),
+        "cola_kick": (None, [P, f, f]),
+        "cola_drift": (None, [P, f, f]),
+        "cola_set_snapshot": (None, [d, P, P]),
+        "move_particles2": (None, [P, f, P, sz]),
+        "growthD": (f, [f]),
+        "growthD2": (f, [f]),
+        "Sq": (d, [d, d, d]),
+        "Sphi": (d, [d, d, d]),
+        "Qfactor": (f, [f]),
+        "gsl_rng_alloc": (P, [P]),
+        "gsl_rng_set": (None, [P, ctypes.c_ulong]),
+        "gsl_rng_uniform": (d, [P]),
+        "gsl_rng_free": (None, [P]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    lib.msg_init()
+    lib.msg_set_loglevel(7)          # silent
+    lib.timer_set_category(0)
+    _lib = lib
+    return lib
+
+
+def ranlxd1_stream(seed, n):
+    """First n draws of the shim's gsl_rng_ranlxd1 after gsl_rng_set(seed)."""
+    lib = load()
+    rtype = ctypes.c_void_p.in_dll(lib, "gsl_rng_ranlxd1")
+    r = lib.gsl_rng_alloc(rtype)
+    lib.gsl_rng_set(r, seed)
+    out = [lib.gsl_rng_uniform(r) for _ in range(n)]
+    lib.gsl_rng_free(r)
+    return out
+
+
+def set_cola_omega(omega_m):
+    """cola.c keeps Omega_m in a file-static (cola.c:58) that cola_kick sets;
+    the growth functions read it.  Kick zero particles to set it."""
+    from cola_halo_b200.types import Particles
+    lib = load()
+    p = Particles()
+    p.np_local = 0
+    p.a_x = 0.5
+    p.a_v = 0.5
+    lib.cola_kick(ctypes.byref(p), omega_m, 0.5)

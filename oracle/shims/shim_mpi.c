@@ -1,0 +1,97 @@
+/* Single-rank MPI shim implementation -- TEST INFRASTRUCTURE (see mpi.h). */
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include "mpi.h"
+
+static oracle_abort_hook g_abort_hook = 0;
+
+void oracle_set_abort_hook(oracle_abort_hook hook) { g_abort_hook = hook; }
+
+static size_t type_size(MPI_Datatype t)
+{
+  switch (t) {
+  case MPI_BYTE: return 1;
+  case MPI_INT: return sizeof(int);
+  case MPI_FLOAT: return sizeof(float);
+  case MPI_DOUBLE: return sizeof(double);
+  case MPI_LONG_LONG: return sizeof(long long);
+  case MPI_LONG: return sizeof(long);
+  case MPI_UNSIGNED: return sizeof(unsigned);
+  default:
+    fprintf(stderr, "mpi shim: unknown datatype %d\n", t);
+    abort();
+  }
+}
+
+int MPI_Init(int* argc, char*** argv) { (void)argc; (void)argv; return MPI_SUCCESS; }
+int MPI_Init_thread(int* argc, char*** argv, int required, int* provided)
+{
+  (void)argc; (void)argv; *provided = required; return MPI_SUCCESS;
+}
+int MPI_Finalize(void) { return MPI_SUCCESS; }
+int MPI_Comm_rank(MPI_Comm comm, int* rank) { (void)comm; *rank = 0; return MPI_SUCCESS; }
+int MPI_Comm_size(MPI_Comm comm, int* size) { (void)comm; *size = 1; return MPI_SUCCESS; }
+int MPI_Barrier(MPI_Comm comm) { (void)comm; return MPI_SUCCESS; }
+
+int MPI_Abort(MPI_Comm comm, int errorcode)
+{
+  (void)comm;
+  fflush(stdout);
+  if (g_abort_hook) {
+    g_abort_hook(errorcode);   /* the hook is expected not to return */
+  }
+  fprintf(stderr, "MPI_Abort(%d)\n", errorcode);
+  exit(errorcode ? errorcode : 1);
+}
+
+int MPI_Sendrecv(const void* sendbuf, int sendcount, MPI_Datatype sendtype,
+                 int dest, int sendtag,
+                 void* recvbuf, int recvcount, MPI_Datatype recvtype,
+                 int source, int recvtag, MPI_Comm comm, MPI_Status* status)
+{
+  (void)dest; (void)sendtag; (void)source; (void)recvtag; (void)comm;
+  /* Single rank: the message sent "to the right" is the one received "from
+   * the left".  The receive count is an upper bound, as in MPI. */
+  size_t nsend = (size_t)sendcount * type_size(sendtype);
+  size_t nrecv = (size_t)recvcount * type_size(recvtype);
+  if (nsend > nrecv) {
+    fprintf(stderr, "mpi shim: Sendrecv truncation %zu > %zu\n", nsend, nrecv);
+    abort();
+  }
+  if (nsend && sendbuf != recvbuf) memmove(recvbuf, sendbuf, nsend);
+  if (status) { status->MPI_SOURCE = 0; status->MPI_TAG = recvtag; status->MPI_ERROR = 0; }
+  return MPI_SUCCESS;
+}
+
+int MPI_Reduce(const void* sendbuf, void* recvbuf, int count,
+               MPI_Datatype datatype, MPI_Op op, int root, MPI_Comm comm)
+{
+  (void)op; (void)root; (void)comm;
+  size_t n = (size_t)count * type_size(datatype);
+  if (n && sendbuf != recvbuf) memmove(recvbuf, sendbuf, n);
+  return MPI_SUCCESS;
+}
+
+int MPI_Allreduce(const void* sendbuf, void* recvbuf, int count,
+                  MPI_Datatype datatype, MPI_Op op, MPI_Comm comm)
+{
+  return MPI_Reduce(sendbuf, recvbuf, count, datatype, op, 0, comm);
+}
+
+int MPI_Bcast(void* buffer, int count, MPI_Datatype datatype, int root,
+              MPI_Comm comm)
+{
+  (void)buffer; (void)count; (void)datatype; (void)root; (void)comm;
+  return MPI_SUCCESS;
+}
+
+int MPI_Allgather(const void* sendbuf, int sendcount, MPI_Datatype sendtype,
+                  void* recvbuf, int recvcount, MPI_Datatype recvtype,
+                  MPI_Comm comm)
+{
+  (void)recvcount; (void)recvtype; (void)comm;
+  size_t n = (size_t)sendcount * type_size(sendtype);
+  if (n && sendbuf != recvbuf) memmove(recvbuf, sendbuf, n);
+  return MPI_SUCCESS;
+}
