@@ -1,0 +1,494 @@
+#!/usr/bin/env python
+"""Throughput benchmark of the COLA step: particle-steps/s.
+
+Workload (default): 256^3 particles, 768^3 PM mesh (factor 3), box
+600 Mpc/h, BBKS no-wiggle P(k) (Omega_m 0.273, h 0.705, n_s 0.96,
+sigma_8 0.81), 2LPT at z = 49, 10 COLA steps linear in a to z = 0.  Inputs
+are seeded synthetic initial conditions (no dataset is involved).
+
+A "step" is one COLA time step: periodic wrap, PM force (deposit, r2c,
+Green/gradient, three c2r, interpolation), kick, drift.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Prints one JSON line (rank 0).  Under torchrun each rank runs its own
+realization (seed + rank) on its own GPU: realizations are independent, so
+the N-GPU number is weak-scaled replicas with no collective on the data path.
+"""
+import argparse
+import ctypes
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+CONFIGS = {
+    # 1 x B200 plain COLA run
+    "c2": dict(nc=256, factor=3, L=600.0, om=0.273, a_init=0.02, nsteps=10, seed=100),
+    # the CPU-runnable case
+    "c1": dict(nc=64, factor=3, L=200.0, om=0.273, a_init=0.02, nsteps=10, seed=100),
+    # one realization of the batched config (128^3, 384^3 mesh)
+    "c3": dict(nc=128, factor=3, L=300.0, om=0.273, a_init=0.02, nsteps=10, seed=100),
+}
+
+METRIC = "particle-steps/s"
+HBM_FALLBACK_GBS = 6650.0
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return HBM_FALLBACK_GBS, "fallback"
+
+
+# ----------------------------------------------------------------- CUDA events
+class Cudart:
+    def __init__(self):
+        for name in ("libcudart.so.12", "libcudart.so"):
+            try:
+                self.lib = ctypes.CDLL(name)
+                break
+            except OSError:
+                continue
+        else:
+            self.lib = ctypes.CDLL("/usr/local/cuda/lib64/libcudart.so")
+        L = self.lib
+        L.cudaEventCreate.argtypes = [ctypes.POINTER(ctypes.c_void_p)]
+        L.cudaEventRecord.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        L.cudaEventSynchronize.argtypes = [ctypes.c_void_p]
+        L.cudaEventElapsedTime.argtypes = [ctypes.POINTER(ctypes.c_float), ctypes.c_void_p,
+                                           ctypes.c_void_p]
+        L.cudaStreamSynchronize.argtypes = [ctypes.c_void_p]
+
+    def event(self):
+        e = ctypes.c_void_p()
+        assert self.lib.cudaEventCreate(ctypes.byref(e)) == 0
+        return e
+
+    def record(self, ev, stream):
+        assert self.lib.cudaEventRecord(ev, stream) == 0
+
+    def elapsed_ms(self, a, b):
+        assert self.lib.cudaEventSynchronize(b) == 0
+        t = ctypes.c_float()
+        assert self.lib.cudaEventElapsedTime(ctypes.byref(t), a, b) == 0
+        return float(t.value)
+
+    def sync_device(self):
+        self.lib.cudaDeviceSynchronize()
+
+
+# --------------------------------------------------------------- clock sampler
+class Clocks:
+    """nvidia-smi samples of SM clock and throttle reasons during a region."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, dev):
+        self.dev = dev
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                 "-i", str(self.dev), "-lms", "50"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------ helpers
+def dist_setup(args):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def algorithmic_bytes(stage, N, npart):
+    """Algorithmic bytes per launch of each stage (each tensor counted once)."""
+    Mr = 4.0 * N ** 3
+    Ms = 8.0 * (N // 2 + 1) * N * N
+    return {
+        "fill": Mr,
+        "deposit": 12.0 * npart,
+        "fz_r2c": Mr + Ms,
+        "fy_fwd": 2 * Ms,
+        "fx_green": 4 * Ms,
+        "fy_inv": 2 * Ms,
+        "zi_c2r": Ms + Mr,
+        "interp": 12.0 * npart + 3 * Mr + 12.0 * npart,
+        "wrap": 24.0 * npart,
+        "kick": 60.0 * npart,
+        "drift": 60.0 * npart,
+    }.get(stage)
+
+
+def load_traffic():
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+def cpu_reference_step_time(cfg, parts_aos, table, steps=1, warmup=0):
+    """Time the reference's own CPU code (oracle/_ref: pm.c, cola.c, move.c
+    built unchanged against the project's MPI/FFTW/GSL shims) for `steps`
+    COLA steps after `warmup` untimed ones.  parts_aos: initial particles
+    (reference Particle layout), or None to generate them with the
+    reference's own lpt.c.  Returns (seconds per step, cores)."""
+    from cola_halo_b200.schedule import Schedule
+    from cola_halo_b200.types import HostParticles
+    from oracle import ref
+    lib = ref.load()
+    nc, factor, L, om = cfg["nc"], cfg["factor"], cfg["L"], cfg["om"]
+    sched = Schedule.linear(cfg["a_init"], 1.0, cfg["nsteps"])
+    lib.power_init(table.encode(), sched.a_init, 0.81, om, 1 - om)
+    lib.comm_init(nc * factor, nc, L)
+    lib.pm_init(nc * factor, factor, L, 1.25, None, 0, None, 0)
+    hp = HostParticles(nc)
+    if parts_aos is None:
+        lib.lpt_init(nc, None, 0)
+        lib.lpt_set_displacement(sched.a_init, om, cfg["seed"], L, hp.ptr)
+    else:
+        hp.p[: nc ** 3] = parts_aos
+        hp.struct.np_local = nc ** 3
+        hp.struct.a_x = sched.a_init
+    hp.struct.a_v = sched.a_init
+
+    def one(i):
+        _, _, avel1, apos1 = sched.times(i % (sched.nloop - 1) + 1)
+        lib.move_particles2(hp.ptr, L, None, 0)
+        lib.pm_calculate_forces(hp.ptr)
+        lib.cola_kick(hp.ptr, om, avel1)
+        lib.cola_drift(hp.ptr, om, apos1)
+    for i in range(warmup):
+        one(i)
+    t0 = time.perf_counter()
+    for i in range(steps):
+        one(warmup + i)
+    dt = (time.perf_counter() - t0) / steps
+    cores = len(os.sched_getaffinity(0))
+    return dt, cores
+
+
+# --------------------------------------------------------------- reference arm
+def run_reference(args, cfg):
+    rank, world, local = dist_setup(args)
+    if rank != 0:
+        return 0
+    from cola_halo_b200.bbks import write_bbks_table
+    npart = cfg["nc"] ** 3
+    base = {"metric": METRIC, "unit": "particle-steps/s", "impl": "reference",
+            "higher_is_better": True, "n_gpus": args.gpus}
+    try:
+        from oracle import ref
+        if not os.path.exists(ref.LIB_PATH):
+            raise RuntimeError("oracle/_ref/libcolaref.so not built")
+    except Exception as e:
+        print(json.dumps(dict(base, unavailable="reference build missing: %s" % e)))
+        return 0
+    table = write_bbks_table(os.path.join(tempfile.mkdtemp(), "bbks.dat"))
+    k_ref = max(1, min(args.steps, 3))
+    w_ref = min(args.warmup, 1)
+    dt, cores = cpu_reference_step_time(cfg, None, table, steps=k_ref, warmup=w_ref)
+    value = npart / dt
+    out = dict(base, value=value, n_gpus=args.gpus, steps=k_ref, warmup=w_ref,
+               ms_per_step=dt * 1e3, scaling="weak", vs_baseline=None, dtype="f32",
+               data="synthetic (seeded 2LPT initial conditions, BBKS P(k))",
+               config=dict(workload=args.config_desc, particles=npart,
+                           mesh=cfg["nc"] * cfg["factor"], boxsize=cfg["L"],
+                           parallelism="1 host, %d OpenMP threads" % cores),
+               cpu_baseline={"value": value, "unit": "particle-steps/s", "cores": cores,
+                             "kind": "reference",
+                             "sample": "%d COLA step(s) of the %s workload after %d warm-up; "
+                                       "shim-FFT, not FFTW" % (k_ref, args.config, w_ref)},
+               e2e={"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0})
+    print(json.dumps(out))
+    return 0
+
+
+# -------------------------------------------------------------------- B200 arm
+def run_b200(args, cfg):
+    rank, world, local = dist_setup(args)
+    dist = None
+    if world > 1:
+        import torch
+        import torch.distributed as td
+        torch.cuda.set_device(local)
+        td.init_process_group("nccl", device_id=torch.device("cuda", local),
+                              timeout=__import__("datetime").timedelta(seconds=600))
+        dist = td
+
+    def barrier():
+        if dist:
+            dist.barrier()
+
+    def allmax(v):
+        if not dist:
+            return v
+        import torch
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    from cola_halo_b200 import Simulation, _lib
+    from cola_halo_b200.bbks import write_bbks_table
+    from cola_halo_b200.schedule import Schedule
+    from cola_halo_b200.types import PARTICLE_DTYPE, PARTICLE_MIN_DTYPE, Particles, Snapshot
+
+    lib = _lib.load()
+    _lib.check(lib.cg_set_device(local), "cg_set_device")
+    cuda = Cudart()
+    nc, factor, L, om = cfg["nc"], cfg["factor"], cfg["L"], cfg["om"]
+    N = nc * factor
+    npart = nc ** 3
+    sched = Schedule.linear(cfg["a_init"], 1.0, cfg["nsteps"])
+    seed = cfg["seed"] + rank
+    table = write_bbks_table(os.path.join(tempfile.mkdtemp(), "bbks.dat"))
+
+    # ---- 2LPT initial conditions on the GPU through the drop-in API,
+    # into pinned host memory (reference Particle layout)
+    nbytes = 56 * npart
+    hp_ptr = lib.cg_host_alloc(nbytes)
+    assert hp_ptr, "pinned host allocation failed"
+    host_parts = np.ctypeslib.as_array((ctypes.c_uint8 * nbytes).from_address(hp_ptr)).view(
+        PARTICLE_DTYPE)
+    P = Particles()
+    P.p = hp_ptr
+    P.force = None
+    P.np_allocated = npart
+    P.np_total = npart
+    P.np_average = float(npart)
+    lib.cg_dropin_set_abort(0)
+    lib.power_init(table.encode(), sched.a_init, 0.81, om, 1 - om)
+    lib.lpt_init(nc, None, 0)
+    t0 = time.perf_counter()
+    rc = lib.lpt_set_displacement(sched.a_init, om, seed, L, ctypes.byref(P))
+    lpt_s = time.perf_counter() - t0
+    assert rc == 0, lib.cg_last_error()
+    ics = host_parts.copy()
+
+    # ---- device-resident step loop (value)
+    sim = Simulation(nc, N, L, om)
+    stream = lib.cg_sim_stream(sim.h)
+    nsteps_run = sched.nloop - 1
+
+    def reset():
+        sim.set_particles(ics, sched.a_init, sched.a_init)
+
+    def step(i):
+        j = i % nsteps_run
+        if j == 0:
+            reset()
+        _, _, avel1, apos1 = sched.times(j + 1)
+        sim.move()
+        sim.forces()
+        sim.kick(avel1)
+        sim.drift(apos1)
+
+    for i in range(args.warmup):
+        step(i)
+    sim.sync()
+    # one density check outside the timed region (pm.c:535-562)
+    dsum = sim.forces(check_density=True)
+    ev0, ev1 = cuda.event(), cuda.event()
+    clocks = Clocks(local)
+    prof_n = lib.cg_prof_begin(64 * (args.steps + 1))
+    barrier()
+    sim.sync()
+    clocks.start()
+    launches0 = lib.cg_launch_count()
+    cuda.record(ev0, stream)
+    for i in range(args.steps):
+        step(args.warmup + i)
+    cuda.record(ev1, stream)
+    ms = cuda.elapsed_ms(ev0, ev1)
+    launches = lib.cg_launch_count() - launches0
+    clk = clocks.stop()
+    stage_ms = (ctypes.c_double * _lib.NSTAGES)()
+    stage_n = (ctypes.c_int * _lib.NSTAGES)()
+    lib.cg_prof_end(stage_ms, stage_n, _lib.NSTAGES)
+    sim.sync()
+    barrier()
+    ms_max = allmax(ms)
+    value = world * npart * args.steps / (ms_max / 1e3)
+
+    stages = {}
+    for s in range(_lib.NSTAGES):
+        if stage_n[s]:
+            name = lib.cg_stage_name(s).decode()
+            stages[name] = {"ms": stage_ms[s], "launches": stage_n[s]}
+    # dominant kernel and its roofline
+    hbm, peak_kind = peaks()
+    dom = max(stages, key=lambda k: stages[k]["ms"])
+    per_launch_ms = stages[dom]["ms"] / stages[dom]["launches"]
+    ab = algorithmic_bytes(dom, N, npart)
+    traffic = load_traffic().get("%s@%d" % (dom, N))
+    roofline = {"kernel": dom, "bound": "hbm",
+                "achieved": ab / (per_launch_ms / 1e3) / 1e9, "peak": hbm, "unit": "GB/s",
+                "frac": ab / (per_launch_ms / 1e3) / 1e9 / hbm, "traffic": traffic,
+                "algorithmic_bytes": ab, "peak_source": peak_kind}
+
+    # ---- end to end through the drop-in C ABI with host buffers
+    sim.close()
+    snap_bytes = 32 * npart
+    sp_ptr = lib.cg_host_alloc(snap_bytes)
+    S = Snapshot()
+    S.p = sp_ptr
+    S.np_allocated = npart
+    S.np_total = npart
+    S.boxsize = L
+    S.nc = nc
+    S.omega_m = om
+    lib.pm_init(N, factor, L, 1.25, None, 0, None, 0)
+    runs = max(1, int(math.ceil(args.steps / float(sched.nloop))))
+
+    def e2e_run():
+        host_parts[:] = ics
+        P.np_local = npart
+        P.a_x = sched.a_init
+        P.a_v = sched.a_init
+        _lib.check(lib.cg_particles_upload(ctypes.byref(P)), "upload")
+        from cola_halo_b200.schedule import run_time_loop
+        run_time_loop(sched, [1.0],
+                      move=lambda: lib.move_particles2(ctypes.byref(P), L, None, 0),
+                      force=lambda: lib.pm_calculate_forces(ctypes.byref(P)),
+                      kick=lambda a: lib.cola_kick(ctypes.byref(P), om, a),
+                      drift=lambda a: lib.cola_drift(ctypes.byref(P), om, a),
+                      snapshot=lambda a, i: lib.cola_set_snapshot(a, ctypes.byref(P),
+                                                                  ctypes.byref(S)))
+        err = lib.cg_last_error()
+        if err:
+            raise RuntimeError(err.decode())
+
+    e2e_run()   # warm-up
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(runs):
+        e2e_run()
+    e2e_s = allmax(time.perf_counter() - t0)
+    e2e_value = world * npart * sched.nloop * runs / e2e_s
+    snap = np.ctypeslib.as_array((ctypes.c_uint8 * snap_bytes).from_address(sp_ptr)).view(
+        PARTICLE_MIN_DTYPE)
+    assert np.isfinite(snap["x"]).all()
+    lib.cg_dropin_finalize()
+
+    # ---- CPU baseline: the reference's own code on this host, 1 step
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            dt, cores = cpu_reference_step_time(cfg, ics, table, steps=1)
+            cpu = {"value": npart / dt, "unit": "particle-steps/s", "cores": cores,
+                   "kind": "reference",
+                   "sample": "1 COLA step of the %s workload (same 2LPT particles) with the "
+                             "reference pm.c/cola.c/move.c; shim-FFT, not FFTW" % args.config}
+        except Exception as e:  # reported, not fatal
+            cpu = {"value": None, "unit": "particle-steps/s", "cores": None,
+                   "kind": "reference", "sample": "unavailable: %s" % e}
+
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded 2LPT initial conditions, BBKS P(k))",
+            "config": {"workload": args.config_desc, "particles": npart, "mesh": N,
+                       "boxsize": L, "schedule": "10 COLA steps linear in a, z=49 -> 0",
+                       "parallelism": "replicas x%d (one realization per GPU)" % world,
+                       "l2": "inputs larger than L2 (%.2f GB per mesh)" % (4.0 * N ** 3 / 1e9)},
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": "particle-steps/s",
+                    "h2d_bytes_per_step": 56 * npart, "d2h_bytes_per_step": snap_bytes,
+                    "what": "one realization per step: drop-in C ABI (cg_particles_upload, "
+                            "move_particles2, pm_calculate_forces, cola_kick, cola_drift, "
+                            "cola_set_snapshot) from pinned host Particle[] to a host "
+                            "Snapshot; %d force evaluations" % sched.nloop},
+            "gpu_launches": int(launches),
+            "clocks": clk,
+            "stages_ms": {k: round(v["ms"] / args.steps, 4) for k, v in stages.items()},
+            "lpt_ms": lpt_s * 1e3,
+            "density_sum": dsum,
+        }
+        print(json.dumps(out))
+    lib.cg_host_free(sp_ptr)
+    lib.cg_host_free(hp_ptr)
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--config", default="c2", choices=sorted(CONFIGS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "b200":
+        args.warmup = 3
+    cfg = CONFIGS[args.config]
+    args.config_desc = "%d^3 particles, %d^3 mesh, L=%g Mpc/h, BBKS, 2LPT z=49, 10 steps" % (
+        cfg["nc"], cfg["nc"] * cfg["factor"], cfg["L"])
+    if args.impl == "reference":
+        return run_reference(args, cfg)
+    return run_b200(args, cfg)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

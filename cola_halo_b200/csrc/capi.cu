@@ -1,0 +1,681 @@
+// C ABI of libcolagpu: the cg_* handle API and the drop-in replacements of
+// the reference entry points (include/colagpu.h, include/colagpu_dropin.h).
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <map>
+#include <memory>
+#include <string>
+
+#include "../../include/colagpu.h"
+#include "../../include/colagpu_dropin.h"
+#include "cosmo.h"
+#include "internal.h"
+#include "lpt.h"
+
+// ----------------------------------------------------------------- errors
+static thread_local std::string g_err;
+
+static int set_err(int code, const char* fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+
+static int cuda_err(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return CG_OK;
+  if (e == cudaErrorMemoryAllocation)
+    return set_err(CG_ENOMEM, "%s: %s", what, cudaGetErrorString(e));
+  return set_err(CG_ECUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define CG_CHECK(expr, what)                         \
+  do {                                               \
+    cudaError_t _e = (expr);                         \
+    if (_e != cudaSuccess) return cuda_err(_e, what); \
+  } while (0)
+
+extern "C" const char* cg_last_error(void) { return g_err.c_str(); }
+extern "C" int cg_version(void) { return 1; }
+extern "C" int cg_mesh_supported(int n) { return pm_supported_mesh(n) ? 1 : 0; }
+extern "C" int cg_set_device(int dev) {
+  CG_CHECK(cudaSetDevice(dev), "cudaSetDevice");
+  return CG_OK;
+}
+extern "C" int cg_device_count(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+
+extern "C" void* cg_host_alloc(size_t bytes) {
+  void* p = nullptr;
+  if (cudaHostAlloc(&p, bytes, cudaHostAllocDefault) != cudaSuccess) {
+    set_err(CG_ENOMEM, "cudaHostAlloc(%zu) failed", bytes);
+    return nullptr;
+  }
+  return p;
+}
+extern "C" void cg_host_free(void* p) {
+  if (p) cudaFreeHost(p);
+}
+
+// ------------------------------------------------------------ cg_sim
+struct cg_sim {
+  int nc = 0;
+  float L = 0;
+  double omega_m = 0;
+  std::unique_ptr<ColaTime> ct;
+  PmPlan pm{};
+  ParticleSoA ps{};
+  float a_x = 0, a_v = 0;
+  cudaStream_t st = nullptr;
+  void* d_aos = nullptr;      // staging: Particle (56 B) / ParticleMinimum (32 B) arrays
+  float* soa_block = nullptr; // one allocation for all SoA float arrays
+};
+
+static void sim_free(cg_sim* s) {
+  if (!s) return;
+  if (s->st) cudaStreamSynchronize(s->st);
+  pm_plan_free(&s->pm);
+  cudaFree(s->soa_block);
+  cudaFree(s->ps.id);
+  cudaFree(s->d_aos);
+  if (s->st) cudaStreamDestroy(s->st);
+  delete s;
+}
+
+extern "C" int cg_sim_create(cg_sim** out, int nc, int ngrid, float boxsize, double omega_m,
+                             long long np_capacity) {
+  if (!out) return set_err(CG_EINVAL, "cg_sim_create: out is NULL");
+  *out = nullptr;
+  if (nc <= 0 || ngrid <= 0 || !(boxsize > 0.0f) || !(omega_m > 0.0 && omega_m <= 1.0))
+    return set_err(CG_EINVAL, "cg_sim_create: bad nc=%d ngrid=%d boxsize=%g omega_m=%g", nc,
+                   ngrid, boxsize, omega_m);
+  if (!pm_supported_mesh(ngrid))
+    return set_err(CG_EUNSUPPORTED, "mesh size %d is not built into this library", ngrid);
+  const long long npl = (long long)nc * nc * nc;
+  if (np_capacity < npl) np_capacity = npl;
+  cg_sim* s = new cg_sim();
+  s->nc = nc;
+  s->L = boxsize;
+  s->omega_m = omega_m;
+  s->ct.reset(new ColaTime(omega_m));
+  cudaError_t e = cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = pm_plan_alloc(&s->pm, ngrid, ngrid / nc > 0 ? ngrid / nc : 1, boxsize);
+  if (e == cudaSuccess) {
+    s->ps.cap = np_capacity;
+    e = cudaMalloc(&s->soa_block, sizeof(float) * 15 * (size_t)np_capacity);
+  }
+  if (e == cudaSuccess) e = cudaMalloc(&s->ps.id, sizeof(long long) * (size_t)np_capacity);
+  if (e == cudaSuccess) e = cudaMalloc(&s->d_aos, 56 * (size_t)np_capacity);
+  if (e != cudaSuccess) {
+    int rc = cuda_err(e, "cg_sim_create");
+    sim_free(s);
+    return rc;
+  }
+  float* b = s->soa_block;
+  const size_t c = (size_t)np_capacity;
+  for (int a = 0; a < 3; a++) {
+    s->ps.x[a] = b + (0 + a) * c;
+    s->ps.v[a] = b + (3 + a) * c;
+    s->ps.dx1[a] = b + (6 + a) * c;
+    s->ps.dx2[a] = b + (9 + a) * c;
+    s->ps.f[a] = b + (12 + a) * c;
+  }
+  cudaMemsetAsync(s->soa_block, 0, sizeof(float) * 15 * c, s->st);
+  *out = s;
+  return CG_OK;
+}
+
+extern "C" void cg_sim_destroy(cg_sim* s) { sim_free(s); }
+
+static bool is_device_ptr(const void* p) {
+  cudaPointerAttributes at;
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
+}
+
+extern "C" int cg_sim_set_particles(cg_sim* s, const void* particles, long long np, float a_x,
+                                    float a_v) {
+  if (!s || (!particles && np > 0)) return set_err(CG_EINVAL, "cg_sim_set_particles: NULL");
+  if (np < 0 || np > s->ps.cap)
+    return set_err(CG_EINVAL, "cg_sim_set_particles: np=%lld exceeds capacity %lld", np,
+                   s->ps.cap);
+  s->ps.n = np;
+  s->a_x = a_x;
+  s->a_v = a_v;
+  if (np == 0) return CG_OK;
+  const cudaMemcpyKind kind =
+      is_device_ptr(particles) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  CG_CHECK(cudaMemcpyAsync(s->d_aos, particles, 56 * (size_t)np, kind, s->st), "upload particles");
+  CG_CHECK(particles_aos_to_soa(s->d_aos, &s->ps, s->st), "aos_to_soa");
+  return CG_OK;
+}
+
+extern "C" int cg_sim_get_particles(cg_sim* s, void* particles) {
+  if (!s || !particles) return set_err(CG_EINVAL, "cg_sim_get_particles: NULL");
+  if (s->ps.n == 0) return CG_OK;
+  CG_CHECK(particles_soa_to_aos(s->d_aos, &s->ps, s->st), "soa_to_aos");
+  CG_CHECK(cudaMemcpyAsync(particles, s->d_aos, 56 * (size_t)s->ps.n, cudaMemcpyDefault, s->st),
+           "download particles");
+  CG_CHECK(cudaStreamSynchronize(s->st), "sync");
+  return CG_OK;
+}
+
+extern "C" int cg_sim_get_forces(cg_sim* s, float* f) {
+  if (!s || !f) return set_err(CG_EINVAL, "cg_sim_get_forces: NULL");
+  const size_t n = (size_t)s->ps.n;
+  if (n == 0) return CG_OK;
+  // interleave on the host side: copy three component arrays into (n,3)
+  float* tmp = (float*)malloc(sizeof(float) * 3 * n);
+  if (!tmp) return set_err(CG_ENOMEM, "host malloc");
+  for (int a = 0; a < 3; a++) {
+    cudaError_t e = cudaMemcpyAsync(tmp + a * n, s->ps.f[a], sizeof(float) * n,
+                                    cudaMemcpyDeviceToHost, s->st);
+    if (e != cudaSuccess) { free(tmp); return cuda_err(e, "download forces"); }
+  }
+  cudaError_t e = cudaStreamSynchronize(s->st);
+  if (e != cudaSuccess) { free(tmp); return cuda_err(e, "sync"); }
+  for (size_t i = 0; i < n; i++)
+    for (int a = 0; a < 3; a++) f[3 * i + a] = tmp[a * n + i];
+  free(tmp);
+  return CG_OK;
+}
+
+extern "C" int cg_sim_get_times(cg_sim* s, float* a_x, float* a_v) {
+  if (!s) return set_err(CG_EINVAL, "cg_sim_get_times: NULL");
+  if (a_x) *a_x = s->a_x;
+  if (a_v) *a_v = s->a_v;
+  return CG_OK;
+}
+
+extern "C" long long cg_sim_np(cg_sim* s) { return s ? s->ps.n : -1; }
+extern "C" void* cg_sim_stream(cg_sim* s) { return s ? (void*)s->st : nullptr; }
+
+extern "C" int cg_sim_move(cg_sim* s) {
+  if (!s) return set_err(CG_EINVAL, "cg_sim_move: NULL");
+  CG_CHECK(dev_wrap(s->ps.x, s->ps.n, s->L, s->st), "wrap");
+  return CG_OK;
+}
+
+static int check_err_word(cg_sim* s) {
+  unsigned err = 0;
+  CG_CHECK(cudaMemcpyAsync(&err, s->pm.err, sizeof(unsigned), cudaMemcpyDeviceToHost, s->st),
+           "read error word");
+  CG_CHECK(cudaStreamSynchronize(s->st), "sync");
+  if (err) {
+    cudaMemsetAsync(s->pm.err, 0, sizeof(unsigned), s->st);
+    return set_err(CG_EPARTICLE, "particle position %s (device error word 0x%x)",
+                   (err & CG_ERR_NONFINITE) ? "not finite" : "below zero in y or z", err);
+  }
+  return CG_OK;
+}
+
+extern "C" int cg_sim_forces(cg_sim* s, double* density_sum) {
+  if (!s) return set_err(CG_EINVAL, "cg_sim_forces: NULL");
+  const float* x[3] = {s->ps.x[0], s->ps.x[1], s->ps.x[2]};
+  CG_CHECK(pm_forces(&s->pm, x, s->ps.n, s->ps.f, s->st), "pm_forces");
+  if (density_sum) {
+    CG_CHECK(cudaMemcpyAsync(density_sum, s->pm.dsum, sizeof(double), cudaMemcpyDeviceToHost,
+                             s->st), "read density sum");
+    int rc = check_err_word(s);
+    if (rc) return rc;
+  }
+  return CG_OK;
+}
+
+extern "C" int cg_sim_kick_coeffs(cg_sim* s, float dda, float q1, float q2) {
+  if (!s) return set_err(CG_EINVAL, "cg_sim_kick_coeffs: NULL");
+  const float* f[3] = {s->ps.f[0], s->ps.f[1], s->ps.f[2]};
+  const float* d1[3] = {s->ps.dx1[0], s->ps.dx1[1], s->ps.dx1[2]};
+  const float* d2[3] = {s->ps.dx2[0], s->ps.dx2[1], s->ps.dx2[2]};
+  CG_CHECK(dev_kick(s->ps.v, f, d1, d2, s->ps.n, s->ct->om32, dda, q1, q2, s->st), "kick");
+  return CG_OK;
+}
+
+extern "C" int cg_sim_drift_coeffs(cg_sim* s, float dyyy, float da1, float da2) {
+  if (!s) return set_err(CG_EINVAL, "cg_sim_drift_coeffs: NULL");
+  const float* v[3] = {s->ps.v[0], s->ps.v[1], s->ps.v[2]};
+  const float* d1[3] = {s->ps.dx1[0], s->ps.dx1[1], s->ps.dx1[2]};
+  const float* d2[3] = {s->ps.dx2[0], s->ps.dx2[1], s->ps.dx2[2]};
+  CG_CHECK(dev_drift(s->ps.x, v, d1, d2, s->ps.n, dyyy, da1, da2, s->st), "drift");
+  return CG_OK;
+}
+
+extern "C" int cg_sim_kick(cg_sim* s, float avel1) {
+  if (!s) return set_err(CG_EINVAL, "cg_sim_kick: NULL");
+  float dda, q1, q2;
+  s->ct->kick(s->a_v, s->a_x, avel1, &dda, &q1, &q2);
+  int rc = cg_sim_kick_coeffs(s, dda, q1, q2);
+  if (rc) return rc;
+  s->a_v = avel1;
+  return CG_OK;
+}
+
+extern "C" int cg_sim_drift(cg_sim* s, float apos1) {
+  if (!s) return set_err(CG_EINVAL, "cg_sim_drift: NULL");
+  float dyyy, da1, da2;
+  s->ct->drift(s->a_x, s->a_v, apos1, &dyyy, &da1, &da2);
+  int rc = cg_sim_drift_coeffs(s, dyyy, da1, da2);
+  if (rc) return rc;
+  s->a_x = apos1;
+  return CG_OK;
+}
+
+// cola.c:341-384: coefficients of the final half kick and drift to aout.
+static int queue_snapshot(cg_sim* s, double aout, float omega_m, void* d_out) {
+  ColaTime ct(omega_m);
+  const float vfac = (float)(100.0 / aout);
+  const float AF = (float)aout;
+  float dda, q1, q2, dyyy, da1, da2;
+  ct.kick(s->a_v, s->a_x, AF, &dda, &q1, &q2);
+  ct.drift(s->a_x, s->a_v, AF, &dyyy, &da1, &da2);
+  const float Dv = (float)ct.DprimeQ((double)AF, 1.0);
+  const float Dv2 = (float)ct.D2v((double)AF);
+  const float* x[3] = {s->ps.x[0], s->ps.x[1], s->ps.x[2]};
+  const float* v[3] = {s->ps.v[0], s->ps.v[1], s->ps.v[2]};
+  const float* f[3] = {s->ps.f[0], s->ps.f[1], s->ps.f[2]};
+  const float* d1[3] = {s->ps.dx1[0], s->ps.dx1[1], s->ps.dx1[2]};
+  const float* d2[3] = {s->ps.dx2[0], s->ps.dx2[1], s->ps.dx2[2]};
+  CG_CHECK(dev_snapshot(x, v, f, d1, d2, s->ps.n, ct.om32, dda, q1, q2, Dv, Dv2, dyyy, da1,
+                         da2, vfac, s->ps.id, d_out, s->st),
+           "snapshot");
+  return CG_OK;
+}
+
+extern "C" int cg_sim_snapshot(cg_sim* s, double aout, float omega_m, void* pmin_out) {
+  if (!s || !pmin_out) return set_err(CG_EINVAL, "cg_sim_snapshot: NULL");
+  int rc = queue_snapshot(s, aout, omega_m, s->d_aos);
+  if (rc) return rc;
+  CG_CHECK(cudaMemcpyAsync(pmin_out, s->d_aos, 32 * (size_t)s->ps.n, cudaMemcpyDefault, s->st),
+           "download snapshot");
+  CG_CHECK(cudaStreamSynchronize(s->st), "sync");
+  return CG_OK;
+}
+
+extern "C" int cg_sim_sync(cg_sim* s) {
+  if (!s) return set_err(CG_EINVAL, "cg_sim_sync: NULL");
+  CG_CHECK(cudaStreamSynchronize(s->st), "sync");
+  return check_err_word(s);
+}
+
+extern "C" int cg_sim_get_mesh(cg_sim* s, int which, float* out) {
+  if (!s || !out || which < 0 || which > 3) return set_err(CG_EINVAL, "cg_sim_get_mesh: bad args");
+  const float* src = which == 0 ? s->pm.dens : s->pm.fmesh[which - 1];
+  CG_CHECK(cudaMemcpyAsync(out, src, s->pm.mesh_bytes, cudaMemcpyDeviceToHost, s->st), "get mesh");
+  CG_CHECK(cudaStreamSynchronize(s->st), "sync");
+  return CG_OK;
+}
+
+// ------------------------------------------------------ mesh transforms
+// Unnormalised 3-D r2c / c2r of host arrays through the device mesh passes
+// (real [x][y][z], half spectrum [kx][ky][kz], kz = 0..n/2, complex
+// interleaved), synchronous.  The c2r ignores Im of kz = 0 and n/2.
+static int host_fft(int n, const float* in, float* out, bool forward) {
+  if (!pm_supported_mesh(n) || !in || !out) return set_err(CG_EINVAL, "cg_fft: bad arguments");
+  MeshFFT f;
+  CG_CHECK(mesh_fft_alloc(&f, n), "mesh_fft_alloc");
+  const size_t nh = (size_t)(n / 2 + 1);
+  const size_t rb = sizeof(float) * (size_t)n * n * n, sb = sizeof(float2) * nh * n * n;
+  float* dr = nullptr;
+  float2* ds = nullptr;
+  float2* hs = (float2*)malloc(sb);
+  cudaError_t e = cudaMalloc(&dr, rb);
+  if (e == cudaSuccess) e = cudaMalloc(&ds, sb);
+  if (e == cudaSuccess && hs) {
+    if (forward) {
+      e = cudaMemcpy(dr, in, rb, cudaMemcpyHostToDevice);
+      if (e == cudaSuccess) e = mesh_r2c(&f, dr, ds, 0);
+      if (e == cudaSuccess) e = cudaMemcpy(hs, ds, sb, cudaMemcpyDeviceToHost);
+      // device layout [kz][kx][ky] -> host [kx][ky][kz]
+      if (e == cudaSuccess)
+        for (size_t k = 0; k < nh; k++)
+          for (size_t i = 0; i < (size_t)n; i++)
+            for (size_t j = 0; j < (size_t)n; j++) {
+              const float2 v = hs[(k * n + i) * n + j];
+              out[2 * ((i * n + j) * nh + k)] = v.x;
+              out[2 * ((i * n + j) * nh + k) + 1] = v.y;
+            }
+    } else {
+      for (size_t k = 0; k < nh; k++)
+        for (size_t i = 0; i < (size_t)n; i++)
+          for (size_t j = 0; j < (size_t)n; j++)
+            hs[(k * n + i) * n + j] = make_float2(in[2 * ((i * n + j) * nh + k)],
+                                                  in[2 * ((i * n + j) * nh + k) + 1]);
+      e = cudaMemcpy(ds, hs, sb, cudaMemcpyHostToDevice);
+      if (e == cudaSuccess) e = mesh_c2r(&f, ds, dr, 0);
+      if (e == cudaSuccess) e = cudaMemcpy(out, dr, rb, cudaMemcpyDeviceToHost);
+    }
+  }
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  cudaFree(dr);
+  cudaFree(ds);
+  free(hs);
+  mesh_fft_free(&f);
+  return cuda_err(e, "cg_fft");
+}
+
+extern "C" int cg_fft_r2c(int n, const float* real_in, float* spec_out) {
+  return host_fft(n, real_in, spec_out, true);
+}
+extern "C" int cg_fft_c2r(int n, const float* spec_in, float* real_out) {
+  return host_fft(n, spec_in, real_out, false);
+}
+
+// ------------------------------------------------------ host coefficients
+extern "C" double cg_growth_D1(double omega_m, double a) { return ColaTime(omega_m).D1(a); }
+extern "C" double cg_growth_D2(double omega_m, double a) { return ColaTime(omega_m).D2(a); }
+extern "C" double cg_cola_Sq(double omega_m, double ai, double af, double aref) {
+  return ColaTime(omega_m).Sq(ai, af, aref);
+}
+extern "C" double cg_cola_Sphi(double omega_m, double ai, double af, double aref) {
+  return ColaTime(omega_m).Sphi(ai, af, aref);
+}
+extern "C" void cg_kick_coeffs(double omega_m, float a_v, float a_x, float avel1, float out3[3]) {
+  ColaTime(omega_m).kick(a_v, a_x, avel1, &out3[0], &out3[1], &out3[2]);
+}
+extern "C" void cg_drift_coeffs(double omega_m, float a_x, float a_v, float apos1,
+                                float out3[3]) {
+  ColaTime(omega_m).drift(a_x, a_v, apos1, &out3[0], &out3[1], &out3[2]);
+}
+
+// ===================================================================
+// Drop-in layer: the reference's entry points over one process-wide
+// realization (the reference keeps file-static state the same way,
+// pm.c:45-71, lpt.c:26-39, cola.c:58).
+// ===================================================================
+namespace {
+struct DropIn {
+  int nc_pm = 0, factor = 0;
+  float boxsize = 0;
+  cg_sim* sim = nullptr;
+  const Particles* bound = nullptr;
+  const Particle* bound_p = nullptr;
+  int bound_np = -1;
+  bool full_sync = false;
+  bool abort_on_error = true;
+  int lpt_nc = 0;
+  PowerTable power;
+  bool power_ready = false;
+  double power_om = 0.3, power_ol = 0.7;
+  std::map<float, std::unique_ptr<ColaTime>> times;
+};
+DropIn g_drop;
+
+// msg_abort (msg.c:36-45): print and exit with the reference's code.
+void dropin_fail(int code, const char* fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  if (g_drop.abort_on_error) {
+    fprintf(stderr, "%s\n", buf);
+    fflush(stderr);
+    exit(code);
+  }
+}
+
+const ColaTime& times_for(float om) {
+  auto it = g_drop.times.find(om);
+  if (it == g_drop.times.end())
+    it = g_drop.times.emplace(om, std::unique_ptr<ColaTime>(new ColaTime(om))).first;
+  return *it->second;
+}
+
+// Make the device state of `p` current.  Returns false on failure.
+bool bind(const Particles* p, bool refresh) {
+  if (!g_drop.nc_pm) {
+    dropin_fail(4001, "pm_init has not been called");
+    return false;
+  }
+  const int nc = g_drop.nc_pm / g_drop.factor;
+  if (!g_drop.sim) {
+    long long cap = p->np_allocated > p->np_local ? p->np_allocated : p->np_local;
+    int rc = cg_sim_create(&g_drop.sim, nc, g_drop.nc_pm, g_drop.boxsize, 0.3, cap);
+    if (rc) {
+      dropin_fail(4001, "Unable to allocate device memory for particle mesh: %s",
+                  cg_last_error());
+      return false;
+    }
+  }
+  if (refresh || g_drop.full_sync || p != g_drop.bound || p->p != g_drop.bound_p ||
+      p->np_local != g_drop.bound_np) {
+    if (p->np_local > g_drop.sim->ps.cap) {
+      // grow: recreate with the larger capacity
+      cg_sim_destroy(g_drop.sim);
+      g_drop.sim = nullptr;
+      int rc = cg_sim_create(&g_drop.sim, nc, g_drop.nc_pm, g_drop.boxsize, 0.3, p->np_local);
+      if (rc) {
+        dropin_fail(4001, "Unable to allocate device memory: %s", cg_last_error());
+        return false;
+      }
+    }
+    if (cg_sim_set_particles(g_drop.sim, p->p, p->np_local, p->a_x, p->a_v)) {
+      dropin_fail(4002, "particle upload failed: %s", cg_last_error());
+      return false;
+    }
+    g_drop.bound = p;
+    g_drop.bound_p = p->p;
+    g_drop.bound_np = p->np_local;
+  }
+  g_drop.sim->a_x = p->a_x;
+  g_drop.sim->a_v = p->a_v;
+  return true;
+}
+
+void full_sync_download(Particles* p, bool forces) {
+  if (!g_drop.full_sync) return;
+  cg_sim_get_particles(g_drop.sim, p->p);
+  if (forces) cg_sim_get_forces(g_drop.sim, (float*)p->force);
+}
+}  // namespace
+
+extern "C" void cg_dropin_set_sync(int full) { g_drop.full_sync = full != 0; }
+extern "C" void cg_dropin_set_abort(int abort_on_error) { g_drop.abort_on_error = abort_on_error != 0; }
+
+extern "C" void cg_dropin_finalize(void) {
+  cg_sim_destroy(g_drop.sim);
+  g_drop.sim = nullptr;
+  g_drop.bound = nullptr;
+  g_drop.bound_p = nullptr;
+  g_drop.bound_np = -1;
+  g_drop.nc_pm = 0;
+  lpt_dropin_release();
+}
+
+extern "C" int cg_particles_upload(Particles* p) {
+  if (!p) return set_err(CG_EINVAL, "cg_particles_upload: NULL");
+  return bind(p, true) ? CG_OK : CG_EINVAL;
+}
+
+extern "C" int cg_particles_download(Particles* p) {
+  if (!p) return set_err(CG_EINVAL, "cg_particles_download: NULL");
+  if (!bind(p, false)) return CG_EINVAL;
+  int rc = cg_sim_get_particles(g_drop.sim, p->p);
+  if (!rc && p->force) rc = cg_sim_get_forces(g_drop.sim, (float*)p->force);
+  return rc;
+}
+
+extern "C" void pm_init(const int nc_pm, const int nc_pm_factor, const float boxsize,
+                        const float np_alloc_factor, void* const mem1, const size_t size1,
+                        void* const mem2, const size_t size2) {
+  (void)np_alloc_factor; (void)mem1; (void)size1; (void)mem2; (void)size2;
+  if (!pm_supported_mesh(nc_pm) || nc_pm_factor <= 0 || nc_pm % nc_pm_factor) {
+    dropin_fail(4001, "pm_init: unsupported mesh %d (factor %d)", nc_pm, nc_pm_factor);
+    return;
+  }
+  if (g_drop.sim && (g_drop.nc_pm != nc_pm || g_drop.boxsize != boxsize)) {
+    cg_sim_destroy(g_drop.sim);
+    g_drop.sim = nullptr;
+  }
+  g_drop.nc_pm = nc_pm;
+  g_drop.factor = nc_pm_factor;
+  g_drop.boxsize = boxsize;
+  g_drop.bound = nullptr;
+}
+
+extern "C" void move_particles2(Particles* const particles, const float BoxSize, void* const buf,
+                                const size_t size) {
+  (void)buf; (void)size;
+  if (!bind(particles, false)) return;
+  g_drop.sim->L = BoxSize;
+  if (cg_sim_move(g_drop.sim)) dropin_fail(6030, "move_particles2: %s", cg_last_error());
+  g_drop.sim->L = g_drop.boxsize;
+  full_sync_download(particles, false);
+}
+
+extern "C" void pm_calculate_forces(Particles* particles) {
+  if (!bind(particles, false)) return;
+  double sum = 0.0;
+  int rc = cg_sim_forces(g_drop.sim, &sum);
+  if (rc) {
+    dropin_fail(rc == CG_EPARTICLE ? 6040 : 4001, "pm_calculate_forces: %s", cg_last_error());
+    return;
+  }
+  // check_total_density (pm.c:548-553)
+  const long long ncp = g_drop.nc_pm / g_drop.factor;
+  const double tol = 1.0e-7 * pow((double)g_drop.factor, 3) * (double)(ncp * ncp * ncp);
+  if (fabs(sum) > tol) {
+    dropin_fail(6040, "Error: total CIC density error is large: %le > %le\n", sum, tol);
+    return;
+  }
+  full_sync_download(particles, true);
+}
+
+extern "C" void cola_kick(Particles* const particles, const float Omega_m, const float avel1) {
+  if (!bind(particles, false)) return;
+  const ColaTime& ct = times_for(Omega_m);
+  float dda, q1, q2;
+  ct.kick(particles->a_v, particles->a_x, avel1, &dda, &q1, &q2);
+  if (cg_sim_kick_coeffs(g_drop.sim, dda, q1, q2)) {
+    dropin_fail(4001, "cola_kick: %s", cg_last_error());
+    return;
+  }
+  particles->a_v = avel1;          // cola.c:115
+  g_drop.sim->a_v = avel1;
+  full_sync_download(particles, false);
+}
+
+extern "C" void cola_drift(Particles* const particles, const float Omega_m, const float apos1) {
+  if (!bind(particles, false)) return;
+  const ColaTime& ct = times_for(Omega_m);
+  float dyyy, da1, da2;
+  ct.drift(particles->a_x, particles->a_v, apos1, &dyyy, &da1, &da2);
+  if (cg_sim_drift_coeffs(g_drop.sim, dyyy, da1, da2)) {
+    dropin_fail(4001, "cola_drift: %s", cg_last_error());
+    return;
+  }
+  particles->a_x = apos1;          // cola.c:151
+  g_drop.sim->a_x = apos1;
+  full_sync_download(particles, false);
+}
+
+extern "C" void cola_set_snapshot(const double aout, Particles const* const particles,
+                                  Snapshot* const snapshot) {
+  if (!bind(particles, false)) return;
+  if (snapshot->np_allocated < particles->np_local) {
+    dropin_fail(4002, "cola_set_snapshot: snapshot holds %d < %d particles",
+                snapshot->np_allocated, particles->np_local);
+    return;
+  }
+  if (cg_sim_snapshot(g_drop.sim, aout, snapshot->omega_m, snapshot->p)) {
+    dropin_fail(4001, "cola_set_snapshot: %s", cg_last_error());
+    return;
+  }
+  snapshot->np_local = particles->np_local;          // cola.c:412-414
+  snapshot->np_average = particles->np_average;
+  snapshot->a = (float)aout;
+}
+
+// ---------------------------------------------------------- power.c
+extern "C" void power_init(const char filename[], const double a_init, const double sigma8,
+                           const double omega_m, const double omega_lambda) {
+  (void)a_init;
+  char err[512];
+  g_drop.power_om = omega_m;
+  g_drop.power_ol = omega_lambda;
+  if (!g_drop.power.read(filename, err, sizeof(err))) {
+    g_drop.power_ready = false;
+    dropin_fail(3000, "Error: %s", err);
+    return;
+  }
+  g_drop.power.norm = 1.0;
+  const double s8 = sqrt(g_drop.power.sigma2(8.0));        // power.c:103-118
+  if (fabs(s8 - sigma8) / sigma8 > 0.05) {
+    g_drop.power_ready = false;
+    dropin_fail(3010, "Input sigma8 %f is far from target sigma8 %f\n", s8, sigma8);
+    return;
+  }
+  g_drop.power_ready = true;
+}
+
+extern "C" double PowerSpec(const double k) {
+  return g_drop.power_ready ? g_drop.power(k) : 0.0;
+}
+
+extern "C" double GrowthFactor(double astart, double aend) {
+  return linear_growth(aend, g_drop.power_om, g_drop.power_ol) /
+         linear_growth(astart, g_drop.power_om, g_drop.power_ol);
+}
+
+// ------------------------------------------------------------- lpt.c
+extern "C" void lpt_init(const int nc, const void* mem, const size_t size) {
+  (void)mem; (void)size;
+  if (nc <= 0 || nc % 2) {
+    dropin_fail(2003, "lpt_init: nc=%d must be even and positive", nc);
+    return;
+  }
+  g_drop.lpt_nc = nc;
+}
+
+extern "C" int lpt_get_local_nx(void) { return g_drop.lpt_nc; }
+
+extern "C" int lpt_set_displacement(const double InitTime, const double omega_m, const int Seed,
+                                    const double Box, Particles* particles) {
+  if (!g_drop.lpt_nc) {
+    dropin_fail(2003, "lpt_init has not been called");
+    return -1;
+  }
+  if (!g_drop.power_ready) {
+    dropin_fail(3000, "power_init has not been called");
+    return -1;
+  }
+  const int nc = g_drop.lpt_nc;
+  const long long np = (long long)nc * nc * nc;
+  if (particles->np_allocated < np) {
+    dropin_fail(2003, "lpt_set_displacement: %d particles allocated, %lld needed",
+                particles->np_allocated, np);
+    return -1;
+  }
+  const double dplus = 1.0 / GrowthFactor(InitTime, 1.0);             // lpt.c:509
+  int rc = lpt_generate(nc, Box, Seed, omega_m, InitTime, dplus, g_drop.power,
+                        particles->p);
+  if (rc) {
+    dropin_fail(2003, "lpt_set_displacement: %s", cg_last_error());
+    return -1;
+  }
+  particles->np_local = (int)np;                                     // lpt.c:573-575
+  particles->a_x = (float)InitTime;
+  particles->a_v = 0.0f;
+  g_drop.bound = nullptr;            // next call uploads the new particles
+  return 0;
+}
+
+int cg_set_error_from_lpt(int code, const char* msg) { return set_err(code, "%s", msg); }

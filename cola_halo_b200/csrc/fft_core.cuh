@@ -1,0 +1,221 @@
+// Shared-memory batched FFT building blocks for the PM mesh transforms.
+//
+// A CTA holds a tile of B complex lines of length L in shared memory and runs
+// a self-sorting (Stockham) decimation-in-time FFT on it, one radix stage at a
+// time: every thread loads all the butterfly inputs it owns into registers,
+// the CTA synchronises, then each thread twiddles, does its radix-R DFTs in
+// registers and writes the outputs back in place.  Radices 16, 8, 4, 2, 3.
+// Twiddles come from a table W_L[k] = exp(-2 pi i k / L) computed on the host
+// in double precision and rounded once to float (one table per line length).
+//
+// Stage s with radix R after sub-transforms of size NS (Stockham autosort):
+//   inputs   a[j + r L/R],                          r = 0..R-1
+//   twiddle  a_r *= W_L^{(j mod NS) r L/(NS R)}     (conjugated for inverse)
+//   DFT_R
+//   outputs  a[(j / NS) NS R + (j mod NS) + r NS]
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace cgfft {
+
+// ------------------------------------------------------------ complex ops
+struct cplx { float x, y; };
+
+__device__ __forceinline__ cplx cmul(cplx a, cplx b) {
+  return {a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x};
+}
+__device__ __forceinline__ cplx cadd(cplx a, cplx b) { return {a.x + b.x, a.y + b.y}; }
+__device__ __forceinline__ cplx csub(cplx a, cplx b) { return {a.x - b.x, a.y - b.y}; }
+// multiply by -i (forward) or +i (inverse):  DIR = -1 forward, +1 inverse
+template <int DIR> __device__ __forceinline__ cplx mul_i(cplx a) {
+  return DIR < 0 ? cplx{a.y, -a.x} : cplx{-a.y, a.x};
+}
+template <int DIR> __device__ __forceinline__ cplx twiddle(const float2* __restrict__ tw, int t) {
+  float2 w = __ldg(tw + t);
+  return DIR < 0 ? cplx{w.x, w.y} : cplx{w.x, -w.y};
+}
+
+// ------------------------------------------------------- radix-R kernels
+// In-register DFT of R points with exp(DIR * 2 pi i k m / R).
+template <int DIR> __device__ __forceinline__ void dft2(cplx* v) {
+  cplx a = v[0], b = v[1];
+  v[0] = cadd(a, b); v[1] = csub(a, b);
+}
+
+template <int DIR> __device__ __forceinline__ void dft3(cplx* v) {
+  // c = cos(2 pi/3) = -1/2, s = sin(2 pi/3) = sqrt(3)/2
+  const float s = 0.866025403784438646763723170753f;
+  cplx a = v[0], b = v[1], c = v[2];
+  cplx t = cadd(b, c);
+  cplx d = csub(b, c);
+  cplx m = {a.x - 0.5f * t.x, a.y - 0.5f * t.y};
+  // DIR*i*s*d
+  cplx r = DIR < 0 ? cplx{s * d.y, -s * d.x} : cplx{-s * d.y, s * d.x};
+  v[0] = cadd(a, t);
+  v[1] = cadd(m, r);
+  v[2] = csub(m, r);
+}
+
+template <int DIR> __device__ __forceinline__ void dft4(cplx* v) {
+  cplx s0 = cadd(v[0], v[2]), d0 = csub(v[0], v[2]);
+  cplx s1 = cadd(v[1], v[3]), d1 = mul_i<DIR>(csub(v[1], v[3]));
+  v[0] = cadd(s0, s1);
+  v[2] = csub(s0, s1);
+  v[1] = cadd(d0, d1);
+  v[3] = csub(d0, d1);
+}
+
+// 8-point: two 4-point DFTs on even/odd samples, then the W8 butterflies.
+template <int DIR> __device__ __forceinline__ void dft8(cplx* v) {
+  const float h = 0.707106781186547524400844362105f;
+  cplx e[4] = {v[0], v[2], v[4], v[6]};
+  cplx o[4] = {v[1], v[3], v[5], v[7]};
+  dft4<DIR>(e);
+  dft4<DIR>(o);
+  // o[k] *= W8^{DIR k}: k=1: (h, DIR h), k=2: DIR i, k=3: (-h, DIR h)
+  cplx o1 = o[1], o3 = o[3];
+  o[1] = DIR < 0 ? cplx{h * (o1.x + o1.y), h * (o1.y - o1.x)}
+                 : cplx{h * (o1.x - o1.y), h * (o1.y + o1.x)};
+  o[2] = mul_i<DIR>(o[2]);
+  o[3] = DIR < 0 ? cplx{h * (o3.y - o3.x), -h * (o3.x + o3.y)}
+                 : cplx{-h * (o3.x + o3.y), h * (o3.x - o3.y)};
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    v[k] = cadd(e[k], o[k]);
+    v[k + 4] = csub(e[k], o[k]);
+  }
+}
+
+// 16-point: 4x4 decomposition, n = 4 n1 + n2, k = k1 + 4 k2.
+template <int DIR> __device__ __forceinline__ void dft16(cplx* v) {
+  // W16^m = (cos(2 pi m/16), DIR sin(2 pi m/16)) for the chosen direction
+  const float c1 = 0.923879532511286756128183189397f;  // cos(pi/8)
+  const float s1 = 0.382683432365089771728459984030f;  // sin(pi/8)
+  const float h = 0.707106781186547524400844362105f;
+  cplx a[4][4];
+#pragma unroll
+  for (int n2 = 0; n2 < 4; n2++) {
+    cplx t[4] = {v[n2], v[n2 + 4], v[n2 + 8], v[n2 + 12]};
+    dft4<DIR>(t);
+#pragma unroll
+    for (int k1 = 0; k1 < 4; k1++) a[n2][k1] = t[k1];
+  }
+  // twiddle a[n2][k1] *= W16^{DIR n2 k1}
+  const float ds = DIR < 0 ? -1.0f : 1.0f;
+  const cplx w1 = {c1, ds * s1}, w2 = {h, ds * h}, w3 = {s1, ds * c1};
+  const cplx w6 = {-h, ds * h}, w9 = {-c1, -ds * s1};
+  a[1][1] = cmul(a[1][1], w1); a[1][2] = cmul(a[1][2], w2); a[1][3] = cmul(a[1][3], w3);
+  a[2][1] = cmul(a[2][1], w2); a[2][2] = mul_i<DIR>(a[2][2]); a[2][3] = cmul(a[2][3], w6);
+  a[3][1] = cmul(a[3][1], w3); a[3][2] = cmul(a[3][2], w6); a[3][3] = cmul(a[3][3], w9);
+#pragma unroll
+  for (int k1 = 0; k1 < 4; k1++) {
+    cplx t[4] = {a[0][k1], a[1][k1], a[2][k1], a[3][k1]};
+    dft4<DIR>(t);
+#pragma unroll
+    for (int k2 = 0; k2 < 4; k2++) v[k1 + 4 * k2] = t[k2];
+  }
+}
+
+template <int R, int DIR> __device__ __forceinline__ void dft(cplx* v) {
+  if constexpr (R == 2) dft2<DIR>(v);
+  else if constexpr (R == 3) dft3<DIR>(v);
+  else if constexpr (R == 4) dft4<DIR>(v);
+  else if constexpr (R == 8) dft8<DIR>(v);
+  else if constexpr (R == 16) dft16<DIR>(v);
+}
+
+// ------------------------------------------------- factorisation of L
+// Radices in application order: 16s, then one of 8/4/2, then 3s.
+__host__ __device__ constexpr int radix_at(int L, int s) {
+  int m = L;
+  int idx = 0;
+  while (m % 16 == 0 && m / 16 >= 1) {
+    if (idx == s) return 16;
+    m /= 16; idx++;
+  }
+  if (m % 8 == 0) { if (idx == s) return 8; m /= 8; idx++; }
+  else if (m % 4 == 0) { if (idx == s) return 4; m /= 4; idx++; }
+  else if (m % 2 == 0) { if (idx == s) return 2; m /= 2; idx++; }
+  while (m % 3 == 0) {
+    if (idx == s) return 3;
+    m /= 3; idx++;
+  }
+  return 0;
+}
+__host__ __device__ constexpr int num_stages(int L) {
+  int s = 0;
+  while (radix_at(L, s) != 0) s++;
+  return s;
+}
+__host__ __device__ constexpr int ns_before(int L, int s) {
+  int ns = 1;
+  for (int i = 0; i < s; i++) ns *= radix_at(L, i);
+  return ns;
+}
+__host__ __device__ constexpr bool supported_length(int L) {
+  int prod = 1;
+  for (int s = 0; s < num_stages(L); s++) prod *= radix_at(L, s);
+  return prod == L && L >= 2;
+}
+
+// ------------------------------------------------------------ one stage
+// Tile access: element n of line b lives at s[b * SB + n * SN].
+// LINE_MAJOR: consecutive threads take consecutive butterflies of one line
+// (conflict-free when SN == 1); otherwise consecutive lines (SB == 1).
+template <int L, int R, int NS, int B, int T, int SB, int SN, bool LINE_MAJOR, int DIR>
+__device__ __forceinline__ void stage(cplx* s, const float2* __restrict__ tw) {
+  constexpr int NBF = L / R;
+  constexpr int TOTAL = NBF * B;
+  constexpr int PER = (TOTAL + T - 1) / T;
+  cplx v[PER][R];
+  const int tid = threadIdx.x;
+#pragma unroll
+  for (int q = 0; q < PER; q++) {
+    const int idx = tid + q * T;
+    if (TOTAL % T == 0 || idx < TOTAL) {
+      const int b = LINE_MAJOR ? idx / NBF : idx % B;
+      const int j = LINE_MAJOR ? idx % NBF : idx / B;
+#pragma unroll
+      for (int r = 0; r < R; r++) v[q][r] = s[b * SB + (j + r * NBF) * SN];
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < PER; q++) {
+    const int idx = tid + q * T;
+    if (TOTAL % T == 0 || idx < TOTAL) {
+      const int b = LINE_MAJOR ? idx / NBF : idx % B;
+      const int j = LINE_MAJOR ? idx % NBF : idx / B;
+      const int jm = NS == 1 ? 0 : j % NS;
+      if (NS > 1) {
+        constexpr int STEP = L / (NS * R);
+#pragma unroll
+        for (int r = 1; r < R; r++) v[q][r] = cmul(v[q][r], twiddle<DIR>(tw, jm * r * STEP));
+      }
+      dft<R, DIR>(v[q]);
+      const int base = (j / NS) * NS * R + jm;
+#pragma unroll
+      for (int r = 0; r < R; r++) s[b * SB + (base + r * NS) * SN] = v[q][r];
+    }
+  }
+  __syncthreads();
+}
+
+template <int L, int S, int B, int T, int SB, int SN, bool LINE_MAJOR, int DIR>
+__device__ __forceinline__ void fft_from(cplx* s, const float2* __restrict__ tw) {
+  if constexpr (S < num_stages(L)) {
+    stage<L, radix_at(L, S), ns_before(L, S), B, T, SB, SN, LINE_MAJOR, DIR>(s, tw);
+    fft_from<L, S + 1, B, T, SB, SN, LINE_MAJOR, DIR>(s, tw);
+  }
+}
+
+// Full in-place FFT of B lines of length L held in shared memory.
+// The caller must __syncthreads() before (tile loaded); returns synchronised.
+template <int L, int B, int T, int SB, int SN, bool LINE_MAJOR, int DIR>
+__device__ __forceinline__ void fft_lines(cplx* s, const float2* __restrict__ tw) {
+  static_assert(supported_length(L), "FFT length must be 2^a 3^b");
+  fft_from<L, 0, B, T, SB, SN, LINE_MAJOR, DIR>(s, tw);
+}
+
+}  // namespace cgfft

@@ -1,0 +1,106 @@
+// Internal declarations shared by the CUDA translation units of libcolagpu.
+#pragma once
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#define CG_THREADS 256
+
+// Stages of the step, for launch accounting and event timing (prof.cu).
+enum {
+  CG_ST_FILL = 0, CG_ST_DEPOSIT, CG_ST_FZ, CG_ST_FY_FWD, CG_ST_FX_GREEN, CG_ST_FY_INV,
+  CG_ST_ZI, CG_ST_INTERP, CG_ST_WRAP, CG_ST_KICK, CG_ST_DRIFT, CG_ST_SNAPSHOT, CG_ST_LPT,
+  CG_ST_OTHER, CG_ST_COUNT
+};
+// Call before every kernel launch: counts it and, while a profile is open,
+// records a CUDA event on the launch stream.
+void prof_mark(cudaStream_t st, int stage);
+
+// Device error word bits (set by kernels, read by the host after a step).
+enum {
+  CG_ERR_BAD_CELL = 1,      // a particle's y or z cell index was negative
+  CG_ERR_NONFINITE = 2,     // a particle position was NaN or infinite
+};
+
+// Mesh transform plan: every buffer of one PM mesh size.
+struct PmPlan {
+  int N;                    // mesh cells per dimension
+  int factor;               // PM factor (mesh/particle per dimension)
+  float L;                  // box size
+  float scale;              // (float)N / (float)L                 pm.c:215
+  float wpar;               // factor^3                            pm.c:216
+  float f1;                 // -1/N^3/(2 pi/L) as float            pm.c:315-317
+  float x_right;            // buffer-particle threshold           pm.c:422-423
+  float shiftx;             // -L                                  pm.c:434
+  float* dens;              // real mesh [x][y][z], N^3
+  float2* spec;             // half spectrum [kz][kx][ky], (N/2+1) N N
+  float2* gsp[3];           // force spectra, same layout
+  float* fmesh[3];          // real force meshes [x][y][z]
+  float2* twN;              // exp(-2 pi i k/N), k < N
+  float2* twH;              // exp(-2 pi i k/(N/2)), k < N/2
+  double* dsum;             // device: sum of the density mesh (check)
+  unsigned* err;            // device: error word
+  size_t mesh_bytes;        // bytes of one real mesh
+  size_t spec_bytes;        // bytes of one half spectrum
+};
+
+// Plain 3-D real transforms on the mesh layouts above (unnormalised, FFTW
+// sign and c2r conventions).  mesh_c2r overwrites its input spectrum.
+struct MeshFFT {
+  int N;
+  float2* twN;
+  float2* twH;
+  double* dsum;             // scratch: receives the sum of the r2c input
+};
+cudaError_t mesh_fft_alloc(MeshFFT* f, int N);
+void mesh_fft_free(MeshFFT* f);
+cudaError_t mesh_r2c(const MeshFFT* f, const float* real, float2* spec, cudaStream_t st);
+cudaError_t mesh_c2r(const MeshFFT* f, float2* spec, float* real, cudaStream_t st);
+
+// pm_kernels.cu
+bool pm_supported_mesh(int N);
+cudaError_t pm_plan_alloc(PmPlan* p, int N, int factor, float L);
+void pm_plan_free(PmPlan* p);
+// Full PM force: deposit -> r2c -> Green/gradient -> 3 c2r -> interpolation.
+// Positions and forces are SoA device arrays of n floats per component.
+cudaError_t pm_forces(PmPlan* p, const float* const x[3], long long n,
+                      float* const f[3], cudaStream_t st);
+// Individual stages (exposed for tests and timing).
+cudaError_t pm_deposit(PmPlan* p, const float* const x[3], long long n, cudaStream_t st);
+cudaError_t pm_r2c(PmPlan* p, cudaStream_t st);
+cudaError_t pm_green_c2r(PmPlan* p, cudaStream_t st);
+cudaError_t pm_interp(PmPlan* p, const float* const x[3], long long n,
+                      float* const f[3], cudaStream_t st);
+
+// Particle state on the device, structure of arrays (one array per
+// component), in the caller's particle order.
+struct ParticleSoA {
+  long long n;              // particles held
+  long long cap;            // capacity
+  float* x[3];
+  float* v[3];
+  float* dx1[3];
+  float* dx2[3];
+  float* f[3];
+  long long* id;
+};
+
+// cola_kernels.cu
+cudaError_t dev_wrap(float* const x[3], long long n, float L, cudaStream_t st);
+cudaError_t dev_kick(float* const v[3], const float* const f[3],
+                      const float* const dx1[3], const float* const dx2[3],
+                      long long n, float omega_m, float dda, float q1, float q2,
+                      cudaStream_t st);
+cudaError_t dev_drift(float* const x[3], const float* const v[3],
+                       const float* const dx1[3], const float* const dx2[3],
+                       long long n, float dyyy, float da1, float da2, cudaStream_t st);
+cudaError_t dev_snapshot(const float* const x[3], const float* const v[3],
+                          const float* const f[3], const float* const dx1[3],
+                          const float* const dx2[3], long long n,
+                          float omega_m, float dda, float q1, float q2,
+                          float Dv, float Dv2, float dyyy, float da1, float da2,
+                          float vfac, const long long* id, void* out_aos,
+                          cudaStream_t st);
+// AoS (reference Particle, 56 B) <-> SoA conversion on the device.
+cudaError_t particles_aos_to_soa(const void* aos, ParticleSoA* s, cudaStream_t st);
+cudaError_t particles_soa_to_aos(void* aos, const ParticleSoA* s, cudaStream_t st);

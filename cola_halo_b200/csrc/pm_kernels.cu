@@ -1,0 +1,619 @@
+// Particle-mesh force on one B200: CIC deposit, 3-D r2c, Green's function /
+// spectral gradient, three 3-D c2r, CIC interpolation.
+//
+// Reference: pm.c:209-412 (PtoMesh, compute_density_k, compute_force_mesh,
+// force_at_particle_locations) and pm.c:416-532 (buffer particles), on one
+// process.  The x-direction periodicity that the reference obtains from
+// buffer particles is restated exactly: a particle with x > x_right also
+// acts through a copy at x - L, with that copy's own CIC weights.
+//
+// Mesh layouts in HBM
+//   real   R[x][y][z]        N^3 floats, z contiguous, no padding
+//   half   S[kz][kx][ky]     (N/2+1) N N complex floats, ky contiguous
+// Transform passes (each one read + one write of a mesh):
+//   FZ   r2c along z of R, transposed store into S        (+ density sum)
+//   FY   c2c along ky, contiguous lines, in place
+//   FX   forward c2c along kx, Green/gradient for the 3 axes, inverse c2c
+//        along kx  -> three spectra G_a (one read, three writes)
+//   FY   inverse c2c along ky on each G_a
+//   ZI   c2r along z of G_a, transposed load, store R_a
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "fft_core.cuh"
+#include "internal.h"
+
+using cgfft::cplx;
+
+namespace {
+
+constexpr int T = CG_THREADS;
+constexpr int TY = 16;   // z-lines per CTA in FZ / ZI
+constexpr int BY = 8;    // y-lines per CTA in FY
+constexpr int TK = 8;    // ky columns per CTA in FX
+
+// ------------------------------------------------------------------ fill
+__global__ void k_fill(float4* __restrict__ p, size_t n4, float v) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  size_t stride = (size_t)gridDim.x * blockDim.x;
+  for (; i < n4; i += stride) p[i] = make_float4(v, v, v, v);
+}
+
+// ------------------------------------------------------------ CIC index
+// pm.c:230-258: cell and weights of one position (float arithmetic, no FMA).
+struct Cic {
+  int i0, i1, j0, j1, k0, k1;
+  float d1, d2, d3, t1, t2, t3;
+  bool ok;
+};
+
+__device__ __forceinline__ Cic cic_index(float px, float py, float pz, int N, float scale) {
+  Cic c;
+  const float X = __fmul_rn(px, scale);
+  const float Y = __fmul_rn(py, scale);
+  const float Z = __fmul_rn(pz, scale);
+  c.ok = isfinite(X) && isfinite(Y) && isfinite(Z);
+  int iI = (int)floorf(X);
+  int J = __float2int_rz(Y);
+  int K = __float2int_rz(Z);
+  c.d1 = __fsub_rn(X, (float)iI);
+  c.d2 = __fsub_rn(Y, (float)J);
+  c.d3 = __fsub_rn(Z, (float)K);
+  c.t1 = __fsub_rn(1.0f, c.d1);
+  c.t2 = __fsub_rn(1.0f, c.d2);
+  c.t3 = __fsub_rn(1.0f, c.d3);
+  if (J >= N) J = 0;
+  if (K >= N) K = 0;
+  if (J < 0 || K < 0) c.ok = false;   // the reference assumes y, z >= 0
+  c.i0 = iI;
+  c.i1 = iI + 1;
+  c.j0 = J;
+  c.j1 = J + 1 >= N ? 0 : J + 1;
+  c.k0 = K;
+  c.k1 = K + 1 >= N ? 0 : K + 1;
+  return c;
+}
+
+__device__ __forceinline__ size_t cell(int i, int j, int k, int N) {
+  return ((size_t)i * N + j) * N + k;
+}
+
+__device__ __forceinline__ void deposit_one(float* __restrict__ d, const Cic& c, int N,
+                                            float wpar) {
+  const float T2W = __fmul_rn(c.t2, wpar);
+  const float D2W = __fmul_rn(c.d2, wpar);
+  if (0 <= c.i0 && c.i0 < N) {
+    atomicAdd(d + cell(c.i0, c.j0, c.k0, N), __fmul_rn(__fmul_rn(c.t3, c.t1), T2W));
+    atomicAdd(d + cell(c.i0, c.j0, c.k1, N), __fmul_rn(__fmul_rn(c.d3, c.t1), T2W));
+    atomicAdd(d + cell(c.i0, c.j1, c.k0, N), __fmul_rn(__fmul_rn(c.t3, c.t1), D2W));
+    atomicAdd(d + cell(c.i0, c.j1, c.k1, N), __fmul_rn(__fmul_rn(c.d3, c.t1), D2W));
+  }
+  if (0 <= c.i1 && c.i1 < N) {
+    atomicAdd(d + cell(c.i1, c.j0, c.k0, N), __fmul_rn(__fmul_rn(c.t3, c.d1), T2W));
+    atomicAdd(d + cell(c.i1, c.j0, c.k1, N), __fmul_rn(__fmul_rn(c.d3, c.d1), T2W));
+    atomicAdd(d + cell(c.i1, c.j1, c.k0, N), __fmul_rn(__fmul_rn(c.t3, c.d1), D2W));
+    atomicAdd(d + cell(c.i1, c.j1, c.k1, N), __fmul_rn(__fmul_rn(c.d3, c.d1), D2W));
+  }
+}
+
+// PtoMesh (pm.c:229-276) incl. the buffer copy of send_buffer_positions
+// (pm.c:437-445, 477-481).  The mesh holds -1 on entry (pm.c:221-224).
+__global__ void __launch_bounds__(T) k_deposit(const float* __restrict__ x0,
+                                               const float* __restrict__ x1,
+                                               const float* __restrict__ x2, long long n,
+                                               float* __restrict__ dens, int N, float scale,
+                                               float wpar, float x_right, float shiftx,
+                                               unsigned* __restrict__ err) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (; i < n; i += stride) {
+    const float px = x0[i], py = x1[i], pz = x2[i];
+    Cic c = cic_index(px, py, pz, N, scale);
+    if (!c.ok) {
+      atomicOr(err, isfinite(px) && isfinite(py) && isfinite(pz) ? CG_ERR_BAD_CELL
+                                                                  : CG_ERR_NONFINITE);
+      continue;
+    }
+    deposit_one(dens, c, N, wpar);
+    if (px > x_right) {
+      Cic g = cic_index(__fadd_rn(px, shiftx), py, pz, N, scale);
+      if (g.ok) deposit_one(dens, g, N, wpar);
+    }
+  }
+}
+
+// force_at_particle_locations (pm.c:370-411) for all three axes, plus the
+// buffer copy's force added back as in add_buffer_forces (pm.c:526-531).
+__device__ __forceinline__ float gather4(const float* __restrict__ m, int i, const Cic& c,
+                                         int N, float wi) {
+  // ((m*T3)*Ti)*T2 + ((m*D3)*Ti)*T2 + ((m*T3)*Ti)*D2 + ((m*D3)*Ti)*D2
+  float a = __fmul_rn(__fmul_rn(__fmul_rn(__ldg(m + cell(i, c.j0, c.k0, N)), c.t3), wi), c.t2);
+  float b = __fmul_rn(__fmul_rn(__fmul_rn(__ldg(m + cell(i, c.j0, c.k1, N)), c.d3), wi), c.t2);
+  float d = __fmul_rn(__fmul_rn(__fmul_rn(__ldg(m + cell(i, c.j1, c.k0, N)), c.t3), wi), c.d2);
+  float e = __fmul_rn(__fmul_rn(__fmul_rn(__ldg(m + cell(i, c.j1, c.k1, N)), c.d3), wi), c.d2);
+  return __fadd_rn(__fadd_rn(__fadd_rn(a, b), d), e);
+}
+
+__device__ __forceinline__ float interp_one(const float* __restrict__ m, const Cic& c, int N) {
+  float f = 0.0f;
+  if (0 <= c.i0 && c.i0 < N) f = __fadd_rn(f, gather4(m, c.i0, c, N, c.t1));
+  if (0 <= c.i1 && c.i1 < N) f = __fadd_rn(f, gather4(m, c.i1, c, N, c.d1));
+  return f;
+}
+
+__global__ void __launch_bounds__(T) k_interp(const float* __restrict__ x0,
+                                              const float* __restrict__ x1,
+                                              const float* __restrict__ x2, long long n,
+                                              const float* __restrict__ m0,
+                                              const float* __restrict__ m1,
+                                              const float* __restrict__ m2,
+                                              float* __restrict__ f0, float* __restrict__ f1,
+                                              float* __restrict__ f2, int N, float scale,
+                                              float x_right, float shiftx) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (; i < n; i += stride) {
+    const float px = x0[i], py = x1[i], pz = x2[i];
+    Cic c = cic_index(px, py, pz, N, scale);
+    float a = 0.0f, b = 0.0f, d = 0.0f;
+    if (c.ok) {
+      a = interp_one(m0, c, N);
+      b = interp_one(m1, c, N);
+      d = interp_one(m2, c, N);
+      if (px > x_right) {
+        Cic g = cic_index(__fadd_rn(px, shiftx), py, pz, N, scale);
+        if (g.ok) {
+          a = __fadd_rn(a, interp_one(m0, g, N));
+          b = __fadd_rn(b, interp_one(m1, g, N));
+          d = __fadd_rn(d, interp_one(m2, g, N));
+        }
+      }
+    }
+    f0[i] = a;
+    f1[i] = b;
+    f2[i] = d;
+  }
+}
+
+// ------------------------------------------------------------- FZ: r2c z
+// One CTA: the TY z-lines (x, y0..y0+TY-1), contiguous in R.  Real FFT of
+// length N through a complex FFT of length H = N/2 on (x_2m + i x_2m+1):
+//   X_k = E_k + W_N^k O_k,  E_k = (Z_k + conj Z_{H-k})/2,
+//   O_k = -i (Z_k - conj Z_{H-k})/2,            k = 0..H
+// The sum of all mesh values (check_total_density, pm.c:535-562) is
+// accumulated in double on the way in.
+template <int N>
+__global__ void __launch_bounds__(T) k_fz_r2c(const float* __restrict__ dens,
+                                              float2* __restrict__ spec,
+                                              const float2* __restrict__ twH,
+                                              const float2* __restrict__ twN,
+                                              double* __restrict__ dsum) {
+  constexpr int H = N / 2;
+  constexpr int SB = H + 1;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  cplx* sm = reinterpret_cast<cplx*>(smraw);
+  const int x = blockIdx.y;
+  const int y0 = blockIdx.x * TY;
+  const float2* src = reinterpret_cast<const float2*>(dens + ((size_t)x * N + y0) * N);
+  double acc = 0.0;
+  for (int idx = threadIdx.x; idx < TY * H; idx += T) {
+    const float2 v = src[idx];
+    const int b = idx / H, m = idx - (idx / H) * H;
+    sm[b * SB + m] = cplx{v.x, v.y};
+    acc += (double)v.x + (double)v.y;
+  }
+  // warp reduce, one atomic per warp
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(dsum, acc);
+  __syncthreads();
+  cgfft::fft_lines<H, TY, T, SB, 1, true, -1>(sm, twH);
+  for (int idx = threadIdx.x; idx < (H + 1) * TY; idx += T) {
+    const int b = idx % TY, k = idx / TY;
+    const cplx zk = sm[b * SB + (k == H ? 0 : k)];
+    const cplx zc0 = sm[b * SB + (k == 0 ? 0 : H - k)];
+    const cplx zc = {zc0.x, -zc0.y};
+    const cplx e = {0.5f * (zk.x + zc.x), 0.5f * (zk.y + zc.y)};
+    const cplx dlt = {zk.x - zc.x, zk.y - zc.y};
+    const cplx o = {0.5f * dlt.y, -0.5f * dlt.x};
+    const float2 w = __ldg(twN + k);
+    const cplx X = {e.x + (w.x * o.x - w.y * o.y), e.y + (w.x * o.y + w.y * o.x)};
+    spec[((size_t)k * N + x) * N + y0 + b] = make_float2(X.x, X.y);
+  }
+}
+
+// --------------------------------------------------- FY: c2c along y
+template <int N, int DIR>
+__global__ void __launch_bounds__(T) k_fy(float2* __restrict__ spec,
+                                          const float2* __restrict__ twN) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  cplx* sm = reinterpret_cast<cplx*>(smraw);
+  float4* g = reinterpret_cast<float4*>(spec + (size_t)blockIdx.x * BY * N);
+  float4* s4 = reinterpret_cast<float4*>(sm);
+  for (int idx = threadIdx.x; idx < BY * N / 2; idx += T) s4[idx] = g[idx];
+  __syncthreads();
+  cgfft::fft_lines<N, BY, T, N, 1, true, DIR>(sm, twN);
+  for (int idx = threadIdx.x; idx < BY * N / 2; idx += T) g[idx] = s4[idx];
+}
+
+// ------------------------------- FX: x forward + Green/gradient + x inverse
+// compute_force_mesh (pm.c:304-346):  F_a = i f2 delta_k,
+//   f2 = f1 / (K^2 + I0^2 + J0^2) * n_a,  f1 = -1/(N^3 2 pi/L),
+//   I0, J0 signed with the Nyquist index kept at +N/2, F(0,0,0) = 0.
+template <int N>
+__global__ void __launch_bounds__(T) k_fx_green(const float2* __restrict__ spec,
+                                                float2* __restrict__ g0,
+                                                float2* __restrict__ g1,
+                                                float2* __restrict__ g2,
+                                                const float2* __restrict__ twN, float f1) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  cplx* D = reinterpret_cast<cplx*>(smraw);
+  cplx* W = D + N * TK;
+  const int kz = blockIdx.y;
+  const int ky0 = blockIdx.x * TK;
+  const size_t plane = (size_t)kz * N * N;
+  for (int idx = threadIdx.x; idx < N * TK; idx += T) {
+    const int n = idx / TK, b = idx % TK;
+    const float2 v = spec[plane + (size_t)n * N + ky0 + b];
+    D[idx] = cplx{v.x, v.y};
+  }
+  __syncthreads();
+  cgfft::fft_lines<N, TK, T, 1, TK, false, -1>(D, twN);
+  float2* gout[3] = {g0, g1, g2};
+#pragma unroll 1
+  for (int a = 0; a < 3; a++) {
+    for (int idx = threadIdx.x; idx < N * TK; idx += T) {
+      const int n = idx / TK, b = idx % TK;
+      const int ky = ky0 + b;
+      const int I0 = n <= N / 2 ? n : n - N;
+      const int J0 = ky <= N / 2 ? ky : ky - N;
+      const int den = kz * kz + I0 * I0 + J0 * J0;
+      cplx out = {0.0f, 0.0f};
+      if (den != 0) {
+        const float di = a == 0 ? (float)I0 : (a == 1 ? (float)J0 : (float)kz);
+        const float f2 = __fmul_rn(__fdiv_rn(f1, (float)den), di);
+        const cplx p = D[idx];
+        out = cplx{-__fmul_rn(f2, p.y), __fmul_rn(f2, p.x)};
+      }
+      W[idx] = out;
+    }
+    __syncthreads();
+    cgfft::fft_lines<N, TK, T, 1, TK, false, 1>(W, twN);
+    float2* go = gout[a];
+    for (int idx = threadIdx.x; idx < N * TK; idx += T) {
+      const int n = idx / TK, b = idx % TK;
+      go[plane + (size_t)n * N + ky0 + b] = make_float2(W[idx].x, W[idx].y);
+    }
+    __syncthreads();
+  }
+}
+
+// ------------------------------------- FX plain: c2c along kx, in place
+template <int N, int DIR>
+__global__ void __launch_bounds__(T) k_fx_plain(float2* __restrict__ spec,
+                                                const float2* __restrict__ twN) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  cplx* D = reinterpret_cast<cplx*>(smraw);
+  const int kz = blockIdx.y;
+  const int ky0 = blockIdx.x * TK;
+  const size_t plane = (size_t)kz * N * N;
+  for (int idx = threadIdx.x; idx < N * TK; idx += T) {
+    const int n = idx / TK, b = idx % TK;
+    const float2 v = spec[plane + (size_t)n * N + ky0 + b];
+    D[idx] = cplx{v.x, v.y};
+  }
+  __syncthreads();
+  cgfft::fft_lines<N, TK, T, 1, TK, false, DIR>(D, twN);
+  for (int idx = threadIdx.x; idx < N * TK; idx += T) {
+    const int n = idx / TK, b = idx % TK;
+    spec[plane + (size_t)n * N + ky0 + b] = make_float2(D[idx].x, D[idx].y);
+  }
+}
+
+// ------------------------------------------------------------ ZI: c2r z
+// One CTA: lines (x, y0..y0+TY-1).  Half-complex convention (the FFTW c2r
+// the reference relies on): Im X_0 and Im X_{N/2} are ignored.
+//   Z_k = (X_k + conj X_{H-k}) + i W_N^{-k} (X_k - conj X_{H-k}),  k < H
+//   z = IDFT_H(Z),  x_2m = Re z_m,  x_2m+1 = Im z_m   (unnormalised)
+template <int N>
+__global__ void __launch_bounds__(T) k_zi_c2r(const float2* __restrict__ gsp,
+                                              float* __restrict__ out,
+                                              const float2* __restrict__ twH,
+                                              const float2* __restrict__ twN) {
+  constexpr int H = N / 2;
+  constexpr int SB = H + 1;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  cplx* sm = reinterpret_cast<cplx*>(smraw);
+  const int x = blockIdx.y;
+  const int y0 = blockIdx.x * TY;
+  for (int idx = threadIdx.x; idx < (H + 1) * TY; idx += T) {
+    const int b = idx % TY, k = idx / TY;
+    const float2 v = gsp[((size_t)k * N + x) * N + y0 + b];
+    sm[b * SB + k] = cplx{v.x, v.y};
+  }
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < (H / 2 + 1) * TY; idx += T) {
+    const int b = idx % TY, k = idx / TY;
+    cplx* L = sm + b * SB;
+    if (k == 0) {
+      const float x0 = L[0].x, xh = L[H].x;
+      L[0] = cplx{x0 + xh, x0 - xh};
+    } else {
+      const int k2 = H - k;
+      const cplx a = L[k], c = L[k2];
+      const float2 wa = __ldg(twN + k), wc = __ldg(twN + k2);
+      // i * conj(w) * d  with conj(w) = (w.x, -w.y)
+      const cplx sa = {a.x + c.x, a.y - c.y}, da = {a.x - c.x, a.y + c.y};
+      const cplx ra = {da.x * wa.x + da.y * wa.y, da.y * wa.x - da.x * wa.y};  // conj(w)*d
+      const cplx za = {sa.x - ra.y, sa.y + ra.x};                            // + i*ra
+      const cplx sc = {c.x + a.x, c.y - a.y}, dc = {c.x - a.x, c.y + a.y};
+      const cplx rc = {dc.x * wc.x + dc.y * wc.y, dc.y * wc.x - dc.x * wc.y};
+      const cplx zc = {sc.x - rc.y, sc.y + rc.x};
+      L[k] = za;
+      if (k2 != k) L[k2] = zc;
+    }
+  }
+  __syncthreads();
+  cgfft::fft_lines<H, TY, T, SB, 1, true, 1>(sm, twH);
+  float2* dst = reinterpret_cast<float2*>(out + ((size_t)x * N + y0) * N);
+  for (int idx = threadIdx.x; idx < TY * H; idx += T) {
+    const int b = idx / H, m = idx - (idx / H) * H;
+    const cplx v = sm[b * SB + m];
+    dst[idx] = make_float2(v.x, v.y);
+  }
+}
+
+// ------------------------------------------------------- dispatch table
+struct MeshKernels {
+  void (*fz)(const float*, float2*, const float2*, const float2*, double*);
+  void (*fyf)(float2*, const float2*);
+  void (*fyi)(float2*, const float2*);
+  void (*fx)(const float2*, float2*, float2*, float2*, const float2*, float);
+  void (*zi)(const float2*, float*, const float2*, const float2*);
+  void (*fxpf)(float2*, const float2*);
+  void (*fxpi)(float2*, const float2*);
+  size_t sm_fz, sm_fy, sm_fx, sm_zi, sm_fxp;
+};
+
+template <int N>
+MeshKernels make_kernels() {
+  MeshKernels k;
+  k.fz = k_fz_r2c<N>;
+  k.fyf = k_fy<N, -1>;
+  k.fyi = k_fy<N, 1>;
+  k.fx = k_fx_green<N>;
+  k.zi = k_zi_c2r<N>;
+  k.fxpf = k_fx_plain<N, -1>;
+  k.fxpi = k_fx_plain<N, 1>;
+  k.sm_fxp = sizeof(cplx) * N * TK;
+  k.sm_fz = sizeof(cplx) * TY * (N / 2 + 1);
+  k.sm_fy = sizeof(cplx) * BY * N;
+  k.sm_fx = sizeof(cplx) * 2 * N * TK;
+  k.sm_zi = sizeof(cplx) * TY * (N / 2 + 1);
+  return k;
+}
+
+#define CG_MESH_SIZES(X) X(16) X(32) X(48) X(64) X(96) X(128) X(192) X(256) X(384) X(512) X(768) X(1024)
+
+bool get_kernels(int N, MeshKernels* out) {
+  switch (N) {
+#define CG_CASE(n) case n: *out = make_kernels<n>(); return true;
+    CG_MESH_SIZES(CG_CASE)
+#undef CG_CASE
+    default: return false;
+  }
+}
+
+cudaError_t set_smem(const void* fn, size_t bytes) {
+  return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+void twiddle_table(float2* h, int L) {
+  for (int k = 0; k < L; k++) {
+    const double a = -2.0 * 3.14159265358979323846264338327950288 * (double)k / (double)L;
+    h[k] = make_float2((float)cos(a), (float)sin(a));
+  }
+}
+
+int grid_for(long long n) {
+  long long b = (n + T - 1) / T;
+  const long long cap = 148LL * 16;   // 16 resident CTAs of 256 threads per SM
+  if (b > cap) b = cap;
+  if (b < 1) b = 1;
+  return (int)b;
+}
+
+}  // namespace
+
+bool pm_supported_mesh(int N) {
+  MeshKernels k;
+  return get_kernels(N, &k);
+}
+
+cudaError_t pm_plan_alloc(PmPlan* p, int N, int factor, float L) {
+  memset(p, 0, sizeof(*p));
+  MeshKernels k;
+  if (!get_kernels(N, &k)) return cudaErrorInvalidValue;
+  p->N = N;
+  p->factor = factor;
+  p->L = L;
+  // float constants exactly as the reference forms them
+  p->scale = (float)N / L;                                        // pm.c:215
+  p->wpar = (float)pow((double)factor, 3.0);                      // pm.c:216
+  {
+    const float sc = (float)(2.0 * 3.1415926535897932384626433832795 / (double)L);  // pm.c:315
+    p->f1 = (float)(-1.0 / pow((double)N, 3.0) / (double)sc);                        // pm.c:317
+  }
+  {
+    const float eps = L / (float)N;                               // pm.c:422
+    p->x_right = L / (float)N * (float)N - eps;                   // pm.c:423
+    p->shiftx = -L;                                               // pm.c:434
+  }
+  const size_t nh = (size_t)(N / 2 + 1);
+  p->mesh_bytes = sizeof(float) * (size_t)N * N * N;
+  p->spec_bytes = sizeof(float2) * nh * N * N;
+  cudaError_t e;
+#define CG_TRY(x) do { e = (x); if (e != cudaSuccess) { pm_plan_free(p); return e; } } while (0)
+  CG_TRY(cudaMalloc(&p->dens, p->mesh_bytes));
+  CG_TRY(cudaMalloc(&p->spec, p->spec_bytes));
+  for (int a = 0; a < 3; a++) {
+    CG_TRY(cudaMalloc(&p->gsp[a], p->spec_bytes));
+    CG_TRY(cudaMalloc(&p->fmesh[a], p->mesh_bytes));
+  }
+  CG_TRY(cudaMalloc(&p->twN, sizeof(float2) * N));
+  CG_TRY(cudaMalloc(&p->twH, sizeof(float2) * (N / 2)));
+  CG_TRY(cudaMalloc(&p->dsum, sizeof(double)));
+  CG_TRY(cudaMalloc(&p->err, sizeof(unsigned)));
+  {
+    float2* h = (float2*)malloc(sizeof(float2) * N);
+    twiddle_table(h, N);
+    CG_TRY(cudaMemcpy(p->twN, h, sizeof(float2) * N, cudaMemcpyHostToDevice));
+    twiddle_table(h, N / 2);
+    CG_TRY(cudaMemcpy(p->twH, h, sizeof(float2) * (N / 2), cudaMemcpyHostToDevice));
+    free(h);
+  }
+  CG_TRY(cudaMemset(p->dsum, 0, sizeof(double)));
+  CG_TRY(cudaMemset(p->err, 0, sizeof(unsigned)));
+  CG_TRY(set_smem((const void*)k.fz, k.sm_fz));
+  CG_TRY(set_smem((const void*)k.fyf, k.sm_fy));
+  CG_TRY(set_smem((const void*)k.fyi, k.sm_fy));
+  CG_TRY(set_smem((const void*)k.fx, k.sm_fx));
+  CG_TRY(set_smem((const void*)k.zi, k.sm_zi));
+  CG_TRY(set_smem((const void*)k.fxpf, k.sm_fxp));
+  CG_TRY(set_smem((const void*)k.fxpi, k.sm_fxp));
+#undef CG_TRY
+  return cudaSuccess;
+}
+
+cudaError_t mesh_fft_alloc(MeshFFT* f, int N) {
+  memset(f, 0, sizeof(*f));
+  MeshKernels k;
+  if (!get_kernels(N, &k)) return cudaErrorInvalidValue;
+  f->N = N;
+  cudaError_t e = cudaMalloc(&f->twN, sizeof(float2) * N);
+  if (e == cudaSuccess) e = cudaMalloc(&f->twH, sizeof(float2) * (N / 2));
+  if (e == cudaSuccess) e = cudaMalloc(&f->dsum, sizeof(double));
+  if (e == cudaSuccess) {
+    float2* h = (float2*)malloc(sizeof(float2) * N);
+    twiddle_table(h, N);
+    e = cudaMemcpy(f->twN, h, sizeof(float2) * N, cudaMemcpyHostToDevice);
+    twiddle_table(h, N / 2);
+    if (e == cudaSuccess) e = cudaMemcpy(f->twH, h, sizeof(float2) * (N / 2), cudaMemcpyHostToDevice);
+    free(h);
+  }
+  if (e == cudaSuccess) e = set_smem((const void*)k.fz, k.sm_fz);
+  if (e == cudaSuccess) e = set_smem((const void*)k.fyf, k.sm_fy);
+  if (e == cudaSuccess) e = set_smem((const void*)k.fyi, k.sm_fy);
+  if (e == cudaSuccess) e = set_smem((const void*)k.zi, k.sm_zi);
+  if (e == cudaSuccess) e = set_smem((const void*)k.fxpf, k.sm_fxp);
+  if (e == cudaSuccess) e = set_smem((const void*)k.fxpi, k.sm_fxp);
+  if (e != cudaSuccess) mesh_fft_free(f);
+  return e;
+}
+
+void mesh_fft_free(MeshFFT* f) {
+  cudaFree(f->twN);
+  cudaFree(f->twH);
+  cudaFree(f->dsum);
+  memset(f, 0, sizeof(*f));
+}
+
+cudaError_t mesh_r2c(const MeshFFT* f, const float* real, float2* spec, cudaStream_t st) {
+  MeshKernels k;
+  if (!get_kernels(f->N, &k)) return cudaErrorInvalidValue;
+  const int N = f->N;
+  prof_mark(st, CG_ST_FZ);
+  k.fz<<<dim3(N / TY, N), T, k.sm_fz, st>>>(real, spec, f->twH, f->twN, f->dsum);
+  prof_mark(st, CG_ST_FY_FWD);
+  k.fyf<<<(N / 2 + 1) * N / BY, T, k.sm_fy, st>>>(spec, f->twN);
+  prof_mark(st, CG_ST_OTHER);
+  k.fxpf<<<dim3(N / TK, N / 2 + 1), T, k.sm_fxp, st>>>(spec, f->twN);
+  return cudaGetLastError();
+}
+
+cudaError_t mesh_c2r(const MeshFFT* f, float2* spec, float* real, cudaStream_t st) {
+  MeshKernels k;
+  if (!get_kernels(f->N, &k)) return cudaErrorInvalidValue;
+  const int N = f->N;
+  prof_mark(st, CG_ST_OTHER);
+  k.fxpi<<<dim3(N / TK, N / 2 + 1), T, k.sm_fxp, st>>>(spec, f->twN);
+  prof_mark(st, CG_ST_FY_INV);
+  k.fyi<<<(N / 2 + 1) * N / BY, T, k.sm_fy, st>>>(spec, f->twN);
+  prof_mark(st, CG_ST_ZI);
+  k.zi<<<dim3(N / TY, N), T, k.sm_zi, st>>>(spec, real, f->twH, f->twN);
+  return cudaGetLastError();
+}
+
+void pm_plan_free(PmPlan* p) {
+  cudaFree(p->dens);
+  cudaFree(p->spec);
+  for (int a = 0; a < 3; a++) {
+    cudaFree(p->gsp[a]);
+    cudaFree(p->fmesh[a]);
+  }
+  cudaFree(p->twN);
+  cudaFree(p->twH);
+  cudaFree(p->dsum);
+  cudaFree(p->err);
+  memset(p, 0, sizeof(*p));
+}
+
+cudaError_t pm_deposit(PmPlan* p, const float* const x[3], long long n, cudaStream_t st) {
+  const size_t n4 = (size_t)p->N * p->N * p->N / 4;
+  prof_mark(st, CG_ST_FILL);
+  k_fill<<<grid_for((long long)n4), T, 0, st>>>(reinterpret_cast<float4*>(p->dens), n4, -1.0f);
+  if (n > 0)
+    prof_mark(st, CG_ST_DEPOSIT);
+    k_deposit<<<grid_for(n), T, 0, st>>>(x[0], x[1], x[2], n, p->dens, p->N, p->scale,
+                                         p->wpar, p->x_right, p->shiftx, p->err);
+  return cudaGetLastError();
+}
+
+cudaError_t pm_r2c(PmPlan* p, cudaStream_t st) {
+  MeshKernels k;
+  get_kernels(p->N, &k);
+  const int N = p->N;
+  cudaMemsetAsync(p->dsum, 0, sizeof(double), st);
+  prof_mark(st, CG_ST_FZ);
+  k.fz<<<dim3(N / TY, N), T, k.sm_fz, st>>>(p->dens, p->spec, p->twH, p->twN, p->dsum);
+  prof_mark(st, CG_ST_FY_FWD);
+  k.fyf<<<(N / 2 + 1) * N / BY, T, k.sm_fy, st>>>(p->spec, p->twN);
+  return cudaGetLastError();
+}
+
+cudaError_t pm_green_c2r(PmPlan* p, cudaStream_t st) {
+  MeshKernels k;
+  get_kernels(p->N, &k);
+  const int N = p->N;
+  prof_mark(st, CG_ST_FX_GREEN);
+  k.fx<<<dim3(N / TK, N / 2 + 1), T, k.sm_fx, st>>>(p->spec, p->gsp[0], p->gsp[1], p->gsp[2],
+                                                     p->twN, p->f1);
+  for (int a = 0; a < 3; a++) {
+    prof_mark(st, CG_ST_FY_INV);
+    k.fyi<<<(N / 2 + 1) * N / BY, T, k.sm_fy, st>>>(p->gsp[a], p->twN);
+    prof_mark(st, CG_ST_ZI);
+    k.zi<<<dim3(N / TY, N), T, k.sm_zi, st>>>(p->gsp[a], p->fmesh[a], p->twH, p->twN);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t pm_interp(PmPlan* p, const float* const x[3], long long n, float* const f[3],
+                      cudaStream_t st) {
+  if (n > 0)
+    prof_mark(st, CG_ST_INTERP);
+    k_interp<<<grid_for(n), T, 0, st>>>(x[0], x[1], x[2], n, p->fmesh[0], p->fmesh[1],
+                                        p->fmesh[2], f[0], f[1], f[2], p->N, p->scale,
+                                        p->x_right, p->shiftx);
+  return cudaGetLastError();
+}
+
+cudaError_t pm_forces(PmPlan* p, const float* const x[3], long long n, float* const f[3],
+                      cudaStream_t st) {
+  cudaError_t e;
+  if ((e = pm_deposit(p, x, n, st)) != cudaSuccess) return e;
+  if ((e = pm_r2c(p, st)) != cudaSuccess) return e;
+  if ((e = pm_green_c2r(p, st)) != cudaSuccess) return e;
+  return pm_interp(p, x, n, f, st);
+}

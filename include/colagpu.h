@@ -1,0 +1,134 @@
+/*
+ * libcolagpu -- B200 particle-mesh force, COLA time step and 2LPT setup for
+ * cola_halo, behind a plain C ABI.
+ *
+ * Two layers:
+ *
+ *   1. Drop-in entry points with the reference's own names and signatures
+ *      (declared in colagpu_dropin.h).  A caller built against the
+ *      reference's pm.h / cola.h / lpt.h / power.h / move.h links this
+ *      library instead of pm.o cola.o lpt.o power.o move.o.
+ *
+ *   2. The handle API below (cg_*): one cg_sim holds the device particle
+ *      state (structure of arrays) and the PM mesh plan of one realization,
+ *      so a process can run several meshes or realizations at once.
+ *
+ * All cg_* functions return 0 on success and a negative CG_E* code on
+ * failure; cg_last_error() describes the last failure of the calling thread.
+ * Work is queued on the handle's own CUDA stream: functions that hand data
+ * back to host memory synchronise that stream, the others return as soon as
+ * the work is queued.
+ *
+ * Particle layouts exchanged with the host are the reference's
+ * (particle.h:6-48): Particle (56 B: x, dx1, dx2, v, id) and ParticleMinimum
+ * (32 B: x, v, id).
+ */
+#ifndef COLAGPU_H
+#define COLAGPU_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CG_OK 0
+#define CG_EINVAL (-1)      /* bad argument */
+#define CG_ECUDA (-2)       /* CUDA runtime error (message has the details) */
+#define CG_ENOMEM (-3)      /* device or pinned-host allocation failed */
+#define CG_EDENSITY (-4)    /* CIC density sum check failed (pm.c:548-553) */
+#define CG_EPARTICLE (-5)   /* a particle position was non-finite or below 0 */
+#define CG_EUNSUPPORTED (-6)/* mesh size not built into this library */
+#define CG_EFILE (-7)       /* input file unreadable */
+
+typedef struct cg_sim cg_sim;
+
+/* Library / error information. */
+const char* cg_last_error(void);
+int cg_version(void);
+/* 1 if mesh size n (cells per dimension) is supported: n in
+ * {32, 48, 64, 96, 128, 192, 256, 384, 512, 768, 1024}. */
+int cg_mesh_supported(int n);
+/* Number of visible CUDA devices (0 when there is none or no driver). */
+int cg_device_count(void);
+/* Make device `dev` current for the calling host thread (one process per
+ * GPU: call once before any other cg_* / drop-in call). */
+int cg_set_device(int dev);
+
+/* Pinned host memory for fast host<->device particle transfers. */
+void* cg_host_alloc(size_t bytes);
+void cg_host_free(void* p);
+
+/* Create a realization: nc^3 particles capacity np_capacity (>= nc^3),
+ * PM mesh of ngrid^3 cells (ngrid = factor * nc), periodic box boxsize.
+ * Replaces pm_init (pm.c:87-198) for one handle. */
+int cg_sim_create(cg_sim** out, int nc, int ngrid, float boxsize, double omega_m,
+                  long long np_capacity);
+void cg_sim_destroy(cg_sim* s);
+
+/* Load particles from a host (or device) array of reference Particle
+ * structs; a_x / a_v are the position and velocity scale factors
+ * (particle.h:18). */
+int cg_sim_set_particles(cg_sim* s, const void* particles, long long np, float a_x, float a_v);
+/* Copy the state back into a host array of reference Particle structs. */
+int cg_sim_get_particles(cg_sim* s, void* particles);
+/* Copy the last computed forces (np x 3 floats, particle order) to host. */
+int cg_sim_get_forces(cg_sim* s, float* f);
+int cg_sim_get_times(cg_sim* s, float* a_x, float* a_v);
+long long cg_sim_np(cg_sim* s);
+
+/* move_particles2 on one GPU (move.c:34-41): periodic wrap of x, y, z. */
+int cg_sim_move(cg_sim* s);
+/* pm_calculate_forces (pm.c:565-596).  If density_sum is non-NULL the
+ * stream is synchronised and the mesh sum (check_total_density) returned. */
+int cg_sim_forces(cg_sim* s, double* density_sum);
+/* cola_kick (cola.c:73-117) / cola_drift (cola.c:119-153) with the time
+ * coefficients computed on the host in double precision. */
+int cg_sim_kick(cg_sim* s, float avel1);
+int cg_sim_drift(cg_sim* s, float apos1);
+/* The same updates with caller-supplied single-precision coefficients
+ * (dda, q1, q2) / (dyyy, da1, da2); they do not change a_x / a_v. */
+int cg_sim_kick_coeffs(cg_sim* s, float dda, float q1, float q2);
+int cg_sim_drift_coeffs(cg_sim* s, float dyyy, float da1, float da2);
+/* cola_set_snapshot (cola.c:341-416) into a host ParticleMinimum array. */
+int cg_sim_snapshot(cg_sim* s, double aout, float omega_m, void* pmin_out);
+/* Wait for all queued work of the handle; reports device-side errors. */
+int cg_sim_sync(cg_sim* s);
+/* Copy one mesh to host: which = 0 density (delta), 1..3 force x, y, z;
+ * ngrid^3 floats, [x][y][z] order. */
+int cg_sim_get_mesh(cg_sim* s, int which, float* out);
+/* The CUDA stream (cudaStream_t) the handle queues its work on. */
+void* cg_sim_stream(cg_sim* s);
+
+/* Unnormalised 3-D real transforms of host arrays on the device, FFTW sign
+ * convention (replaces the fftwf_mpi r2c / c2r plans of pm.c:141-147 and
+ * lpt.c:118-134 for one process).  real: n^3 floats [x][y][z]; spec:
+ * n*n*(n/2+1) interleaved complex [x][y][kz].  The c2r is c2c over x and y
+ * followed by a c2r over z that ignores Im of kz = 0 and kz = n/2, as
+ * FFTW's c2r does.  Synchronous; allocates its own scratch. */
+int cg_fft_r2c(int n, const float* real_in, float* spec_out);
+int cg_fft_c2r(int n, const float* spec_in, float* real_out);
+
+/* Kernel accounting (no reference counterpart; the reference's wall-clock
+ * timers are timer.c).  cg_launch_count: kernels launched by this library
+ * since load.  cg_prof_begin / cg_prof_end bracket a region: every launch in
+ * between records a CUDA event; cg_prof_end synchronises, and fills
+ * ms[stage] (device time) and counts[stage] (launches) for nstages stages
+ * named by cg_stage_name(stage).  Returns the number of launches timed. */
+long long cg_launch_count(void);
+const char* cg_stage_name(int stage);
+int cg_prof_begin(int max_marks);
+int cg_prof_end(double* ms, int* counts, int nstages);
+
+/* Host time coefficients (double-precision restatement of cola.c:156-292). */
+double cg_growth_D1(double omega_m, double a);
+double cg_growth_D2(double omega_m, double a);
+double cg_cola_Sq(double omega_m, double ai, double af, double aref);
+double cg_cola_Sphi(double omega_m, double ai, double af, double aref);
+void cg_kick_coeffs(double omega_m, float a_v, float a_x, float avel1, float out3[3]);
+void cg_drift_coeffs(double omega_m, float a_x, float a_v, float apos1, float out3[3]);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,122 @@
+/*
+ * Drop-in replacements for the cola_halo hot-path entry points.
+ *
+ * Each function has the name, signature and argument meaning of the
+ * reference function it replaces (cited below), so the reference's driver
+ * (main.c) links against libcolagpu instead of pm.o, cola.o, lpt.o, power.o
+ * and move.o.  The data types are the reference's (particle.h:6-48).
+ *
+ * Errors: like the reference (msg_abort -> MPI_Abort, msg.c:36-45) a failure
+ * prints a message and exits the process with the reference's error code
+ * (4001 mesh allocation, 6040 density check, 3000 power table, 3010 sigma8),
+ * unless cg_dropin_set_abort(0) was called, in which case the call returns
+ * and cg_last_error() describes the failure.
+ *
+ * Particle residency: the first call that sees a Particles object uploads its
+ * particles to the GPU; from then on the device copy is the working state and
+ * the host array p[] is not read again.  cola_set_snapshot writes its result
+ * to the host Snapshot as the reference does.  A caller that changes p[]
+ * itself calls cg_particles_upload(); one that wants p[] / force[] on the
+ * host calls cg_particles_download().  With cg_dropin_set_sync(1) every call
+ * instead reads its inputs from, and writes its outputs to, the host arrays
+ * (the reference's exact memory behaviour, at PCIe cost).
+ */
+#ifndef COLAGPU_DROPIN_H
+#define COLAGPU_DROPIN_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* particle.h:6-48.  The reference's `typedef float float3[3]` is kept for C
+ * callers; CUDA's own float3 vector type has the same name, so inside a CUDA
+ * translation unit the force member is spelled float (*)[3] (same ABI). */
+#if !defined(__CUDACC__) && !defined(__VECTOR_TYPES_H__)
+typedef float float3[3];
+#endif
+
+typedef struct {
+  float x[3];
+  float dx1[3]; /* ZA displacement */
+  float dx2[3]; /* 2LPT displacement */
+  float v[3];   /* velocity */
+  long long id;
+} Particle;
+
+typedef struct {
+  Particle* p;
+  float (*force)[3];
+  float a_x, a_v;
+  int np_local, np_allocated;
+  long long np_total;
+  float np_average;
+} Particles;
+
+typedef struct {
+  float x[3];
+  float v[3];
+  long long id;
+} ParticleMinimum;
+
+typedef struct {
+  ParticleMinimum* p;
+  int np_local;
+  int np_allocated;
+  long long np_total;
+  float np_average;
+  float a;
+  float boxsize;
+  int nc;
+  float omega_m, h;
+  int seed;
+  char* filename;
+} Snapshot;
+
+/* pm.h:6-9 (pm.c:87-198).  mem1 / mem2 are accepted and not used: the
+ * meshes live in device memory. */
+void pm_init(const int nc_pm, const int nc_pm_factor, const float boxsize,
+             const float np_alloc_factor, void* const mem1, const size_t size1,
+             void* const mem2, const size_t size2);
+/* pm.h:11 (pm.c:565-596) */
+void pm_calculate_forces(Particles* particles);
+/* cola.h:7-8 (cola.c:73-117) */
+void cola_kick(Particles* const particles, const float Omega_m, const float avel1);
+/* cola.h:9-10 (cola.c:119-153) */
+void cola_drift(Particles* const particles, const float Omega_m, const float apos1);
+/* cola.h:18 (cola.c:341-416) */
+void cola_set_snapshot(const double aout, Particles const* const particles,
+                       Snapshot* const snapshot);
+/* move.h:7 (move.c:15-98); one process: the periodic wrap (move.c:34-41). */
+void move_particles2(Particles* const particles, const float BoxSize, void* const buf,
+                     const size_t size);
+/* lpt.h:6 (lpt.c:46-143).  mem / size are accepted and not used. */
+void lpt_init(const int nc, const void* mem, const size_t size);
+/* lpt.h:7 (lpt.c:145-578).  Declared void in lpt.h but defined int in
+ * lpt.c (returns 0); exported as int. */
+int lpt_set_displacement(const double InitTime, const double omega_m, const int Seed,
+                         const double Box, Particles* particles);
+/* lpt.h:8 (lpt.c:611-614) */
+int lpt_get_local_nx(void);
+/* power.h:5 (power.c:36-60) */
+void power_init(const char filename[], const double a_init, const double sigma8,
+                const double omega_m, const double omega_lambda);
+/* power.h:4 (power.c:120-151) */
+double PowerSpec(const double k);
+/* power.h:6 (power.c:199-202) */
+double GrowthFactor(double astart, double aend);
+
+/* Residency and error controls of the drop-in layer (no reference
+ * counterpart). */
+int cg_particles_upload(Particles* particles);
+int cg_particles_download(Particles* particles);
+void cg_dropin_set_sync(int full);
+void cg_dropin_set_abort(int abort_on_error);
+/* Release every device buffer of the drop-in layer. */
+void cg_dropin_finalize(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,76 @@
+"""PM force (deposit -> r2c -> Green/gradient -> c2r -> interpolation) on the
+GPU vs the oracle restatement of pm.c on the same particles."""
+import numpy as np
+import pytest
+
+from oracle import restate as R
+from tests.helpers import lattice_particles
+
+pytestmark = pytest.mark.gpu
+
+OM = 0.273
+
+
+@pytest.mark.parametrize("nc,factor,L", [(16, 3, 100.0), (32, 3, 200.0), (16, 2, 64.0),
+                                         (32, 1, 300.0)])
+def test_forces_match_oracle(gpu_lib, bbks_table, nc, factor, L):
+    from cola_halo_b200 import Simulation
+    N = nc * factor
+    p = lattice_particles(nc, L, 100 + nc, OM, 0.1, bbks_table)
+    sim = Simulation(nc, N, L, OM)
+    sim.set_particles(p, 0.1, 0.1)
+    sim.move()
+    dsum = sim.forces(check_density=True)
+    f = sim.get_forces()
+    x = R.wrap(p["x"], L)
+    fo, dens = R.pm_calculate_forces(x, N, L, factor)
+    # density mesh
+    d = sim.get_mesh(0)
+    assert np.abs(d - dens).max() < 2e-5 * max(1.0, np.abs(dens).max())
+    s, tol, ok = R.check_total_density(d.astype(np.float64), factor, nc ** 3)
+    assert ok and abs(dsum - s) < 1e-6 * nc ** 3
+    # force meshes vs the oracle's float64 meshes
+    _, _, meshes = R.pm_force_meshes(x, N, L, factor)
+    for a in range(3):
+        m = sim.get_mesh(1 + a)
+        assert np.abs(m - meshes[a]).max() < 2e-5 * np.abs(meshes[a]).max()
+    # particle forces
+    scale = np.abs(fo).max()
+    assert np.abs(f - fo).max() < 2e-5 * scale
+    assert np.sqrt(np.mean((f - fo) ** 2)) < 2e-6 * scale
+
+
+def test_interp_bit_exact_given_mesh(gpu_lib, bbks_table):
+    """With the device's own force meshes, the CIC gather (pm.c:370-411 plus
+    the buffer copy) is reproduced bit for bit by the restatement."""
+    from cola_halo_b200 import Simulation
+    nc, factor, L = 16, 3, 100.0
+    N = nc * factor
+    p = lattice_particles(nc, L, 5, OM, 0.1, bbks_table)
+    sim = Simulation(nc, N, L, OM)
+    sim.set_particles(p, 0.1, 0.1)
+    sim.move()
+    sim.forces()
+    f = sim.get_forces()
+    x = sim.get_particles()["x"]
+    for a in range(3):
+        fo = R.cic_interp(x, sim.get_mesh(1 + a), N, L)
+        np.testing.assert_array_equal(f[:, a], fo)
+
+
+def test_single_particle_mass(gpu_lib):
+    """One particle deposits factor^3 in total (pm.c:216,264-275), also when
+    it sits in the last x cell and acts through its buffer copy."""
+    from cola_halo_b200 import Simulation
+    nc, factor, L = 16, 3, 48.0
+    N = nc * factor
+    sim = Simulation(nc, N, L, OM, np_capacity=nc ** 3)
+    for xyz in ([10.3, 20.7, 5.5], [47.6, 0.2, 47.9], [0.0, 47.99, 13.0]):
+        p = np.zeros(1, dtype=__import__("cola_halo_b200").PARTICLE_DTYPE)
+        p["x"] = xyz
+        sim.set_particles(p, 0.1, 0.1)
+        sim.forces()
+        d = sim.get_mesh(0).astype(np.float64)
+        assert abs((d + 1.0).sum() - factor ** 3) < 1e-4
+        want = R.cic_deposit(np.array([xyz], dtype=np.float32), N, L, factor)
+        assert np.abs(d - want).max() < 1e-6

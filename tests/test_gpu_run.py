@@ -1,0 +1,97 @@
+"""Whole realizations: the reference time loop (main.c:117-206) on the GPU,
+fed the reference's own 2LPT output, vs the shim-built reference (pm.c,
+cola.c, move.c run on the CPU) -- positions within 1e-5 of the box."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from cola_halo_b200.schedule import Schedule, output_scale_factors, run_time_loop
+from cola_halo_b200.types import HostParticles, HostSnapshot
+from tests.helpers import periodic_diff
+
+pytestmark = pytest.mark.gpu
+
+OM = 0.273
+
+
+def reference_run(ref, table, nc, factor, L, seed, sched, zout=(0.0,)):
+    """Run the reference's own code; returns (2LPT particles, snapshots)."""
+    ref.power_init(table.encode(), sched.a_init, 0.81, OM, 1 - OM)
+    ref.comm_init(nc * factor, nc, L)
+    ref.lpt_init(nc, None, 0)
+    parts = HostParticles(nc)
+    ref.lpt_set_displacement(sched.a_init, OM, seed, L, parts.ptr)
+    ics = parts.local().copy()
+    ref.pm_init(nc * factor, factor, L, 1.25, None, 0, None, 0)
+    snap = HostSnapshot(nc, parts.struct.np_allocated, L, OM)
+    parts.struct.a_v = sched.a_init                       # main.c:145
+    snaps = []
+
+    def take(a, i):
+        ref.cola_set_snapshot(a, parts.ptr, snap.ptr)
+        snaps.append((a, snap.local().copy()))
+    run_time_loop(sched, output_scale_factors(zout),
+                  move=lambda: ref.move_particles2(parts.ptr, L, None, 0),
+                  force=lambda: ref.pm_calculate_forces(parts.ptr),
+                  kick=lambda a: ref.cola_kick(parts.ptr, OM, a),
+                  drift=lambda a: ref.cola_drift(parts.ptr, OM, a),
+                  snapshot=take)
+    return ics, snaps
+
+
+@pytest.mark.parametrize("nc,factor,L,sched", [
+    (16, 3, 100.0, Schedule.reference(10)),
+    (32, 3, 200.0, Schedule.reference(10)),
+    (32, 3, 200.0, Schedule.linear(0.02, 1.0, 10)),
+    (64, 3, 200.0, Schedule.reference(10)),
+])
+def test_handle_api_run_matches_reference(gpu_lib, ref, bbks_table, nc, factor, L, sched):
+    from cola_halo_b200 import Simulation
+    ics, snaps = reference_run(ref, bbks_table, nc, factor, L, 100, sched, zout=(0.5, 0.0))
+    sim = Simulation(nc, nc * factor, L, OM)
+    sim.set_particles(ics, sched.a_init, sched.a_init)
+    got = sim.run(sched, zout=(0.5, 0.0), check_density=True)
+    assert len(got) == len(snaps) == 2
+    for (a_r, s_r), (a_g, s_g) in zip(snaps, got):
+        assert a_r == a_g
+        dx = periodic_diff(s_g["x"], s_r["x"], L)
+        assert dx.max() <= 1e-5 * L, dx.max() / L
+        dv = np.abs(s_g["v"] - s_r["v"])
+        assert dv.max() <= 1e-3 * np.abs(s_r["v"]).max()
+        np.testing.assert_array_equal(s_g["id"], s_r["id"])
+
+
+def test_dropin_api_run_matches_reference(gpu_lib, ref, bbks_table):
+    """Same loop through the drop-in entry points on host Particles."""
+    nc, factor, L = 32, 3, 200.0
+    sched = Schedule.reference(10)
+    ics, snaps = reference_run(ref, bbks_table, nc, factor, L, 7, sched)
+    lib = gpu_lib
+    lib.cg_dropin_set_abort(0)
+    lib.pm_init(nc * factor, factor, L, 1.25, None, 0, None, 0)
+    parts = HostParticles(nc)
+    parts.p[: nc ** 3] = ics
+    parts.struct.np_local = nc ** 3
+    parts.struct.a_x = sched.a_init
+    parts.struct.a_v = sched.a_init
+    snap = HostSnapshot(nc, parts.struct.np_allocated, L, OM)
+    out = []
+
+    def take(a, i):
+        lib.cola_set_snapshot(a, parts.ptr, snap.ptr)
+        out.append(snap.local().copy())
+    run_time_loop(sched, output_scale_factors([0.0]),
+                  move=lambda: lib.move_particles2(parts.ptr, L, None, 0),
+                  force=lambda: lib.pm_calculate_forces(parts.ptr),
+                  kick=lambda a: lib.cola_kick(parts.ptr, OM, a),
+                  drift=lambda a: lib.cola_drift(parts.ptr, OM, a),
+                  snapshot=take)
+    assert lib.cg_last_error() in (b"", None) or out, lib.cg_last_error()
+    assert abs(parts.struct.a_x - 1.0) < 1e-6
+    dx = periodic_diff(out[-1]["x"], snaps[-1][1]["x"], L)
+    assert dx.max() <= 1e-5 * L
+    # host particle array refreshed on request
+    assert lib.cg_particles_download(parts.ptr) == 0
+    assert np.isfinite(parts.force[: nc ** 3]).all()
+    lib.cg_dropin_finalize()
