@@ -47,7 +47,15 @@ SIGNATURES = {
     "cg_sim_snapshot": (i32, [P, f64, f32, P]),
     "cg_sim_sync": (i32, [P]),
     "cg_sim_get_mesh": (i32, [P, i32, P]),
+    "cg_sim_power_spectrum": (i32, [P, i32, i32, P, P, P]),
     "cg_sim_stream": (P, [P]),
+    "cg_batch_create": (i32, [ctypes.POINTER(P), i32, P, f64, i32]),
+    "cg_batch_destroy": (None, [P]),
+    "cg_batch_set_particles": (i32, [P, i32, P, i64]),
+    "cg_batch_run": (i32, [P]),
+    "cg_batch_get_snapshot": (i32, [P, i32, P]),
+    "cg_batch_power_spectrum": (i32, [P, i32, P, P, P]),
+    "cg_batch_num_nodes": (i32, [P, ctypes.POINTER(sz)]),
     "cg_fft_r2c": (i32, [i32, P, P]),
     "cg_fft_c2r": (i32, [i32, P, P]),
     "cg_launch_count": (i64, []),

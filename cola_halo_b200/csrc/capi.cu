@@ -314,6 +314,38 @@ extern "C" int cg_sim_sync(cg_sim* s) {
   return check_err_word(s);
 }
 
+extern "C" int cg_sim_power_spectrum(cg_sim* s, int nbins, int flags, double* k, double* pk,
+                                     double* nmodes) {
+  if (!s || !k || !pk || nbins < 1 || nbins > s->pm.N)
+    return set_err(CG_EINVAL, "cg_sim_power_spectrum: bad arguments");
+  const float* x[3] = {s->ps.x[0], s->ps.x[1], s->ps.x[2]};
+  CG_CHECK(pm_power_spectrum(&s->pm, x, s->ps.n, nbins, flags & CG_PK_DECONVOLVE_CIC,
+                             s->pm.pk_acc, s->st),
+           "power spectrum");
+  double* h = (double*)malloc(sizeof(double) * 3 * nbins);
+  if (!h) return set_err(CG_ENOMEM, "host malloc");
+  cudaError_t e = cudaMemcpyAsync(h, s->pm.pk_acc, sizeof(double) * 3 * nbins,
+                                  cudaMemcpyDeviceToHost, s->st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
+  if (e != cudaSuccess) {
+    free(h);
+    return cuda_err(e, "power spectrum readback");
+  }
+  const double N = s->pm.N, L = s->L;
+  const double kf = 2.0 * M_PI / L;
+  const double norm = L * L * L / (N * N * N * N * N * N);
+  const double shot = (flags & CG_PK_SUBTRACT_SHOT) && s->ps.n > 0 ? L * L * L / (double)s->ps.n
+                                                                   : 0.0;
+  for (int b = 0; b < nbins; b++) {
+    const double w = h[b];
+    k[b] = w > 0 ? kf * h[nbins + b] / w : 0.0;
+    pk[b] = w > 0 ? norm * h[2 * nbins + b] / w - shot : 0.0;
+    if (nmodes) nmodes[b] = w;
+  }
+  free(h);
+  return CG_OK;
+}
+
 extern "C" int cg_sim_get_mesh(cg_sim* s, int which, float* out) {
   if (!s || !out || which < 0 || which > 3) return set_err(CG_EINVAL, "cg_sim_get_mesh: bad args");
   const float* src = which == 0 ? s->pm.dens : s->pm.fmesh[which - 1];
@@ -564,6 +596,11 @@ extern "C" void cola_kick(Particles* const particles, const float Omega_m, const
   const ColaTime& ct = times_for(Omega_m);
   float dda, q1, q2;
   ct.kick(particles->a_v, particles->a_x, avel1, &dda, &q1, &q2);
+  // the kick's -1.5 Omega_m factor (cola.c:105) takes this call's Omega_m
+  if (!g_drop.sim->ct || g_drop.sim->ct->om32 != Omega_m) {
+    g_drop.sim->omega_m = Omega_m;
+    g_drop.sim->ct.reset(new ColaTime(Omega_m));
+  }
   if (cg_sim_kick_coeffs(g_drop.sim, dda, q1, q2)) {
     dropin_fail(4001, "cola_kick: %s", cg_last_error());
     return;

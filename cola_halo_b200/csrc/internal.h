@@ -39,6 +39,7 @@ struct PmPlan {
   float2* twN;              // exp(-2 pi i k/N), k < N
   float2* twH;              // exp(-2 pi i k/(N/2)), k < N/2
   double* dsum;             // device: sum of the density mesh (check)
+  double* pk_acc;           // device: 3 N doubles of power-spectrum bin sums
   unsigned* err;            // device: error word
   size_t mesh_bytes;        // bytes of one real mesh
   size_t spec_bytes;        // bytes of one half spectrum
@@ -69,6 +70,10 @@ cudaError_t pm_forces(PmPlan* p, const float* const x[3], long long n,
 cudaError_t pm_deposit(PmPlan* p, const float* const x[3], long long n, cudaStream_t st);
 cudaError_t pm_r2c(PmPlan* p, cudaStream_t st);
 cudaError_t pm_green_c2r(PmPlan* p, cudaStream_t st);
+// Power spectrum of the CIC density of x: deposit, r2c, shell sums into
+// acc[3 * nbins] (device doubles: sum w, sum w |n|, sum w |delta_k|^2).
+cudaError_t pm_power_spectrum(PmPlan* p, const float* const x[3], long long n, int nbins,
+                              int deconv, double* acc, cudaStream_t st);
 cudaError_t pm_interp(PmPlan* p, const float* const x[3], long long n,
                       float* const f[3], cudaStream_t st);
 

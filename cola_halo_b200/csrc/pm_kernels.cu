@@ -365,6 +365,53 @@ __global__ void __launch_bounds__(T) k_zi_c2r(const float2* __restrict__ gsp,
   }
 }
 
+// ---------------------------------------------------- power spectrum bins
+// Shell average of |delta_k|^2 over the half spectrum S[kz][kx][ky]: bin b
+// holds modes with |n| in [b + 1/2, b + 3/2) (|n| in units of the
+// fundamental), weight 2 for 0 < kz < N/2 (each stands for itself and its
+// conjugate), 1 on the kz = 0 and kz = N/2 planes.  Optional division by the
+// CIC window prod_i sinc^2(pi n_i / N) squared.  acc = [sum w, sum w |n|,
+// sum w |S|^2] per bin, accumulated in double.
+__global__ void __launch_bounds__(T) k_pk_bin(const float2* __restrict__ spec, int N, int nbins,
+                                              int deconv, double* __restrict__ acc) {
+  extern __shared__ double sb[];
+  for (int i = threadIdx.x; i < 3 * nbins; i += T) sb[i] = 0.0;
+  __syncthreads();
+  const size_t total = (size_t)(N / 2 + 1) * N * N;
+  for (size_t t = (size_t)blockIdx.x * T + threadIdx.x; t < total; t += (size_t)gridDim.x * T) {
+    const int kz = (int)(t / ((size_t)N * N));
+    const int i = (int)((t / N) % N);
+    const int j = (int)(t % N);
+    const int si = i <= N / 2 ? i : i - N;
+    const int sj = j <= N / 2 ? j : j - N;
+    const double n2 = (double)si * si + (double)sj * sj + (double)kz * kz;
+    const double nm = sqrt(n2);
+    const int b = (int)floor(nm + 0.5) - 1;
+    if (b < 0 || b >= nbins) continue;
+    const double w = (kz == 0 || kz == N / 2) ? 1.0 : 2.0;
+    const float2 s = spec[t];
+    double p = (double)s.x * s.x + (double)s.y * s.y;
+    if (deconv) {
+      double win = 1.0;
+      const int ns[3] = {si, sj, kz};
+      for (int a = 0; a < 3; a++) {
+        if (ns[a] != 0) {
+          const double x = M_PI * ns[a] / N;
+          const double sc = sin(x) / x;
+          win *= sc * sc;
+        }
+      }
+      p /= win * win;
+    }
+    atomicAdd(&sb[b], w);
+    atomicAdd(&sb[nbins + b], w * nm);
+    atomicAdd(&sb[2 * nbins + b], w * p);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < 3 * nbins; i += T)
+    if (sb[i] != 0.0) atomicAdd(&acc[i], sb[i]);
+}
+
 // ------------------------------------------------------- dispatch table
 struct MeshKernels {
   void (*fz)(const float*, float2*, const float2*, const float2*, double*);
@@ -465,6 +512,7 @@ cudaError_t pm_plan_alloc(PmPlan* p, int N, int factor, float L) {
   CG_TRY(cudaMalloc(&p->twN, sizeof(float2) * N));
   CG_TRY(cudaMalloc(&p->twH, sizeof(float2) * (N / 2)));
   CG_TRY(cudaMalloc(&p->dsum, sizeof(double)));
+  CG_TRY(cudaMalloc(&p->pk_acc, sizeof(double) * 3 * N));
   CG_TRY(cudaMalloc(&p->err, sizeof(unsigned)));
   {
     float2* h = (float2*)malloc(sizeof(float2) * N);
@@ -556,6 +604,7 @@ void pm_plan_free(PmPlan* p) {
   cudaFree(p->twN);
   cudaFree(p->twH);
   cudaFree(p->dsum);
+  cudaFree(p->pk_acc);
   cudaFree(p->err);
   memset(p, 0, sizeof(*p));
 }
@@ -616,4 +665,26 @@ cudaError_t pm_forces(PmPlan* p, const float* const x[3], long long n, float* co
   if ((e = pm_r2c(p, st)) != cudaSuccess) return e;
   if ((e = pm_green_c2r(p, st)) != cudaSuccess) return e;
   return pm_interp(p, x, n, f, st);
+}
+
+cudaError_t pm_power_spectrum(PmPlan* p, const float* const x[3], long long n, int nbins,
+                              int deconv, double* acc, cudaStream_t st) {
+  MeshKernels k;
+  if (!get_kernels(p->N, &k)) return cudaErrorInvalidValue;
+  if (nbins < 1 || nbins > p->N) return cudaErrorInvalidValue;
+  const int N = p->N;
+  cudaError_t e = pm_deposit(p, x, n, st);
+  if (e != cudaSuccess) return e;
+  cudaMemsetAsync(p->dsum, 0, sizeof(double), st);
+  prof_mark(st, CG_ST_FZ);
+  k.fz<<<dim3(N / TY, N), T, k.sm_fz, st>>>(p->dens, p->spec, p->twH, p->twN, p->dsum);
+  prof_mark(st, CG_ST_FY_FWD);
+  k.fyf<<<(N / 2 + 1) * N / BY, T, k.sm_fy, st>>>(p->spec, p->twN);
+  prof_mark(st, CG_ST_OTHER);
+  k.fxpf<<<dim3(N / TK, N / 2 + 1), T, k.sm_fxp, st>>>(p->spec, p->twN);
+  cudaMemsetAsync(acc, 0, sizeof(double) * 3 * nbins, st);
+  prof_mark(st, CG_ST_OTHER);
+  k_pk_bin<<<grid_for((long long)(N / 2 + 1) * N * N), T, sizeof(double) * 3 * nbins, st>>>(
+      p->spec, N, nbins, deconv, acc);
+  return cudaGetLastError();
 }

@@ -71,6 +71,18 @@ class Simulation:
         _lib.check(self.lib.cg_sim_get_mesh(self.h, which, out.ctypes.data), "cg_sim_get_mesh")
         return out
 
+    def power_spectrum(self, nbins=None, deconvolve_cic=False, subtract_shot=False):
+        """(k, P(k), modes) of the current positions' CIC density."""
+        nb = nbins or self.ngrid // 2
+        k = np.zeros(nb)
+        p = np.zeros(nb)
+        m = np.zeros(nb)
+        flags = (1 if deconvolve_cic else 0) | (2 if subtract_shot else 0)
+        _lib.check(self.lib.cg_sim_power_spectrum(self.h, nb, flags, k.ctypes.data,
+                                                  p.ctypes.data, m.ctypes.data),
+                   "cg_sim_power_spectrum")
+        return k, p, m
+
     def times(self):
         ax, av = ctypes.c_float(), ctypes.c_float()
         self.lib.cg_sim_get_times(self.h, ctypes.byref(ax), ctypes.byref(av))

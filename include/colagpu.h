@@ -94,11 +94,51 @@ int cg_sim_drift_coeffs(cg_sim* s, float dyyy, float da1, float da2);
 int cg_sim_snapshot(cg_sim* s, double aout, float omega_m, void* pmin_out);
 /* Wait for all queued work of the handle; reports device-side errors. */
 int cg_sim_sync(cg_sim* s);
+/* Power spectrum of the particles' CIC density on the PM mesh (no
+ * reference counterpart; the reference writes only a coarse density grid,
+ * coarse_grid.c).  delta_k = r2c(delta)/ngrid^3, P = L^3 |delta_k|^2
+ * averaged over shells: bin b has |n| in [b+1/2, b+3/2) in units of the
+ * fundamental 2 pi/L.  Outputs nbins values each of mean k (h/Mpc), P(k)
+ * ((Mpc/h)^3) and the number of modes.  nbins <= ngrid.  Overwrites the
+ * density mesh; synchronous. */
+#define CG_PK_DECONVOLVE_CIC 1   /* divide by the CIC window squared */
+#define CG_PK_SUBTRACT_SHOT 2    /* subtract L^3 / np */
+int cg_sim_power_spectrum(cg_sim* s, int nbins, int flags, double* k, double* pk,
+                          double* nmodes);
 /* Copy one mesh to host: which = 0 density (delta), 1..3 force x, y, z;
  * ngrid^3 floats, [x][y][z] order. */
 int cg_sim_get_mesh(cg_sim* s, int which, float* out);
 /* The CUDA stream (cudaStream_t) the handle queues its work on. */
 void* cg_sim_stream(cg_sim* s);
+
+/* Batched realizations in one CUDA graph launch (no reference counterpart:
+ * the reference loops over seeds one at a time, main.c:117-209).  Each
+ * realization has its own particles, mesh, box size and schedule: nsteps
+ * drifts linear in a from a_init to a_final (nsteps + 1 force
+ * evaluations), one snapshot at aout, and the P(k) of its final positions
+ * (ngrid/2 bins, as cg_sim_power_spectrum without flags).  The whole batch
+ * is recorded into one graph on the first cg_batch_run and relaunched on
+ * later calls; every launch restarts from the stored initial particles. */
+typedef struct {
+  int nc;            /* particles per dimension */
+  int ngrid;         /* mesh cells per dimension (a multiple of nc) */
+  float boxsize;     /* Mpc/h */
+  double a_init, a_final;
+  int nsteps;
+  float aout;        /* snapshot scale factor */
+} cg_realization_spec;
+typedef struct cg_batch cg_batch;
+int cg_batch_create(cg_batch** out, int nreal, const cg_realization_spec* specs,
+                    double omega_m, int nstreams);
+void cg_batch_destroy(cg_batch* b);
+/* Initial particles of realization i: nc^3 reference Particle structs. */
+int cg_batch_set_particles(cg_batch* b, int i, const void* particles, long long np);
+/* Launch (recording first if needed) and wait; checks every density sum. */
+int cg_batch_run(cg_batch* b);
+int cg_batch_get_snapshot(cg_batch* b, int i, void* pmin_out);
+int cg_batch_power_spectrum(cg_batch* b, int i, double* k, double* pk, double* nmodes);
+/* Number of nodes of the recorded graph (after the first run). */
+int cg_batch_num_nodes(cg_batch* b, size_t* nodes);
 
 /* Unnormalised 3-D real transforms of host arrays on the device, FFTW sign
  * convention (replaces the fftwf_mpi r2c / c2r plans of pm.c:141-147 and
