@@ -343,6 +343,7 @@ def run_b200(args, cfg):
         step(i)
     sim.sync()
     # one density check outside the timed region (pm.c:535-562)
+    sim.move()
     dsum = sim.forces(check_density=True)
     ev0, ev1 = cuda.event(), cuda.event()
     clocks = Clocks(local)

@@ -218,4 +218,127 @@ __device__ __forceinline__ void fft_lines(cplx* s, const float2* __restrict__ tw
   fft_from<L, 0, B, T, SB, SN, LINE_MAJOR, DIR>(s, tw);
 }
 
+// =====================================================================
+// Direct-I/O variant: the first radix stage reads its butterfly legs
+// straight from global memory and the last stage writes straight to global
+// memory (both access patterns are j + r L/R, coalesced across consecutive
+// butterflies), so only the S-1 exchanges between stages go through shared
+// memory.  Shared-memory tiles are padded (one element per 16 along a line,
+// one per 32 in column-interleaved tiles) to spread the stride-R writes of
+// the early stages over the banks.
+// =====================================================================
+
+// Line-major shared tile: element n of line b at b*SB + n + n/16.
+template <int SB>
+struct SmemLine {
+  cplx* s;
+  __device__ __forceinline__ cplx ld(int b, int n) const { return s[b * SB + n + (n >> 4)]; }
+  __device__ __forceinline__ void st(int b, int n, cplx v) const { s[b * SB + n + (n >> 4)] = v; }
+  static constexpr bool kShared = true;
+};
+template <int L> __host__ __device__ constexpr int line_pitch() { return L + L / 16 + 1; }
+
+// Column-interleaved shared tile: element n of column b at i = n*B + b,
+// stored at i + i/32.
+template <int B>
+struct SmemCol {
+  cplx* s;
+  __device__ __forceinline__ int at(int b, int n) const {
+    const int i = n * B + b;
+    return i + (i >> 5);
+  }
+  __device__ __forceinline__ cplx ld(int b, int n) const { return s[at(b, n)]; }
+  __device__ __forceinline__ void st(int b, int n, cplx v) const { s[at(b, n)] = v; }
+  static constexpr bool kShared = true;
+};
+template <int L, int B> __host__ __device__ constexpr int col_tile_elems() {
+  return L * B + (L * B) / 32 + 1;
+}
+
+// Global lines: element n of line b at p[b * ls + n * es].
+struct Gmem {
+  float2* p;
+  size_t ls;
+  size_t es;
+  __device__ __forceinline__ cplx ld(int b, int n) const {
+    const float2 v = __ldg(p + b * ls + (size_t)n * es);
+    return cplx{v.x, v.y};
+  }
+  __device__ __forceinline__ void st(int b, int n, cplx v) const {
+    p[b * ls + (size_t)n * es] = make_float2(v.x, v.y);
+  }
+  static constexpr bool kShared = false;
+};
+
+template <int L, int R, int NS, int B, int T, bool LINE_MAJOR, int DIR, class In, class Out>
+__device__ __forceinline__ void stage_io(const In& in, const Out& out,
+                                         const float2* __restrict__ tw, bool inplace) {
+  constexpr int NBF = L / R;
+  constexpr int TOTAL = NBF * B;
+  constexpr int PER = (TOTAL + T - 1) / T;
+  cplx v[PER][R];
+  const int tid = threadIdx.x;
+#pragma unroll
+  for (int q = 0; q < PER; q++) {
+    const int idx = tid + q * T;
+    if (TOTAL % T == 0 || idx < TOTAL) {
+      const int b = LINE_MAJOR ? idx / NBF : idx % B;
+      const int j = LINE_MAJOR ? idx % NBF : idx / B;
+#pragma unroll
+      for (int r = 0; r < R; r++) v[q][r] = in.ld(b, j + r * NBF);
+    }
+  }
+  if (inplace) __syncthreads();
+#pragma unroll
+  for (int q = 0; q < PER; q++) {
+    const int idx = tid + q * T;
+    if (TOTAL % T == 0 || idx < TOTAL) {
+      const int b = LINE_MAJOR ? idx / NBF : idx % B;
+      const int j = LINE_MAJOR ? idx % NBF : idx / B;
+      const int jm = NS == 1 ? 0 : j % NS;
+      if (NS > 1) {
+        constexpr int STEP = L / (NS * R);
+#pragma unroll
+        for (int r = 1; r < R; r++) v[q][r] = cmul(v[q][r], twiddle<DIR>(tw, jm * r * STEP));
+      }
+      dft<R, DIR>(v[q]);
+      const int base = (j / NS) * NS * R + jm;
+#pragma unroll
+      for (int r = 0; r < R; r++) out.st(b, base + r * NS, v[q][r]);
+    }
+  }
+}
+
+// Stages S0..end of an L-point FFT: stage S0 reads `first`, the last stage
+// writes `last`, stages in between work in place on shared tile `mid`.
+// Every stage that writes `mid` is followed by a barrier.
+template <int L, int S, int B, int T, bool LM, int DIR, class First, class Mid, class Last>
+__device__ __forceinline__ void fft_io_from(const First& first, const Mid& mid, const Last& last,
+                                            const float2* __restrict__ tw) {
+  constexpr int NSTAGE = num_stages(L);
+  constexpr int R = radix_at(L, S);
+  constexpr int NS = ns_before(L, S);
+  if constexpr (S == NSTAGE - 1) {
+    if constexpr (S == 0)
+      stage_io<L, R, NS, B, T, LM, DIR>(first, last, tw, First::kShared && Last::kShared);
+    else
+      stage_io<L, R, NS, B, T, LM, DIR>(mid, last, tw, Last::kShared);
+    if constexpr (Last::kShared) __syncthreads();
+  } else {
+    if constexpr (S == 0)
+      stage_io<L, R, NS, B, T, LM, DIR>(first, mid, tw, First::kShared);
+    else
+      stage_io<L, R, NS, B, T, LM, DIR>(mid, mid, tw, true);
+    __syncthreads();
+    fft_io_from<L, S + 1, B, T, LM, DIR>(first, mid, last, tw);
+  }
+}
+
+template <int L, int B, int T, bool LM, int DIR, class First, class Mid, class Last>
+__device__ __forceinline__ void fft_io(const First& first, const Mid& mid, const Last& last,
+                                       const float2* __restrict__ tw) {
+  static_assert(supported_length(L), "FFT length must be 2^a 3^b");
+  fft_io_from<L, 0, B, T, LM, DIR>(first, mid, last, tw);
+}
+
 }  // namespace cgfft

@@ -365,6 +365,153 @@ __global__ void __launch_bounds__(T) k_zi_c2r(const float2* __restrict__ gsp,
   }
 }
 
+// ====================================================================
+// Direct-I/O pass kernels (cgfft::fft_io): the first radix stage loads
+// straight from HBM, the last stores straight to HBM, and only the
+// exchanges between stages use the (padded) shared tile.
+// ====================================================================
+using cgfft::Gmem;
+using cgfft::SmemCol;
+using cgfft::SmemLine;
+
+// ky columns per CTA of the fused Green pass: one radix-16 butterfly per
+// thread in the 16-point stages ((N/16) * TK <= 256) keeps the three
+// inverse transforms of the tile within the register budget.
+__host__ __device__ constexpr int tk_green(int N) { return N >= 768 ? 4 : TK; }
+
+template <int N, int DIR>
+__global__ void __launch_bounds__(T) k_fy2(float2* __restrict__ spec,
+                                           const float2* __restrict__ twN) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const SmemLine<cgfft::line_pitch<N>()> mid{reinterpret_cast<cplx*>(smraw)};
+  const Gmem g{spec + (size_t)blockIdx.x * BY * N, (size_t)N, 1};
+  cgfft::fft_io<N, BY, T, true, DIR>(g, mid, g, twN);
+}
+
+template <int N, int DIR>
+__global__ void __launch_bounds__(T) k_fx_plain2(float2* __restrict__ spec,
+                                                 const float2* __restrict__ twN) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const SmemCol<TK> mid{reinterpret_cast<cplx*>(smraw)};
+  const Gmem g{spec + (size_t)blockIdx.y * N * N + blockIdx.x * TK, 1, (size_t)N};
+  cgfft::fft_io<N, TK, T, false, DIR>(g, mid, g, twN);
+}
+
+template <int N>
+__global__ void __launch_bounds__(T) k_fx_green2(const float2* __restrict__ spec,
+                                                 float2* __restrict__ g0,
+                                                 float2* __restrict__ g1,
+                                                 float2* __restrict__ g2,
+                                                 const float2* __restrict__ twN, float f1) {
+  constexpr int TKG = tk_green(N);
+  extern __shared__ __align__(16) unsigned char smraw[];
+  constexpr int TILE = cgfft::col_tile_elems<N, TKG>();
+  const SmemCol<TKG> D{reinterpret_cast<cplx*>(smraw)};
+  const SmemCol<TKG> W{reinterpret_cast<cplx*>(smraw) + TILE};
+  const int kz = blockIdx.y;
+  const int ky0 = blockIdx.x * TKG;
+  const size_t off = (size_t)kz * N * N + ky0;
+  const Gmem gin{const_cast<float2*>(spec) + off, 1, (size_t)N};
+  cgfft::fft_io<N, TKG, T, false, -1>(gin, D, D, twN);
+  float2* gout[3] = {g0, g1, g2};
+#pragma unroll 1
+  for (int a = 0; a < 3; a++) {
+    for (int idx = threadIdx.x; idx < N * TKG; idx += T) {
+      const int n = idx / TKG, b = idx % TKG;
+      const int ky = ky0 + b;
+      const int I0 = n <= N / 2 ? n : n - N;
+      const int J0 = ky <= N / 2 ? ky : ky - N;
+      const int den = kz * kz + I0 * I0 + J0 * J0;
+      cplx out = {0.0f, 0.0f};
+      if (den != 0) {
+        const float di = a == 0 ? (float)I0 : (a == 1 ? (float)J0 : (float)kz);
+        const float f2 = __fmul_rn(__fdiv_rn(f1, (float)den), di);
+        const cplx p = D.ld(b, n);
+        out = cplx{-__fmul_rn(f2, p.y), __fmul_rn(f2, p.x)};
+      }
+      W.st(b, n, out);
+    }
+    __syncthreads();
+    const Gmem go{gout[a] + off, 1, (size_t)N};
+    cgfft::fft_io<N, TKG, T, false, 1>(W, W, go, twN);
+    __syncthreads();
+  }
+}
+
+// r2c along z; the density sum is the sum over lines of X_0 (the plain sum
+// of each line, formed by the transform) accumulated in double.
+template <int N>
+__global__ void __launch_bounds__(T) k_fz2(const float* __restrict__ dens,
+                                           float2* __restrict__ spec,
+                                           const float2* __restrict__ twH,
+                                           const float2* __restrict__ twN,
+                                           double* __restrict__ dsum) {
+  constexpr int H = N / 2;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const SmemLine<cgfft::line_pitch<H>()> mid{reinterpret_cast<cplx*>(smraw)};
+  const int x = blockIdx.y;
+  const int y0 = blockIdx.x * TY;
+  const Gmem gin{reinterpret_cast<float2*>(const_cast<float*>(dens)) + ((size_t)x * N + y0) * H,
+                 (size_t)H, 1};
+  cgfft::fft_io<H, TY, T, true, -1>(gin, mid, mid, twH);
+  double acc = 0.0;
+  for (int idx = threadIdx.x; idx < (H + 1) * TY; idx += T) {
+    const int b = idx % TY, k = idx / TY;
+    const cplx zk = mid.ld(b, k == H ? 0 : k);
+    const cplx zc0 = mid.ld(b, k == 0 ? 0 : H - k);
+    const cplx zc = {zc0.x, -zc0.y};
+    const cplx e = {0.5f * (zk.x + zc.x), 0.5f * (zk.y + zc.y)};
+    const cplx dlt = {zk.x - zc.x, zk.y - zc.y};
+    const cplx o = {0.5f * dlt.y, -0.5f * dlt.x};
+    const float2 w = __ldg(twN + k);
+    const cplx X = {e.x + (w.x * o.x - w.y * o.y), e.y + (w.x * o.y + w.y * o.x)};
+    if (k == 0) acc += (double)zk.x + (double)zk.y;
+    spec[((size_t)k * N + x) * N + y0 + b] = make_float2(X.x, X.y);
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0 && acc != 0.0) atomicAdd(dsum, acc);
+}
+
+template <int N>
+__global__ void __launch_bounds__(T) k_zi2(const float2* __restrict__ gsp,
+                                           float* __restrict__ out,
+                                           const float2* __restrict__ twH,
+                                           const float2* __restrict__ twN) {
+  constexpr int H = N / 2;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const SmemLine<cgfft::line_pitch<H + 1>()> mid{reinterpret_cast<cplx*>(smraw)};
+  const int x = blockIdx.y;
+  const int y0 = blockIdx.x * TY;
+  for (int idx = threadIdx.x; idx < (H + 1) * TY; idx += T) {
+    const int b = idx % TY, k = idx / TY;
+    const float2 v = gsp[((size_t)k * N + x) * N + y0 + b];
+    mid.st(b, k, cplx{v.x, v.y});
+  }
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < (H / 2 + 1) * TY; idx += T) {
+    const int b = idx % TY, k = idx / TY;
+    if (k == 0) {
+      const float x0 = mid.ld(b, 0).x, xh = mid.ld(b, H).x;
+      mid.st(b, 0, cplx{x0 + xh, x0 - xh});
+    } else {
+      const int k2 = H - k;
+      const cplx a = mid.ld(b, k), c = mid.ld(b, k2);
+      const float2 wa = __ldg(twN + k), wc = __ldg(twN + k2);
+      const cplx sa = {a.x + c.x, a.y - c.y}, da = {a.x - c.x, a.y + c.y};
+      const cplx ra = {da.x * wa.x + da.y * wa.y, da.y * wa.x - da.x * wa.y};
+      const cplx za = {sa.x - ra.y, sa.y + ra.x};
+      const cplx sc = {c.x + a.x, c.y - a.y}, dc = {c.x - a.x, c.y + a.y};
+      const cplx rc = {dc.x * wc.x + dc.y * wc.y, dc.y * wc.x - dc.x * wc.y};
+      const cplx zc = {sc.x - rc.y, sc.y + rc.x};
+      mid.st(b, k, za);
+      if (k2 != k) mid.st(b, k2, zc);
+    }
+  }
+  __syncthreads();
+  const Gmem gout{reinterpret_cast<float2*>(out) + ((size_t)x * N + y0) * H, (size_t)H, 1};
+  cgfft::fft_io<H, TY, T, true, 1>(mid, mid, gout, twH);
+}
+
 // ---------------------------------------------------- power spectrum bins
 // Shell average of |delta_k|^2 over the half spectrum S[kz][kx][ky]: bin b
 // holds modes with |n| in [b + 1/2, b + 3/2) (|n| in units of the
@@ -422,23 +569,43 @@ struct MeshKernels {
   void (*fxpf)(float2*, const float2*);
   void (*fxpi)(float2*, const float2*);
   size_t sm_fz, sm_fy, sm_fx, sm_zi, sm_fxp;
+  int tkx;   // ky columns per CTA of the fx (Green) kernel
 };
 
 template <int N>
 MeshKernels make_kernels() {
   MeshKernels k;
-  k.fz = k_fz_r2c<N>;
-  k.fyf = k_fy<N, -1>;
-  k.fyi = k_fy<N, 1>;
-  k.fx = k_fx_green<N>;
-  k.zi = k_zi_c2r<N>;
-  k.fxpf = k_fx_plain<N, -1>;
-  k.fxpi = k_fx_plain<N, 1>;
-  k.sm_fxp = sizeof(cplx) * N * TK;
-  k.sm_fz = sizeof(cplx) * TY * (N / 2 + 1);
-  k.sm_fy = sizeof(cplx) * BY * N;
-  k.sm_fx = sizeof(cplx) * 2 * N * TK;
-  k.sm_zi = sizeof(cplx) * TY * (N / 2 + 1);
+  static const bool v1 = getenv("COLAGPU_FFT_V1") && getenv("COLAGPU_FFT_V1")[0] == '1';
+  if (v1) {
+    // shared-memory staged passes (every stage goes through the tile)
+    k.fz = k_fz_r2c<N>;
+    k.fyf = k_fy<N, -1>;
+    k.fyi = k_fy<N, 1>;
+    k.fx = k_fx_green<N>;
+    k.zi = k_zi_c2r<N>;
+    k.fxpf = k_fx_plain<N, -1>;
+    k.fxpi = k_fx_plain<N, 1>;
+    k.sm_fxp = sizeof(cplx) * N * TK;
+    k.sm_fz = sizeof(cplx) * TY * (N / 2 + 1);
+    k.sm_fy = sizeof(cplx) * BY * N;
+    k.sm_fx = sizeof(cplx) * 2 * N * TK;
+    k.sm_zi = sizeof(cplx) * TY * (N / 2 + 1);
+    k.tkx = TK;
+    return k;
+  }
+  k.fz = k_fz2<N>;
+  k.fyf = k_fy2<N, -1>;
+  k.fyi = k_fy2<N, 1>;
+  k.fx = k_fx_green2<N>;
+  k.zi = k_zi2<N>;
+  k.fxpf = k_fx_plain2<N, -1>;
+  k.fxpi = k_fx_plain2<N, 1>;
+  k.sm_fxp = sizeof(cplx) * cgfft::col_tile_elems<N, TK>();
+  k.sm_fz = sizeof(cplx) * TY * cgfft::line_pitch<N / 2>();
+  k.sm_fy = sizeof(cplx) * BY * cgfft::line_pitch<N>();
+  k.sm_fx = sizeof(cplx) * 2 * cgfft::col_tile_elems<N, tk_green(N)>();
+  k.tkx = tk_green(N);
+  k.sm_zi = sizeof(cplx) * TY * cgfft::line_pitch<N / 2 + 1>();
   return k;
 }
 
@@ -637,7 +804,7 @@ cudaError_t pm_green_c2r(PmPlan* p, cudaStream_t st) {
   get_kernels(p->N, &k);
   const int N = p->N;
   prof_mark(st, CG_ST_FX_GREEN);
-  k.fx<<<dim3(N / TK, N / 2 + 1), T, k.sm_fx, st>>>(p->spec, p->gsp[0], p->gsp[1], p->gsp[2],
+  k.fx<<<dim3(N / k.tkx, N / 2 + 1), T, k.sm_fx, st>>>(p->spec, p->gsp[0], p->gsp[1], p->gsp[2],
                                                      p->twN, p->f1);
   for (int a = 0; a < 3; a++) {
     prof_mark(st, CG_ST_FY_INV);
