@@ -49,6 +49,18 @@ SIGNATURES = {
     "cg_sim_get_mesh": (i32, [P, i32, P]),
     "cg_sim_power_spectrum": (i32, [P, i32, i32, P, P, P]),
     "cg_sim_stream": (P, [P]),
+    "cg_sim_copy_particles": (i32, [P, P]),
+    "cg_net_create": (i32, [ctypes.POINTER(P), i32, ctypes.c_ulonglong]),
+    "cg_net_destroy": (None, [P]),
+    "cg_net_num_params": (i32, []),
+    "cg_net_get_params": (i32, [P, P]),
+    "cg_net_set_params": (i32, [P, P]),
+    "cg_net_set_scales": (i32, [P, f32, f32, f32]),
+    "cg_net_set_tensor_cores": (i32, [P, i32]),
+    "cg_net_forward_host": (i32, [P, P, P]),
+    "cg_net_backward_host": (i32, [P, P, P, P]),
+    "cg_net_train_step": (i32, [P, P, P, f32, dptr]),
+    "cg_net_forces": (i32, [P, P]),
     "cg_batch_create": (i32, [ctypes.POINTER(P), i32, P, f64, i32]),
     "cg_batch_destroy": (None, [P]),
     "cg_batch_set_particles": (i32, [P, i32, P, i64]),

@@ -16,6 +16,9 @@
 #include "cosmo.h"
 #include "internal.h"
 #include "lpt.h"
+#include "convnet.h"
+
+#include <vector>
 
 // ----------------------------------------------------------------- errors
 static thread_local std::string g_err;
@@ -351,6 +354,179 @@ extern "C" int cg_sim_get_mesh(cg_sim* s, int which, float* out) {
   const float* src = which == 0 ? s->pm.dens : s->pm.fmesh[which - 1];
   CG_CHECK(cudaMemcpyAsync(out, src, s->pm.mesh_bytes, cudaMemcpyDeviceToHost, s->st), "get mesh");
   CG_CHECK(cudaStreamSynchronize(s->st), "sync");
+  return CG_OK;
+}
+
+extern "C" int cg_sim_copy_particles(cg_sim* dst, const cg_sim* src) {
+  if (!dst || !src || src->ps.n > dst->ps.cap)
+    return set_err(CG_EINVAL, "cg_sim_copy_particles: bad arguments");
+  CG_CHECK(cudaStreamSynchronize(src->st), "sync");
+  const size_t n = (size_t)src->ps.n;
+  for (int a = 0; a < 3; a++) {
+    CG_CHECK(cudaMemcpyAsync(dst->ps.x[a], src->ps.x[a], 4 * n, cudaMemcpyDeviceToDevice, dst->st), "copy");
+    CG_CHECK(cudaMemcpyAsync(dst->ps.v[a], src->ps.v[a], 4 * n, cudaMemcpyDeviceToDevice, dst->st), "copy");
+    CG_CHECK(cudaMemcpyAsync(dst->ps.dx1[a], src->ps.dx1[a], 4 * n, cudaMemcpyDeviceToDevice, dst->st), "copy");
+    CG_CHECK(cudaMemcpyAsync(dst->ps.dx2[a], src->ps.dx2[a], 4 * n, cudaMemcpyDeviceToDevice, dst->st), "copy");
+  }
+  CG_CHECK(cudaMemcpyAsync(dst->ps.id, src->ps.id, 8 * n, cudaMemcpyDeviceToDevice, dst->st), "copy");
+  dst->ps.n = src->ps.n;
+  dst->a_x = src->a_x;
+  dst->a_v = src->a_v;
+  return CG_OK;
+}
+
+// ---------------------------------------------------- learned correction
+struct cg_net {
+  CNet n{};
+  cudaStream_t st = nullptr;
+};
+
+extern "C" int cg_net_create(cg_net** out, int ngrid, unsigned long long seed) {
+  if (!out || !pm_supported_mesh(ngrid)) return set_err(CG_EINVAL, "cg_net_create: bad mesh");
+  cg_net* h = new cg_net();
+  cudaError_t e = cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cnet_alloc(&h->n, ngrid, seed);
+  if (e != cudaSuccess) {
+    if (h->st) cudaStreamDestroy(h->st);
+    delete h;
+    return cuda_err(e, "cg_net_create");
+  }
+  h->n.use_tc = 1;
+  *out = h;
+  return CG_OK;
+}
+
+extern "C" void cg_net_destroy(cg_net* h) {
+  if (!h) return;
+  cudaStreamSynchronize(h->st);
+  cnet_free(&h->n);
+  cudaStreamDestroy(h->st);
+  delete h;
+}
+
+extern "C" int cg_net_set_tensor_cores(cg_net* h, int on) {
+  if (!h) return set_err(CG_EINVAL, "cg_net_set_tensor_cores: NULL");
+  h->n.use_tc = on ? 1 : 0;
+  return CG_OK;
+}
+
+extern "C" int cg_net_set_scales(cg_net* h, float in_delta, float in_phi, float out_scale) {
+  if (!h || !(out_scale > 0)) return set_err(CG_EINVAL, "cg_net_set_scales: bad arguments");
+  h->n.in_scale[0] = in_delta;
+  h->n.in_scale[1] = in_phi;
+  h->n.out_scale = out_scale;
+  return CG_OK;
+}
+
+extern "C" int cg_net_get_params(cg_net* h, float* out) {
+  if (!h || !out) return set_err(CG_EINVAL, "cg_net_get_params: NULL");
+  CG_CHECK(cudaMemcpyAsync(out, h->n.params, sizeof(float) * CNET_PARAMS, cudaMemcpyDeviceToHost,
+                           h->st), "get params");
+  CG_CHECK(cudaStreamSynchronize(h->st), "sync");
+  return CG_OK;
+}
+
+extern "C" int cg_net_set_params(cg_net* h, const float* p) {
+  if (!h || !p) return set_err(CG_EINVAL, "cg_net_set_params: NULL");
+  CG_CHECK(cudaMemcpyAsync(h->n.params, p, sizeof(float) * CNET_PARAMS, cudaMemcpyHostToDevice,
+                           h->st), "set params");
+  CG_CHECK(cnet_sync_bf16(&h->n, h->st), "bf16 weights");
+  CG_CHECK(cudaStreamSynchronize(h->st), "sync");
+  return CG_OK;
+}
+
+extern "C" int cg_net_num_params(void) { return CNET_PARAMS; }
+
+// Host-array entry points (checks and tools): in2 = [v][2] features
+// (already scaled), out3 = [v][3] raw network output, grad3 = dL/dout.
+static int net_load_input(cg_net* h, const float* in2) {
+  const size_t nv = (size_t)h->n.N * h->n.N * h->n.N;
+  std::vector<__nv_bfloat16> b(nv * CNET_C, __float2bfloat16_rn(0.0f));
+  for (size_t v = 0; v < nv; v++) {
+    b[v * CNET_C] = __float2bfloat16_rn(in2[2 * v]);
+    b[v * CNET_C + 1] = __float2bfloat16_rn(in2[2 * v + 1]);
+  }
+  CG_CHECK(cudaMemcpyAsync(h->n.act[0], b.data(), b.size() * sizeof(__nv_bfloat16),
+                           cudaMemcpyHostToDevice, h->st), "upload input");
+  CG_CHECK(cudaStreamSynchronize(h->st), "sync");
+  return CG_OK;
+}
+
+static int net_check_tc() {
+  if (conv_tc_error_word()) return set_err(CG_ECUDA, "tensor-core convolution wait timed out");
+  return CG_OK;
+}
+
+extern "C" int cg_net_forward_host(cg_net* h, const float* in2, float* out3) {
+  if (!h || !in2 || !out3) return set_err(CG_EINVAL, "cg_net_forward_host: NULL");
+  int rc = net_load_input(h, in2);
+  if (rc) return rc;
+  CG_CHECK(cnet_forward(&h->n, h->st), "forward");
+  const size_t nv = (size_t)h->n.N * h->n.N * h->n.N;
+  std::vector<float> o(nv * CNET_C);
+  CG_CHECK(cudaMemcpyAsync(o.data(), h->n.out, o.size() * 4, cudaMemcpyDeviceToHost, h->st), "dl");
+  CG_CHECK(cudaStreamSynchronize(h->st), "sync");
+  for (size_t v = 0; v < nv; v++)
+    for (int c = 0; c < 3; c++) out3[3 * v + c] = o[v * CNET_C + c];
+  return net_check_tc();
+}
+
+extern "C" int cg_net_backward_host(cg_net* h, const float* in2, const float* grad3,
+                                    float* grads) {
+  if (!h || !in2 || !grad3 || !grads) return set_err(CG_EINVAL, "cg_net_backward_host: NULL");
+  int rc = net_load_input(h, in2);
+  if (rc) return rc;
+  CG_CHECK(cnet_forward(&h->n, h->st), "forward");
+  const size_t nv = (size_t)h->n.N * h->n.N * h->n.N;
+  std::vector<float> g(nv * CNET_C, 0.0f);
+  for (size_t v = 0; v < nv; v++)
+    for (int c = 0; c < 3; c++) g[v * CNET_C + c] = grad3[3 * v + c];
+  CG_CHECK(cudaMemcpyAsync(h->n.g0, g.data(), g.size() * 4, cudaMemcpyHostToDevice, h->st), "ul");
+  CG_CHECK(cnet_backward(&h->n, h->st), "backward");
+  CG_CHECK(cudaMemcpyAsync(grads, h->n.grads, sizeof(float) * CNET_PARAMS, cudaMemcpyDeviceToHost,
+                           h->st), "dl");
+  CG_CHECK(cudaStreamSynchronize(h->st), "sync");
+  return net_check_tc();
+}
+
+// One training step on the current particles of two realizations holding
+// the same particles: coarse (the net's mesh) and fine (the target mesh).
+extern "C" int cg_net_train_step(cg_net* h, cg_sim* coarse, cg_sim* fine, float lr,
+                                 double* loss) {
+  if (!h || !coarse || !fine || coarse->pm.N != h->n.N || coarse->ps.n != fine->ps.n)
+    return set_err(CG_EINVAL, "cg_net_train_step: bad arguments");
+  int rc = cg_sim_forces(coarse, nullptr);
+  if (!rc) rc = cg_sim_forces(fine, nullptr);
+  if (rc) return rc;
+  CG_CHECK(cudaStreamSynchronize(fine->st), "sync fine");
+  CG_CHECK(cudaStreamSynchronize(coarse->st), "sync coarse");
+  cudaStream_t st = h->st;
+  const float* x[3] = {coarse->ps.x[0], coarse->ps.x[1], coarse->ps.x[2]};
+  const float* ff[3] = {fine->ps.f[0], fine->ps.f[1], fine->ps.f[2]};
+  const float* fc[3] = {coarse->ps.f[0], coarse->ps.f[1], coarse->ps.f[2]};
+  CG_CHECK(cnet_features(&h->n, coarse->pm.dens, st), "features");
+  CG_CHECK(cnet_target(&h->n, x, coarse->ps.n, coarse->L, ff, fc, st), "target");
+  CG_CHECK(cnet_forward(&h->n, st), "forward");
+  CG_CHECK(cnet_loss_grad(&h->n, 1.0 / (double)coarse->ps.n, st), "loss");
+  CG_CHECK(cnet_backward(&h->n, st), "backward");
+  if (lr > 0) CG_CHECK(cnet_adam(&h->n, lr, st), "adam");
+  if (loss) {
+    CG_CHECK(cudaMemcpyAsync(loss, h->n.loss, sizeof(double), cudaMemcpyDeviceToHost, st), "loss");
+  }
+  CG_CHECK(cudaStreamSynchronize(st), "sync");
+  return net_check_tc();
+}
+
+// Forces of the coarse realization with the learned correction added.
+extern "C" int cg_net_forces(cg_net* h, cg_sim* coarse) {
+  if (!h || !coarse || coarse->pm.N != h->n.N) return set_err(CG_EINVAL, "cg_net_forces: bad");
+  int rc = cg_sim_forces(coarse, nullptr);
+  if (rc) return rc;
+  cudaStream_t st = coarse->st;   // stay on the realization's stream
+  const float* x[3] = {coarse->ps.x[0], coarse->ps.x[1], coarse->ps.x[2]};
+  CG_CHECK(cnet_features(&h->n, coarse->pm.dens, st), "features");
+  CG_CHECK(cnet_forward(&h->n, st), "forward");
+  CG_CHECK(cnet_apply(&h->n, x, coarse->ps.n, coarse->L, coarse->ps.f, st), "apply");
   return CG_OK;
 }
 

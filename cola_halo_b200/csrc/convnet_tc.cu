@@ -1,0 +1,231 @@
+// 3x3x3 periodic convolution, 16 -> 16 channels, bf16 x bf16 -> fp32, on the
+// fifth-generation tensor cores (tcgen05.mma, accumulator in tensor memory).
+//
+// Implicit GEMM per tile of 128 consecutive z voxels of one (x, y) line:
+//   D[128 voxels][16 co] = sum over 27 taps of A_t[128][16 ci] . B_t[16 ci][16 co]
+// A_t are the tile's neighbour voxels for tap t, copied from HBM/L2 into
+// shared memory in the no-swizzle K-major core-matrix layout (8 rows x 16 B
+// per core matrix; the two 8-channel halves 128 B apart (LBO), 8-row groups
+// 256 B apart (SBO)).  B_t are the tap weights in the same layout.  One
+// thread issues the 27 MMAs (M=128, N=16, K=16 each), tcgen05.commit
+// arrives on an mbarrier, the four warps read their 32 accumulator lanes
+// with tcgen05.ld and apply bias + activation.  CTAs are persistent over
+// tiles; every mbarrier wait is bounded and reports through an error word.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "convnet.h"
+
+namespace {
+
+constexpr int C = CNET_C;
+constexpr int TILE_M = 128;
+constexpr int A_BYTES = TILE_M * C * 2;          // 4096: one tap's A operand
+constexpr int B_BYTES = C * C * 2;               // 512: one tap's B operand
+constexpr int SMEM = 27 * A_BYTES + 27 * B_BYTES + 64;
+constexpr int THREADS = 128;
+constexpr long long kWaitLimit = 1LL << 24;
+
+__device__ unsigned g_tc_err = 0;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// Shared-memory matrix descriptor: no swizzle, K-major, LBO = 128 B between
+// the two K halves, SBO = 256 B between 8-row groups, version 1.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr) {
+  return (uint64_t)((saddr & 0x3FFFF) >> 4) | ((uint64_t)(128 >> 4) << 16) |
+         ((uint64_t)(256 >> 4) << 32) | (1ULL << 46);
+}
+
+// Instruction descriptor, kind::f16: D f32, A bf16, B bf16, both K-major,
+// N = 16, M = 128.
+constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((16u >> 3) << 17) |
+                            ((128u >> 4) << 24);
+
+// offset of element (row, k) of a [rows][16] bf16 operand in core-matrix layout
+__device__ __forceinline__ int cm_off(int row, int k) {
+  return (((row >> 3) * 2 + (k >> 3)) << 7) + ((row & 7) << 4) + ((k & 7) << 1);
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase) {
+  for (long long i = 0; i < kWaitLimit; i++) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(phase)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+template <bool FLIP>
+__global__ void __launch_bounds__(THREADS, 1) k_conv_tc(const __nv_bfloat16* __restrict__ in, int N,
+                                                        const __nv_bfloat16* __restrict__ w,
+                                                        const float* __restrict__ bias, int act,
+                                                        float* __restrict__ out_f,
+                                                        __nv_bfloat16* __restrict__ out_b) {
+  extern __shared__ __align__(1024) uint8_t sm[];
+  uint8_t* sA = sm;
+  uint8_t* sB = sm + 27 * A_BYTES;
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(sB + 27 * B_BYTES);
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(mbar + 1);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                 :: "r"(smem_u32(tslot)), "r"(32) : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(mbar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  // B_t: element (n = output channel, k = input channel) of tap t
+  for (int i = tid; i < 27 * C * C; i += THREADS) {
+    const int t = i / (C * C), n = (i / C) % C, k = i % C;
+    const __nv_bfloat16 v = FLIP ? w[((26 - t) * C + n) * C + k]   // W[26-t][ci=n][co=k]
+                                 : w[(t * C + k) * C + n];         // W[t][ci=k][co=n]
+    *reinterpret_cast<__nv_bfloat16*>(sB + t * B_BYTES + cm_off(n, k)) = v;
+  }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tslot;
+  const uint32_t bar = smem_u32(mbar);
+  const int tiles_per_line = N / TILE_M;
+  const int ntiles = N * N * tiles_per_line;
+  uint32_t phase = 0;
+  bool ok = true;
+
+  for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+    const int line = tile / tiles_per_line;
+    const int z0 = (tile % tiles_per_line) * TILE_M;
+    const int x = line / N, y = line % N;
+    // A_t: 27 taps x 128 rows x 2 halves of 16 bytes
+    for (int i = tid; i < 27 * TILE_M * 2; i += THREADS) {
+      const int t = i / (TILE_M * 2), r = (i >> 1) % TILE_M, h = i & 1;
+      int xx = x + t / 9 - 1, yy = y + (t / 3) % 3 - 1, zz = z0 + r + t % 3 - 1;
+      xx = xx < 0 ? xx + N : (xx >= N ? xx - N : xx);
+      yy = yy < 0 ? yy + N : (yy >= N ? yy - N : yy);
+      zz = zz < 0 ? zz + N : (zz >= N ? zz - N : zz);
+      const __nv_bfloat16* src = in + (((size_t)xx * N + yy) * N + zz) * C + h * 8;
+      const uint32_t dst = smem_u32(sA + t * A_BYTES + cm_off(r, h * 8));
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" :: "r"(dst), "l"(src) : "memory");
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (tid == 0) {
+      for (int t = 0; t < 27; t++) {
+        const uint64_t da = umma_desc(smem_u32(sA + t * A_BYTES));
+        const uint64_t db = umma_desc(smem_u32(sB + t * B_BYTES));
+        const uint32_t acc = t > 0 ? 1u : 0u;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "setp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n"
+            :: "r"(tmem), "l"(da), "l"(db), "r"(kIdesc), "r"(acc)
+            : "memory");
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                   :: "r"(bar) : "memory");
+    }
+    // every thread waits (bounded); the CTA agrees on the outcome so that all
+    // threads take the same path through the barriers below
+    const bool got = mbar_wait(bar, phase);
+    ok = __syncthreads_and(got ? 1 : 0) != 0;
+    if (!ok && tid == 0) atomicOr(&g_tc_err, 1u);
+    phase ^= 1u;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (ok) {
+      uint32_t r[16];
+      const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16);
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+          "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+          : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
+            "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]),
+            "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+          : "r"(taddr));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      const size_t v = ((size_t)x * N + y) * N + z0 + warp * 32 + lane;
+      float o[C];
+#pragma unroll
+      for (int c = 0; c < C; c++) {
+        float a = __uint_as_float(r[c]) + (bias ? bias[c] : 0.0f);
+        if (act) a = a > 0.0f ? a : 0.1f * a;
+        o[c] = a;
+      }
+      if (out_f) {
+        float4* d = reinterpret_cast<float4*>(out_f + v * C);
+#pragma unroll
+        for (int q = 0; q < 4; q++) d[q] = make_float4(o[4 * q], o[4 * q + 1], o[4 * q + 2], o[4 * q + 3]);
+      }
+      if (out_b) {
+        __nv_bfloat16 hb[C];
+#pragma unroll
+        for (int c = 0; c < C; c++) hb[c] = __float2bfloat16_rn(o[c]);
+        uint4* d = reinterpret_cast<uint4*>(out_b + v * C);
+        d[0] = *reinterpret_cast<const uint4*>(&hb[0]);
+        d[1] = *reinterpret_cast<const uint4*>(&hb[8]);
+      }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+  }
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(32)
+                 : "memory");
+}
+
+template <bool FLIP>
+cudaError_t launch(const __nv_bfloat16* in, int N, const __nv_bfloat16* w, const float* bias,
+                   int act, float* of, __nv_bfloat16* ob, cudaStream_t st) {
+  if (N < TILE_M || N % TILE_M) return cudaErrorNotSupported;
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(k_conv_tc<FLIP>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  const int ntiles = N * N * (N / TILE_M);
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int grid = ntiles < sms ? ntiles : sms;
+  prof_mark(st, CG_ST_OTHER);
+  k_conv_tc<FLIP><<<grid, THREADS, SMEM, st>>>(in, N, w, bias, act, of, ob);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t conv_tc_forward(const __nv_bfloat16* in, int N, const __nv_bfloat16* w,
+                            const float* bias, int act, float* out_f, __nv_bfloat16* out_b,
+                            cudaStream_t st) {
+  return launch<false>(in, N, w, bias, act, out_f, out_b, st);
+}
+
+cudaError_t conv_tc_backward_data(const __nv_bfloat16* g, int N, const __nv_bfloat16* w,
+                                  float* out_f, cudaStream_t st) {
+  return launch<true>(g, N, w, nullptr, 0, out_f, nullptr, st);
+}
+
+unsigned conv_tc_error_word() {
+  unsigned v = 0;
+  cudaMemcpyFromSymbol(&v, g_tc_err, sizeof(v));
+  return v;
+}

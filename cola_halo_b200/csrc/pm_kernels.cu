@@ -438,6 +438,72 @@ __global__ void __launch_bounds__(T) k_fx_green2(const float2* __restrict__ spec
   }
 }
 
+// Store of an inverse-x-transformed column scaled for the y and z force
+// components: n_y = J0 is constant along an x line (fixed ky) and n_z = kz
+// is constant over the CTA, so IFFT_x(i f1 n_a/|n|^2 delta) =
+// n_a IFFT_x(i f1/|n|^2 delta) for a = y, z -- one inverse transform serves
+// both components.
+struct GmemYZ {
+  float2* gy;
+  float2* gz;
+  size_t es;
+  int ky0, N;
+  float fz;
+  __device__ __forceinline__ void st(int b, int n, cplx v) const {
+    const int ky = ky0 + b;
+    const float fy = (float)(ky <= N / 2 ? ky : ky - N);
+    gy[b + (size_t)n * es] = make_float2(v.x * fy, v.y * fy);
+    gz[b + (size_t)n * es] = make_float2(v.x * fz, v.y * fz);
+  }
+  static constexpr bool kShared = false;
+};
+
+template <int N>
+__global__ void __launch_bounds__(T) k_fx_green3(const float2* __restrict__ spec,
+                                                 float2* __restrict__ g0,
+                                                 float2* __restrict__ g1,
+                                                 float2* __restrict__ g2,
+                                                 const float2* __restrict__ twN, float f1) {
+  constexpr int TKG = tk_green(N);
+  extern __shared__ __align__(16) unsigned char smraw[];
+  constexpr int TILE = cgfft::col_tile_elems<N, TKG>();
+  const SmemCol<TKG> D{reinterpret_cast<cplx*>(smraw)};
+  const SmemCol<TKG> W{reinterpret_cast<cplx*>(smraw) + TILE};
+  const int kz = blockIdx.y;
+  const int ky0 = blockIdx.x * TKG;
+  const size_t off = (size_t)kz * N * N + ky0;
+  const Gmem gin{const_cast<float2*>(spec) + off, 1, (size_t)N};
+  cgfft::fft_io<N, TKG, T, false, -1>(gin, D, D, twN);
+#pragma unroll 1
+  for (int pass = 0; pass < 2; pass++) {
+    // pass 0: x component i f1 n_x/|n|^2 delta;  pass 1: i f1/|n|^2 delta
+    for (int idx = threadIdx.x; idx < N * TKG; idx += T) {
+      const int n = idx / TKG, b = idx % TKG;
+      const int ky = ky0 + b;
+      const int I0 = n <= N / 2 ? n : n - N;
+      const int J0 = ky <= N / 2 ? ky : ky - N;
+      const int den = kz * kz + I0 * I0 + J0 * J0;
+      cplx out = {0.0f, 0.0f};
+      if (den != 0) {
+        float f2 = __fdiv_rn(f1, (float)den);
+        if (pass == 0) f2 = __fmul_rn(f2, (float)I0);
+        const cplx p = D.ld(b, n);
+        out = cplx{-__fmul_rn(f2, p.y), __fmul_rn(f2, p.x)};
+      }
+      W.st(b, n, out);
+    }
+    __syncthreads();
+    if (pass == 0) {
+      const Gmem go{g0 + off, 1, (size_t)N};
+      cgfft::fft_io<N, TKG, T, false, 1>(W, W, go, twN);
+    } else {
+      const GmemYZ go{g1 + off, g2 + off, (size_t)N, ky0, N, (float)kz};
+      cgfft::fft_io<N, TKG, T, false, 1>(W, W, go, twN);
+    }
+    __syncthreads();
+  }
+}
+
 // r2c along z; the density sum is the sum over lines of X_0 (the plain sum
 // of each line, formed by the transform) accumulated in double.
 template <int N>
@@ -596,7 +662,8 @@ MeshKernels make_kernels() {
   k.fz = k_fz2<N>;
   k.fyf = k_fy2<N, -1>;
   k.fyi = k_fy2<N, 1>;
-  k.fx = k_fx_green2<N>;
+  static const bool green3 = !(getenv("COLAGPU_GREEN3") && getenv("COLAGPU_GREEN3")[0] == '0');
+  k.fx = green3 ? k_fx_green3<N> : k_fx_green2<N>;
   k.zi = k_zi2<N>;
   k.fxpf = k_fx_plain2<N, -1>;
   k.fxpi = k_fx_plain2<N, 1>;

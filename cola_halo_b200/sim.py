@@ -45,6 +45,11 @@ class Simulation:
                    "cg_sim_set_particles")
         self._keep = p
 
+    def set_particles_ptr(self, ptr, n, a_x, a_v):
+        """Load n reference Particle structs from a host or device address."""
+        _lib.check(self.lib.cg_sim_set_particles(self.h, ptr, n, a_x, a_v),
+                   "cg_sim_set_particles")
+
     def set_state(self, x, dx1, dx2, v=None, ids=None, a_x=0.0, a_v=0.0):
         n = x.shape[0]
         p = np.zeros(n, dtype=PARTICLE_DTYPE)

@@ -111,6 +111,39 @@ int cg_sim_get_mesh(cg_sim* s, int which, float* out);
 /* The CUDA stream (cudaStream_t) the handle queues its work on. */
 void* cg_sim_stream(cg_sim* s);
 
+/* Copy the particle state (x, v, dx1, dx2, id, a_x, a_v) of src into dst
+ * (device to device), e.g. to evaluate two meshes on the same particles. */
+int cg_sim_copy_particles(cg_sim* dst, const cg_sim* src);
+
+/* Learned small-scale force correction (no reference counterpart).  A
+ * three-layer 3x3x3 periodic conv net on a coarse mesh (2 -> 16 -> 16 -> 3
+ * channels, leaky-ReLU 0.1, bf16 weights and activations, fp32
+ * accumulation; convolutions on tcgen05 tensor cores when the mesh is a
+ * multiple of 128) maps (delta, phi) of the coarse mesh to a force residual
+ * that is CIC-interpolated to the particles and added to the coarse PM
+ * force.  Trained by the library's own forward/backward kernels and Adam on
+ * pairs generated by the PM method: the fine-mesh minus coarse-mesh force
+ * at the same particles, deposited on the coarse mesh (mass-weighted MSE).
+ * Parameters: 3 layers x (27*16*16 weights W[tap][ci][cout] + 16 biases). */
+typedef struct cg_net cg_net;
+int cg_net_create(cg_net** out, int ngrid, unsigned long long seed);
+void cg_net_destroy(cg_net* h);
+int cg_net_num_params(void);
+int cg_net_get_params(cg_net* h, float* params);
+int cg_net_set_params(cg_net* h, const float* params);
+int cg_net_set_scales(cg_net* h, float in_delta, float in_phi, float out_scale);
+/* 1: tcgen05 convolutions (default); 0: CUDA-core convolutions. */
+int cg_net_set_tensor_cores(cg_net* h, int on);
+/* Host-array forward / backward (checks): in2 [v][2] scaled features,
+ * out3 [v][3] raw outputs, grad3 = dLoss/dout3, grads [num_params]. */
+int cg_net_forward_host(cg_net* h, const float* in2, float* out3);
+int cg_net_backward_host(cg_net* h, const float* in2, const float* grad3, float* grads);
+/* Training step on two realizations holding the same particles; returns the
+ * loss before the update.  lr <= 0 evaluates without updating. */
+int cg_net_train_step(cg_net* h, cg_sim* coarse, cg_sim* fine, float lr, double* loss);
+/* cg_sim_forces of the coarse realization plus the learned correction. */
+int cg_net_forces(cg_net* h, cg_sim* coarse);
+
 /* Batched realizations in one CUDA graph launch (no reference counterpart:
  * the reference loops over seeds one at a time, main.c:117-209).  Each
  * realization has its own particles, mesh, box size and schedule: nsteps
