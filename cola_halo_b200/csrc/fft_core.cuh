@@ -1,12 +1,15 @@
 // Shared-memory batched FFT building blocks for the PM mesh transforms.
 //
-// A CTA holds a tile of B complex lines of length L in shared memory and runs
-// a self-sorting (Stockham) decimation-in-time FFT on it, one radix stage at a
-// time: every thread loads all the butterfly inputs it owns into registers,
-// the CTA synchronises, then each thread twiddles, does its radix-R DFTs in
-// registers and writes the outputs back in place.  Radices 16, 8, 4, 2, 3.
-// Twiddles come from a table W_L[k] = exp(-2 pi i k / L) computed on the host
-// in double precision and rounded once to float (one table per line length).
+// A CTA holds a tile of B complex lines of length L and runs a self-sorting
+// (Stockham) decimation-in-time FFT on it, one radix stage at a time: every
+// thread loads the butterfly legs it owns into registers, twiddles them,
+// does its radix-R DFTs in registers and writes the outputs.  The first
+// stage may load straight from global memory and the last may store straight
+// to global memory, so a pass over a mesh reads and writes HBM once; the
+// exchanges between stages go through a padded shared tile.  Radices 16, 8,
+// 4, 2 and 3, largest first up to a maximum radix RM.  Twiddles come from a
+// table W_L[k] = exp(-2 pi i k / L) computed on the host in double precision
+// and rounded once to float (one table per line length).
 //
 // Stage s with radix R after sub-transforms of size NS (Stockham autosort):
 //   inputs   a[j + r L/R],                          r = 0..R-1
@@ -126,107 +129,50 @@ template <int R, int DIR> __device__ __forceinline__ void dft(cplx* v) {
 }
 
 // ------------------------------------------------- factorisation of L
-// Radices in application order: 16s, then one of 8/4/2, then 3s.
-__host__ __device__ constexpr int radix_at(int L, int s) {
+// Radices in application order: RM as often as it divides, then one smaller
+// power of two, then 3s.  RM is 16 or 8.
+__host__ __device__ constexpr int radix_at(int L, int s, int RM = 16) {
   int m = L;
   int idx = 0;
-  while (m % 16 == 0 && m / 16 >= 1) {
-    if (idx == s) return 16;
-    m /= 16; idx++;
+  while (m % RM == 0) {
+    if (idx == s) return RM;
+    m /= RM; idx++;
   }
-  if (m % 8 == 0) { if (idx == s) return 8; m /= 8; idx++; }
-  else if (m % 4 == 0) { if (idx == s) return 4; m /= 4; idx++; }
-  else if (m % 2 == 0) { if (idx == s) return 2; m /= 2; idx++; }
+  for (int r = RM / 2; r >= 2; r /= 2) {
+    if (m % r == 0) {
+      if (idx == s) return r;
+      m /= r; idx++;
+      break;
+    }
+  }
   while (m % 3 == 0) {
     if (idx == s) return 3;
     m /= 3; idx++;
   }
   return 0;
 }
-__host__ __device__ constexpr int num_stages(int L) {
+__host__ __device__ constexpr int num_stages(int L, int RM = 16) {
   int s = 0;
-  while (radix_at(L, s) != 0) s++;
+  while (radix_at(L, s, RM) != 0) s++;
   return s;
 }
-__host__ __device__ constexpr int ns_before(int L, int s) {
+__host__ __device__ constexpr int ns_before(int L, int s, int RM = 16) {
   int ns = 1;
-  for (int i = 0; i < s; i++) ns *= radix_at(L, i);
+  for (int i = 0; i < s; i++) ns *= radix_at(L, i, RM);
   return ns;
 }
-__host__ __device__ constexpr bool supported_length(int L) {
+__host__ __device__ constexpr bool supported_length(int L, int RM = 16) {
   int prod = 1;
-  for (int s = 0; s < num_stages(L); s++) prod *= radix_at(L, s);
+  for (int s = 0; s < num_stages(L, RM); s++) prod *= radix_at(L, s, RM);
   return prod == L && L >= 2;
 }
 
-// ------------------------------------------------------------ one stage
-// Tile access: element n of line b lives at s[b * SB + n * SN].
-// LINE_MAJOR: consecutive threads take consecutive butterflies of one line
-// (conflict-free when SN == 1); otherwise consecutive lines (SB == 1).
-template <int L, int R, int NS, int B, int T, int SB, int SN, bool LINE_MAJOR, int DIR>
-__device__ __forceinline__ void stage(cplx* s, const float2* __restrict__ tw) {
-  constexpr int NBF = L / R;
-  constexpr int TOTAL = NBF * B;
-  constexpr int PER = (TOTAL + T - 1) / T;
-  cplx v[PER][R];
-  const int tid = threadIdx.x;
-#pragma unroll
-  for (int q = 0; q < PER; q++) {
-    const int idx = tid + q * T;
-    if (TOTAL % T == 0 || idx < TOTAL) {
-      const int b = LINE_MAJOR ? idx / NBF : idx % B;
-      const int j = LINE_MAJOR ? idx % NBF : idx / B;
-#pragma unroll
-      for (int r = 0; r < R; r++) v[q][r] = s[b * SB + (j + r * NBF) * SN];
-    }
-  }
-  __syncthreads();
-#pragma unroll
-  for (int q = 0; q < PER; q++) {
-    const int idx = tid + q * T;
-    if (TOTAL % T == 0 || idx < TOTAL) {
-      const int b = LINE_MAJOR ? idx / NBF : idx % B;
-      const int j = LINE_MAJOR ? idx % NBF : idx / B;
-      const int jm = NS == 1 ? 0 : j % NS;
-      if (NS > 1) {
-        constexpr int STEP = L / (NS * R);
-#pragma unroll
-        for (int r = 1; r < R; r++) v[q][r] = cmul(v[q][r], twiddle<DIR>(tw, jm * r * STEP));
-      }
-      dft<R, DIR>(v[q]);
-      const int base = (j / NS) * NS * R + jm;
-#pragma unroll
-      for (int r = 0; r < R; r++) s[b * SB + (base + r * NS) * SN] = v[q][r];
-    }
-  }
-  __syncthreads();
-}
-
-template <int L, int S, int B, int T, int SB, int SN, bool LINE_MAJOR, int DIR>
-__device__ __forceinline__ void fft_from(cplx* s, const float2* __restrict__ tw) {
-  if constexpr (S < num_stages(L)) {
-    stage<L, radix_at(L, S), ns_before(L, S), B, T, SB, SN, LINE_MAJOR, DIR>(s, tw);
-    fft_from<L, S + 1, B, T, SB, SN, LINE_MAJOR, DIR>(s, tw);
-  }
-}
-
-// Full in-place FFT of B lines of length L held in shared memory.
-// The caller must __syncthreads() before (tile loaded); returns synchronised.
-template <int L, int B, int T, int SB, int SN, bool LINE_MAJOR, int DIR>
-__device__ __forceinline__ void fft_lines(cplx* s, const float2* __restrict__ tw) {
-  static_assert(supported_length(L), "FFT length must be 2^a 3^b");
-  fft_from<L, 0, B, T, SB, SN, LINE_MAJOR, DIR>(s, tw);
-}
-
-// =====================================================================
-// Direct-I/O variant: the first radix stage reads its butterfly legs
-// straight from global memory and the last stage writes straight to global
-// memory (both access patterns are j + r L/R, coalesced across consecutive
-// butterflies), so only the S-1 exchanges between stages go through shared
-// memory.  Shared-memory tiles are padded (one element per 16 along a line,
-// one per 32 in column-interleaved tiles) to spread the stride-R writes of
-// the early stages over the banks.
-// =====================================================================
+// ------------------------------------------------------------ tile access
+// The first stage reads its legs j + r L/R and the last writes its outputs
+// (j/NS) NS R + (j mod NS) + r NS; with consecutive threads on consecutive
+// butterflies of a line both are coalesced in global memory.  Shared tiles
+// are padded (one element per 16 along a line, one per 32 in
+// column-interleaved tiles) to spread the stride-R writes over the banks.
 
 // Line-major shared tile: element n of line b at b*SB + n + n/16.
 template <int SB>
@@ -236,7 +182,12 @@ struct SmemLine {
   __device__ __forceinline__ void st(int b, int n, cplx v) const { s[b * SB + n + (n >> 4)] = v; }
   static constexpr bool kShared = true;
 };
-template <int L> __host__ __device__ constexpr int line_pitch() { return L + L / 16 + 1; }
+// Line pitch >= the padded length, rounded to 1 (mod 16) elements: when
+// consecutive threads walk across lines (same n, consecutive b), the 8-byte
+// accesses then fall 2 words apart mod 32 banks -- conflict-free.
+template <int L> __host__ __device__ constexpr int line_pitch() {
+  return ((L + L / 16 + 1 + 14) / 16) * 16 + 1;
+}
 
 // Column-interleaved shared tile: element n of column b at i = n*B + b,
 // stored at i + i/32.
@@ -309,15 +260,17 @@ __device__ __forceinline__ void stage_io(const In& in, const Out& out,
   }
 }
 
-// Stages S0..end of an L-point FFT: stage S0 reads `first`, the last stage
-// writes `last`, stages in between work in place on shared tile `mid`.
-// Every stage that writes `mid` is followed by a barrier.
-template <int L, int S, int B, int T, bool LM, int DIR, class First, class Mid, class Last>
+// ------------------------------------------------------------ one pass
+// Stages S..end of an L-point FFT (maximum radix RM): stage 0 reads `first`,
+// the last stage writes `last`, the stages in between work in place on the
+// shared tile `mid`.  Every stage that writes `mid` is followed by a barrier.
+template <int L, int S, int B, int T, bool LM, int DIR, int RM, class First, class Mid,
+          class Last>
 __device__ __forceinline__ void fft_io_from(const First& first, const Mid& mid, const Last& last,
                                             const float2* __restrict__ tw) {
-  constexpr int NSTAGE = num_stages(L);
-  constexpr int R = radix_at(L, S);
-  constexpr int NS = ns_before(L, S);
+  constexpr int NSTAGE = num_stages(L, RM);
+  constexpr int R = radix_at(L, S, RM);
+  constexpr int NS = ns_before(L, S, RM);
   if constexpr (S == NSTAGE - 1) {
     if constexpr (S == 0)
       stage_io<L, R, NS, B, T, LM, DIR>(first, last, tw, First::kShared && Last::kShared);
@@ -330,15 +283,18 @@ __device__ __forceinline__ void fft_io_from(const First& first, const Mid& mid, 
     else
       stage_io<L, R, NS, B, T, LM, DIR>(mid, mid, tw, true);
     __syncthreads();
-    fft_io_from<L, S + 1, B, T, LM, DIR>(first, mid, last, tw);
+    fft_io_from<L, S + 1, B, T, LM, DIR, RM>(first, mid, last, tw);
   }
 }
 
-template <int L, int B, int T, bool LM, int DIR, class First, class Mid, class Last>
+// One L-point FFT of each of the B lines of a tile.  LM: consecutive threads
+// take consecutive butterflies of one line (true) or the same butterfly of
+// consecutive lines (false).  DIR = -1 forward, +1 inverse (unnormalised).
+template <int L, int B, int T, bool LM, int DIR, int RM = 16, class First, class Mid, class Last>
 __device__ __forceinline__ void fft_io(const First& first, const Mid& mid, const Last& last,
                                        const float2* __restrict__ tw) {
-  static_assert(supported_length(L), "FFT length must be 2^a 3^b");
-  fft_io_from<L, 0, B, T, LM, DIR>(first, mid, last, tw);
+  static_assert(supported_length(L, RM), "FFT length must be 2^a 3^b");
+  fft_io_from<L, 0, B, T, LM, DIR, RM>(first, mid, last, tw);
 }
 
 }  // namespace cgfft

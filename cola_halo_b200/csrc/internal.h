@@ -8,7 +8,7 @@
 
 // Stages of the step, for launch accounting and event timing (prof.cu).
 enum {
-  CG_ST_FILL = 0, CG_ST_DEPOSIT, CG_ST_FZ, CG_ST_FY_FWD, CG_ST_FX_GREEN, CG_ST_FY_INV,
+  CG_ST_FILL = 0, CG_ST_DEPOSIT, CG_ST_FZ, CG_ST_FX_FWD, CG_ST_GREEN, CG_ST_FX_INV,
   CG_ST_ZI, CG_ST_INTERP, CG_ST_WRAP, CG_ST_KICK, CG_ST_DRIFT, CG_ST_SNAPSHOT, CG_ST_LPT,
   CG_ST_OTHER, CG_ST_COUNT
 };
@@ -40,6 +40,10 @@ struct PmPlan {
   float2* twH;              // exp(-2 pi i k/(N/2)), k < N/2
   double* dsum;             // device: sum of the density mesh (check)
   double* pk_acc;           // device: 3 N doubles of power-spectrum bin sums
+  unsigned* keys;           // cell-sorted deposit: per-particle bin key
+  float4* sorted;           //   positions in bin order
+  unsigned* bins;           //   counts, offsets, cursors, scan block sums
+  long long sort_cap;       //   particles the two arrays above hold
   unsigned* err;            // device: error word
   size_t mesh_bytes;        // bytes of one real mesh
   size_t spec_bytes;        // bytes of one half spectrum
@@ -68,7 +72,12 @@ cudaError_t pm_forces(PmPlan* p, const float* const x[3], long long n,
                       float* const f[3], cudaStream_t st);
 // Individual stages (exposed for tests and timing).
 cudaError_t pm_deposit(PmPlan* p, const float* const x[3], long long n, cudaStream_t st);
+// deposit_tiled.cu: the same density mesh, each cell written once by the CTA
+// owning its 16^3 tile (particles binned by tile, warp-aggregated counts).
+cudaError_t pm_deposit_tiled(PmPlan* p, const float* const x[3], long long n, cudaStream_t st);
+// dens -> spec transformed along z and x (+ density sum into dsum)
 cudaError_t pm_r2c(PmPlan* p, cudaStream_t st);
+// spec -> y transform, Green/gradient -> three force meshes fmesh[a]
 cudaError_t pm_green_c2r(PmPlan* p, cudaStream_t st);
 // Power spectrum of the CIC density of x: deposit, r2c, shell sums into
 // acc[3 * nbins] (device doubles: sum w, sum w |n|, sum w |delta_k|^2).

@@ -10,13 +10,14 @@
 // Mesh layouts in HBM
 //   real   R[x][y][z]        N^3 floats, z contiguous, no padding
 //   half   S[kz][kx][ky]     (N/2+1) N N complex floats, ky contiguous
-// Transform passes (each one read + one write of a mesh):
-//   FZ   r2c along z of R, transposed store into S        (+ density sum)
-//   FY   c2c along ky, contiguous lines, in place
-//   FX   forward c2c along kx, Green/gradient for the 3 axes, inverse c2c
-//        along kx  -> three spectra G_a (one read, three writes)
-//   FY   inverse c2c along ky on each G_a
-//   ZI   c2r along z of G_a, transposed load, store R_a
+// Transform passes of the force (each one read + one write of a mesh):
+//   FZ     r2c along z of R, transposed store into S      (+ density sum)
+//   FX     forward c2c along kx (stride N), in place
+//   GREEN  forward c2c along ky (contiguous lines), Green/gradient, inverse
+//          c2c along ky -> three spectra G_a (one read, three writes)
+//   FX     inverse c2c along kx on each G_a, in place
+//   ZI     c2r along z of G_a, transposed load, store R_a
+// The plain 3-D transforms (mesh_r2c / mesh_c2r) run FZ, FY, FX and back.
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdio.h>
@@ -178,340 +179,34 @@ __global__ void __launch_bounds__(T) k_interp(const float* __restrict__ x0,
   }
 }
 
-// ------------------------------------------------------------- FZ: r2c z
-// One CTA: the TY z-lines (x, y0..y0+TY-1), contiguous in R.  Real FFT of
-// length N through a complex FFT of length H = N/2 on (x_2m + i x_2m+1):
-//   X_k = E_k + W_N^k O_k,  E_k = (Z_k + conj Z_{H-k})/2,
-//   O_k = -i (Z_k - conj Z_{H-k})/2,            k = 0..H
-// The sum of all mesh values (check_total_density, pm.c:535-562) is
-// accumulated in double on the way in.
-template <int N>
-__global__ void __launch_bounds__(T) k_fz_r2c(const float* __restrict__ dens,
-                                              float2* __restrict__ spec,
-                                              const float2* __restrict__ twH,
-                                              const float2* __restrict__ twN,
-                                              double* __restrict__ dsum) {
-  constexpr int H = N / 2;
-  constexpr int SB = H + 1;
-  extern __shared__ __align__(16) unsigned char smraw[];
-  cplx* sm = reinterpret_cast<cplx*>(smraw);
-  const int x = blockIdx.y;
-  const int y0 = blockIdx.x * TY;
-  const float2* src = reinterpret_cast<const float2*>(dens + ((size_t)x * N + y0) * N);
-  double acc = 0.0;
-  for (int idx = threadIdx.x; idx < TY * H; idx += T) {
-    const float2 v = src[idx];
-    const int b = idx / H, m = idx - (idx / H) * H;
-    sm[b * SB + m] = cplx{v.x, v.y};
-    acc += (double)v.x + (double)v.y;
-  }
-  // warp reduce, one atomic per warp
-  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-  if ((threadIdx.x & 31) == 0) atomicAdd(dsum, acc);
-  __syncthreads();
-  cgfft::fft_lines<H, TY, T, SB, 1, true, -1>(sm, twH);
-  for (int idx = threadIdx.x; idx < (H + 1) * TY; idx += T) {
-    const int b = idx % TY, k = idx / TY;
-    const cplx zk = sm[b * SB + (k == H ? 0 : k)];
-    const cplx zc0 = sm[b * SB + (k == 0 ? 0 : H - k)];
-    const cplx zc = {zc0.x, -zc0.y};
-    const cplx e = {0.5f * (zk.x + zc.x), 0.5f * (zk.y + zc.y)};
-    const cplx dlt = {zk.x - zc.x, zk.y - zc.y};
-    const cplx o = {0.5f * dlt.y, -0.5f * dlt.x};
-    const float2 w = __ldg(twN + k);
-    const cplx X = {e.x + (w.x * o.x - w.y * o.y), e.y + (w.x * o.y + w.y * o.x)};
-    spec[((size_t)k * N + x) * N + y0 + b] = make_float2(X.x, X.y);
-  }
-}
-
-// --------------------------------------------------- FY: c2c along y
-template <int N, int DIR>
-__global__ void __launch_bounds__(T) k_fy(float2* __restrict__ spec,
-                                          const float2* __restrict__ twN) {
-  extern __shared__ __align__(16) unsigned char smraw[];
-  cplx* sm = reinterpret_cast<cplx*>(smraw);
-  float4* g = reinterpret_cast<float4*>(spec + (size_t)blockIdx.x * BY * N);
-  float4* s4 = reinterpret_cast<float4*>(sm);
-  for (int idx = threadIdx.x; idx < BY * N / 2; idx += T) s4[idx] = g[idx];
-  __syncthreads();
-  cgfft::fft_lines<N, BY, T, N, 1, true, DIR>(sm, twN);
-  for (int idx = threadIdx.x; idx < BY * N / 2; idx += T) g[idx] = s4[idx];
-}
-
-// ------------------------------- FX: x forward + Green/gradient + x inverse
-// compute_force_mesh (pm.c:304-346):  F_a = i f2 delta_k,
-//   f2 = f1 / (K^2 + I0^2 + J0^2) * n_a,  f1 = -1/(N^3 2 pi/L),
-//   I0, J0 signed with the Nyquist index kept at +N/2, F(0,0,0) = 0.
-template <int N>
-__global__ void __launch_bounds__(T) k_fx_green(const float2* __restrict__ spec,
-                                                float2* __restrict__ g0,
-                                                float2* __restrict__ g1,
-                                                float2* __restrict__ g2,
-                                                const float2* __restrict__ twN, float f1) {
-  extern __shared__ __align__(16) unsigned char smraw[];
-  cplx* D = reinterpret_cast<cplx*>(smraw);
-  cplx* W = D + N * TK;
-  const int kz = blockIdx.y;
-  const int ky0 = blockIdx.x * TK;
-  const size_t plane = (size_t)kz * N * N;
-  for (int idx = threadIdx.x; idx < N * TK; idx += T) {
-    const int n = idx / TK, b = idx % TK;
-    const float2 v = spec[plane + (size_t)n * N + ky0 + b];
-    D[idx] = cplx{v.x, v.y};
-  }
-  __syncthreads();
-  cgfft::fft_lines<N, TK, T, 1, TK, false, -1>(D, twN);
-  float2* gout[3] = {g0, g1, g2};
-#pragma unroll 1
-  for (int a = 0; a < 3; a++) {
-    for (int idx = threadIdx.x; idx < N * TK; idx += T) {
-      const int n = idx / TK, b = idx % TK;
-      const int ky = ky0 + b;
-      const int I0 = n <= N / 2 ? n : n - N;
-      const int J0 = ky <= N / 2 ? ky : ky - N;
-      const int den = kz * kz + I0 * I0 + J0 * J0;
-      cplx out = {0.0f, 0.0f};
-      if (den != 0) {
-        const float di = a == 0 ? (float)I0 : (a == 1 ? (float)J0 : (float)kz);
-        const float f2 = __fmul_rn(__fdiv_rn(f1, (float)den), di);
-        const cplx p = D[idx];
-        out = cplx{-__fmul_rn(f2, p.y), __fmul_rn(f2, p.x)};
-      }
-      W[idx] = out;
-    }
-    __syncthreads();
-    cgfft::fft_lines<N, TK, T, 1, TK, false, 1>(W, twN);
-    float2* go = gout[a];
-    for (int idx = threadIdx.x; idx < N * TK; idx += T) {
-      const int n = idx / TK, b = idx % TK;
-      go[plane + (size_t)n * N + ky0 + b] = make_float2(W[idx].x, W[idx].y);
-    }
-    __syncthreads();
-  }
-}
-
-// ------------------------------------- FX plain: c2c along kx, in place
-template <int N, int DIR>
-__global__ void __launch_bounds__(T) k_fx_plain(float2* __restrict__ spec,
-                                                const float2* __restrict__ twN) {
-  extern __shared__ __align__(16) unsigned char smraw[];
-  cplx* D = reinterpret_cast<cplx*>(smraw);
-  const int kz = blockIdx.y;
-  const int ky0 = blockIdx.x * TK;
-  const size_t plane = (size_t)kz * N * N;
-  for (int idx = threadIdx.x; idx < N * TK; idx += T) {
-    const int n = idx / TK, b = idx % TK;
-    const float2 v = spec[plane + (size_t)n * N + ky0 + b];
-    D[idx] = cplx{v.x, v.y};
-  }
-  __syncthreads();
-  cgfft::fft_lines<N, TK, T, 1, TK, false, DIR>(D, twN);
-  for (int idx = threadIdx.x; idx < N * TK; idx += T) {
-    const int n = idx / TK, b = idx % TK;
-    spec[plane + (size_t)n * N + ky0 + b] = make_float2(D[idx].x, D[idx].y);
-  }
-}
-
-// ------------------------------------------------------------ ZI: c2r z
-// One CTA: lines (x, y0..y0+TY-1).  Half-complex convention (the FFTW c2r
-// the reference relies on): Im X_0 and Im X_{N/2} are ignored.
-//   Z_k = (X_k + conj X_{H-k}) + i W_N^{-k} (X_k - conj X_{H-k}),  k < H
-//   z = IDFT_H(Z),  x_2m = Re z_m,  x_2m+1 = Im z_m   (unnormalised)
-template <int N>
-__global__ void __launch_bounds__(T) k_zi_c2r(const float2* __restrict__ gsp,
-                                              float* __restrict__ out,
-                                              const float2* __restrict__ twH,
-                                              const float2* __restrict__ twN) {
-  constexpr int H = N / 2;
-  constexpr int SB = H + 1;
-  extern __shared__ __align__(16) unsigned char smraw[];
-  cplx* sm = reinterpret_cast<cplx*>(smraw);
-  const int x = blockIdx.y;
-  const int y0 = blockIdx.x * TY;
-  for (int idx = threadIdx.x; idx < (H + 1) * TY; idx += T) {
-    const int b = idx % TY, k = idx / TY;
-    const float2 v = gsp[((size_t)k * N + x) * N + y0 + b];
-    sm[b * SB + k] = cplx{v.x, v.y};
-  }
-  __syncthreads();
-  for (int idx = threadIdx.x; idx < (H / 2 + 1) * TY; idx += T) {
-    const int b = idx % TY, k = idx / TY;
-    cplx* L = sm + b * SB;
-    if (k == 0) {
-      const float x0 = L[0].x, xh = L[H].x;
-      L[0] = cplx{x0 + xh, x0 - xh};
-    } else {
-      const int k2 = H - k;
-      const cplx a = L[k], c = L[k2];
-      const float2 wa = __ldg(twN + k), wc = __ldg(twN + k2);
-      // i * conj(w) * d  with conj(w) = (w.x, -w.y)
-      const cplx sa = {a.x + c.x, a.y - c.y}, da = {a.x - c.x, a.y + c.y};
-      const cplx ra = {da.x * wa.x + da.y * wa.y, da.y * wa.x - da.x * wa.y};  // conj(w)*d
-      const cplx za = {sa.x - ra.y, sa.y + ra.x};                            // + i*ra
-      const cplx sc = {c.x + a.x, c.y - a.y}, dc = {c.x - a.x, c.y + a.y};
-      const cplx rc = {dc.x * wc.x + dc.y * wc.y, dc.y * wc.x - dc.x * wc.y};
-      const cplx zc = {sc.x - rc.y, sc.y + rc.x};
-      L[k] = za;
-      if (k2 != k) L[k2] = zc;
-    }
-  }
-  __syncthreads();
-  cgfft::fft_lines<H, TY, T, SB, 1, true, 1>(sm, twH);
-  float2* dst = reinterpret_cast<float2*>(out + ((size_t)x * N + y0) * N);
-  for (int idx = threadIdx.x; idx < TY * H; idx += T) {
-    const int b = idx / H, m = idx - (idx / H) * H;
-    const cplx v = sm[b * SB + m];
-    dst[idx] = make_float2(v.x, v.y);
-  }
-}
-
-// ====================================================================
-// Direct-I/O pass kernels (cgfft::fft_io): the first radix stage loads
-// straight from HBM, the last stores straight to HBM, and only the
-// exchanges between stages use the (padded) shared tile.
-// ====================================================================
+// ------------------------------------------------------------ FFT passes
+// Every pass: a CTA owns a tile of complete lines; the first radix stage
+// loads its legs straight from HBM, the last stage stores straight to HBM,
+// and only the exchanges between stages use the padded shared tile
+// (fft_core.cuh).
 using cgfft::Gmem;
 using cgfft::SmemCol;
 using cgfft::SmemLine;
 
-// ky columns per CTA of the fused Green pass: one radix-16 butterfly per
-// thread in the 16-point stages ((N/16) * TK <= 256) keeps the three
-// inverse transforms of the tile within the register budget.
-__host__ __device__ constexpr int tk_green(int N) { return N >= 768 ? 4 : TK; }
+// Maximum radix of the strided x passes and of the fused y pass: radix 8
+// keeps these kernels at two CTAs per SM from 768 up.
+__host__ __device__ constexpr int rm_x(int N) { return N >= 768 ? 8 : 16; }
+__host__ __device__ constexpr int rm_green(int N) { return N >= 768 ? 8 : 16; }
+constexpr int BYG = 8;   // lines per CTA of the fused y pass
 
-template <int N, int DIR>
-__global__ void __launch_bounds__(T) k_fy2(float2* __restrict__ spec,
-                                           const float2* __restrict__ twN) {
-  extern __shared__ __align__(16) unsigned char smraw[];
-  const SmemLine<cgfft::line_pitch<N>()> mid{reinterpret_cast<cplx*>(smraw)};
-  const Gmem g{spec + (size_t)blockIdx.x * BY * N, (size_t)N, 1};
-  cgfft::fft_io<N, BY, T, true, DIR>(g, mid, g, twN);
-}
-
-template <int N, int DIR>
-__global__ void __launch_bounds__(T) k_fx_plain2(float2* __restrict__ spec,
-                                                 const float2* __restrict__ twN) {
-  extern __shared__ __align__(16) unsigned char smraw[];
-  const SmemCol<TK> mid{reinterpret_cast<cplx*>(smraw)};
-  const Gmem g{spec + (size_t)blockIdx.y * N * N + blockIdx.x * TK, 1, (size_t)N};
-  cgfft::fft_io<N, TK, T, false, DIR>(g, mid, g, twN);
-}
-
+// FZ: r2c along z of R (TY z-lines (x, y0..y0+TY-1) per CTA) through a
+// complex FFT of length H = N/2 on (x_2m + i x_2m+1):
+//   X_k = E_k + W_N^k O_k,  E_k = (Z_k + conj Z_{H-k})/2,
+//   O_k = -i (Z_k - conj Z_{H-k})/2,            k = 0..H
+// stored transposed into S[kz][x][y].  The sum of the mesh
+// (check_total_density, pm.c:535-562) is the sum over lines of
+// Re Z_0 + Im Z_0, accumulated in double.
 template <int N>
-__global__ void __launch_bounds__(T) k_fx_green2(const float2* __restrict__ spec,
-                                                 float2* __restrict__ g0,
-                                                 float2* __restrict__ g1,
-                                                 float2* __restrict__ g2,
-                                                 const float2* __restrict__ twN, float f1) {
-  constexpr int TKG = tk_green(N);
-  extern __shared__ __align__(16) unsigned char smraw[];
-  constexpr int TILE = cgfft::col_tile_elems<N, TKG>();
-  const SmemCol<TKG> D{reinterpret_cast<cplx*>(smraw)};
-  const SmemCol<TKG> W{reinterpret_cast<cplx*>(smraw) + TILE};
-  const int kz = blockIdx.y;
-  const int ky0 = blockIdx.x * TKG;
-  const size_t off = (size_t)kz * N * N + ky0;
-  const Gmem gin{const_cast<float2*>(spec) + off, 1, (size_t)N};
-  cgfft::fft_io<N, TKG, T, false, -1>(gin, D, D, twN);
-  float2* gout[3] = {g0, g1, g2};
-#pragma unroll 1
-  for (int a = 0; a < 3; a++) {
-    for (int idx = threadIdx.x; idx < N * TKG; idx += T) {
-      const int n = idx / TKG, b = idx % TKG;
-      const int ky = ky0 + b;
-      const int I0 = n <= N / 2 ? n : n - N;
-      const int J0 = ky <= N / 2 ? ky : ky - N;
-      const int den = kz * kz + I0 * I0 + J0 * J0;
-      cplx out = {0.0f, 0.0f};
-      if (den != 0) {
-        const float di = a == 0 ? (float)I0 : (a == 1 ? (float)J0 : (float)kz);
-        const float f2 = __fmul_rn(__fdiv_rn(f1, (float)den), di);
-        const cplx p = D.ld(b, n);
-        out = cplx{-__fmul_rn(f2, p.y), __fmul_rn(f2, p.x)};
-      }
-      W.st(b, n, out);
-    }
-    __syncthreads();
-    const Gmem go{gout[a] + off, 1, (size_t)N};
-    cgfft::fft_io<N, TKG, T, false, 1>(W, W, go, twN);
-    __syncthreads();
-  }
-}
-
-// Store of an inverse-x-transformed column scaled for the y and z force
-// components: n_y = J0 is constant along an x line (fixed ky) and n_z = kz
-// is constant over the CTA, so IFFT_x(i f1 n_a/|n|^2 delta) =
-// n_a IFFT_x(i f1/|n|^2 delta) for a = y, z -- one inverse transform serves
-// both components.
-struct GmemYZ {
-  float2* gy;
-  float2* gz;
-  size_t es;
-  int ky0, N;
-  float fz;
-  __device__ __forceinline__ void st(int b, int n, cplx v) const {
-    const int ky = ky0 + b;
-    const float fy = (float)(ky <= N / 2 ? ky : ky - N);
-    gy[b + (size_t)n * es] = make_float2(v.x * fy, v.y * fy);
-    gz[b + (size_t)n * es] = make_float2(v.x * fz, v.y * fz);
-  }
-  static constexpr bool kShared = false;
-};
-
-template <int N>
-__global__ void __launch_bounds__(T) k_fx_green3(const float2* __restrict__ spec,
-                                                 float2* __restrict__ g0,
-                                                 float2* __restrict__ g1,
-                                                 float2* __restrict__ g2,
-                                                 const float2* __restrict__ twN, float f1) {
-  constexpr int TKG = tk_green(N);
-  extern __shared__ __align__(16) unsigned char smraw[];
-  constexpr int TILE = cgfft::col_tile_elems<N, TKG>();
-  const SmemCol<TKG> D{reinterpret_cast<cplx*>(smraw)};
-  const SmemCol<TKG> W{reinterpret_cast<cplx*>(smraw) + TILE};
-  const int kz = blockIdx.y;
-  const int ky0 = blockIdx.x * TKG;
-  const size_t off = (size_t)kz * N * N + ky0;
-  const Gmem gin{const_cast<float2*>(spec) + off, 1, (size_t)N};
-  cgfft::fft_io<N, TKG, T, false, -1>(gin, D, D, twN);
-#pragma unroll 1
-  for (int pass = 0; pass < 2; pass++) {
-    // pass 0: x component i f1 n_x/|n|^2 delta;  pass 1: i f1/|n|^2 delta
-    for (int idx = threadIdx.x; idx < N * TKG; idx += T) {
-      const int n = idx / TKG, b = idx % TKG;
-      const int ky = ky0 + b;
-      const int I0 = n <= N / 2 ? n : n - N;
-      const int J0 = ky <= N / 2 ? ky : ky - N;
-      const int den = kz * kz + I0 * I0 + J0 * J0;
-      cplx out = {0.0f, 0.0f};
-      if (den != 0) {
-        float f2 = __fdiv_rn(f1, (float)den);
-        if (pass == 0) f2 = __fmul_rn(f2, (float)I0);
-        const cplx p = D.ld(b, n);
-        out = cplx{-__fmul_rn(f2, p.y), __fmul_rn(f2, p.x)};
-      }
-      W.st(b, n, out);
-    }
-    __syncthreads();
-    if (pass == 0) {
-      const Gmem go{g0 + off, 1, (size_t)N};
-      cgfft::fft_io<N, TKG, T, false, 1>(W, W, go, twN);
-    } else {
-      const GmemYZ go{g1 + off, g2 + off, (size_t)N, ky0, N, (float)kz};
-      cgfft::fft_io<N, TKG, T, false, 1>(W, W, go, twN);
-    }
-    __syncthreads();
-  }
-}
-
-// r2c along z; the density sum is the sum over lines of X_0 (the plain sum
-// of each line, formed by the transform) accumulated in double.
-template <int N>
-__global__ void __launch_bounds__(T) k_fz2(const float* __restrict__ dens,
-                                           float2* __restrict__ spec,
-                                           const float2* __restrict__ twH,
-                                           const float2* __restrict__ twN,
-                                           double* __restrict__ dsum) {
+__global__ void __launch_bounds__(T) k_fz(const float* __restrict__ dens,
+                                          float2* __restrict__ spec,
+                                          const float2* __restrict__ twH,
+                                          const float2* __restrict__ twN,
+                                          double* __restrict__ dsum) {
   constexpr int H = N / 2;
   extern __shared__ __align__(16) unsigned char smraw[];
   const SmemLine<cgfft::line_pitch<H>()> mid{reinterpret_cast<cplx*>(smraw)};
@@ -538,21 +233,133 @@ __global__ void __launch_bounds__(T) k_fz2(const float* __restrict__ dens,
   if ((threadIdx.x & 31) == 0 && acc != 0.0) atomicAdd(dsum, acc);
 }
 
-template <int N>
-__global__ void __launch_bounds__(T) k_zi2(const float2* __restrict__ gsp,
-                                           float* __restrict__ out,
-                                           const float2* __restrict__ twH,
-                                           const float2* __restrict__ twN) {
-  constexpr int H = N / 2;
+// FY: c2c along ky, BY contiguous lines per CTA, in place.
+template <int N, int DIR>
+__global__ void __launch_bounds__(T) k_fy(float2* __restrict__ spec,
+                                          const float2* __restrict__ twN) {
   extern __shared__ __align__(16) unsigned char smraw[];
-  const SmemLine<cgfft::line_pitch<H + 1>()> mid{reinterpret_cast<cplx*>(smraw)};
+  const SmemLine<cgfft::line_pitch<N>()> mid{reinterpret_cast<cplx*>(smraw)};
+  const Gmem g{spec + (size_t)blockIdx.x * BY * N, (size_t)N, 1};
+  cgfft::fft_io<N, BY, T, true, DIR>(g, mid, g, twN);
+}
+
+// FX: c2c along kx (stride N), TK ky columns per CTA, in place.
+template <int N, int DIR>
+__global__ void __launch_bounds__(T) k_fx(float2* __restrict__ spec,
+                                          const float2* __restrict__ twN) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const SmemCol<TK> mid{reinterpret_cast<cplx*>(smraw)};
+  const Gmem g{spec + (size_t)blockIdx.y * N * N + blockIdx.x * TK, 1, (size_t)N};
+  cgfft::fft_io<N, TK, T, false, DIR, rm_x(N)>(g, mid, g, twN);
+}
+
+// compute_force_mesh (pm.c:304-346) on lines (kz, kx) that are already
+// transformed along z and x:  F_a = i f2 delta_k,
+//   f2 = f1 / (K^2 + I0^2 + J0^2) * n_a,  f1 = -1/(N^3 2 pi/L),
+//   I0, J0 signed with the Nyquist index kept at +N/2, F(0,0,0) = 0.
+// GreenLoad applies the factor while the first inverse stage loads the
+// forward-transformed tile: MODE 0 the y component (n_y = J0, the position
+// along the line), MODE 1 the factor without n_a.
+template <int P, int MODE>
+struct GreenLoad {
+  cplx* s;
+  int kz, kx0, N;
+  float f1;
+  __device__ __forceinline__ cplx ld(int b, int n) const {
+    const cplx p = s[b * P + n + (n >> 4)];
+    const int kx = kx0 + b;
+    const int I0 = kx <= N / 2 ? kx : kx - N;
+    const int J0 = n <= N / 2 ? n : n - N;
+    const int den = kz * kz + I0 * I0 + J0 * J0;
+    if (den == 0) return cplx{0.0f, 0.0f};
+    float f2 = __fdiv_rn(f1, (float)den);
+    if (MODE == 0) f2 = __fmul_rn(f2, (float)J0);
+    return cplx{-__fmul_rn(f2, p.y), __fmul_rn(f2, p.x)};
+  }
+  static constexpr bool kShared = true;
+};
+
+// n_x = I0 and n_z = kz are constant along a y line, so
+// IFFT_y(i f1 n_a/|n|^2 delta) = n_a IFFT_y(i f1/|n|^2 delta) for a = x, z:
+// one inverse transform serves both components.
+struct GmemXZ {
+  float2* gx;
+  float2* gz;
+  int kx0, N;
+  float fz;
+  __device__ __forceinline__ void st(int b, int n, cplx v) const {
+    const int kx = kx0 + b;
+    const float fx = (float)(kx <= N / 2 ? kx : kx - N);
+    gx[(size_t)b * N + n] = make_float2(v.x * fx, v.y * fx);
+    gz[(size_t)b * N + n] = make_float2(v.x * fz, v.y * fz);
+  }
+  static constexpr bool kShared = false;
+};
+
+// The three transforms of the fused pass as separate (not inlined) calls:
+// each keeps its own register live range, so the kernel fits two CTAs per SM.
+template <int N, int DIR, class First, class Mid, class Last>
+__device__ __noinline__ void fft_tile_y(const First f, const Mid m, const Last l,
+                                        const float2* __restrict__ tw) {
+  cgfft::fft_io<N, BYG, T, true, DIR, rm_green(N)>(f, m, l, tw);
+}
+
+// GREEN: forward c2c along ky, Green/gradient, inverse c2c along ky for the
+// y component and for the shared x/z factor: spec -> g0 (x), g1 (y), g2 (z).
+// BYG lines (kz, kx0 .. kx0+BYG-1) per CTA; N is a multiple of BYG so the
+// lines of a CTA share kz.
+template <int N>
+__global__ void __launch_bounds__(T, 2) k_green(const float2* __restrict__ spec,
+                                                float2* __restrict__ g0,
+                                                float2* __restrict__ g1,
+                                                float2* __restrict__ g2,
+                                                const float2* __restrict__ twN, float f1) {
+  constexpr int P = cgfft::line_pitch<N>();
+  extern __shared__ __align__(16) unsigned char smraw[];
+  cplx* D = reinterpret_cast<cplx*>(smraw);
+  cplx* W = D + BYG * P;
+  const size_t l0 = (size_t)blockIdx.x * BYG;
+  const int kz = (int)(l0 / N);
+  const int kx0 = (int)(l0 % N);
+  const size_t off = l0 * N;
+  const Gmem gin{const_cast<float2*>(spec) + off, (size_t)N, 1};
+  const SmemLine<P> d{D}, w{W};
+  fft_tile_y<N, -1>(gin, d, d, twN);
+  const GreenLoad<P, 0> gy{D, kz, kx0, N, f1};
+  const Gmem oy{g1 + off, (size_t)N, 1};
+  fft_tile_y<N, 1>(gy, w, oy, twN);
+  __syncthreads();
+  const GreenLoad<P, 1> gs{D, kz, kx0, N, f1};
+  const GmemXZ oxz{g0 + off, g2 + off, kx0, N, (float)kz};
+  fft_tile_y<N, 1>(gs, d, oxz, twN);
+}
+
+// ZI: c2r along z of S (lines (x, y0..y0+TY-1) per CTA) into R.  The
+// transposed tile is gathered with cp.async (8-byte copies, no register
+// staging).  Half-complex convention (the FFTW c2r the reference relies
+// on): Im X_0 and Im X_{N/2} are ignored.
+//   Z_k = (X_k + conj X_{H-k}) + i W_N^{-k} (X_k - conj X_{H-k}),  k < H
+//   z = IDFT_H(Z),  x_2m = Re z_m,  x_2m+1 = Im z_m   (unnormalised)
+template <int N>
+__global__ void __launch_bounds__(T) k_zi(const float2* __restrict__ gsp,
+                                          float* __restrict__ out,
+                                          const float2* __restrict__ twH,
+                                          const float2* __restrict__ twN) {
+  constexpr int H = N / 2;
+  constexpr int PZ = cgfft::line_pitch<H + 1>();
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const SmemLine<PZ> mid{reinterpret_cast<cplx*>(smraw)};
   const int x = blockIdx.y;
   const int y0 = blockIdx.x * TY;
+  const unsigned sbase = (unsigned)__cvta_generic_to_shared(smraw);
   for (int idx = threadIdx.x; idx < (H + 1) * TY; idx += T) {
     const int b = idx % TY, k = idx / TY;
-    const float2 v = gsp[((size_t)k * N + x) * N + y0 + b];
-    mid.st(b, k, cplx{v.x, v.y});
+    const float2* src = gsp + ((size_t)k * N + x) * N + y0 + b;
+    const unsigned dst = sbase + 8u * (unsigned)(b * PZ + k + (k >> 4));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(src) : "memory");
   }
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
   __syncthreads();
   for (int idx = threadIdx.x; idx < (H / 2 + 1) * TY; idx += T) {
     const int b = idx % TY, k = idx / TY;
@@ -563,6 +370,7 @@ __global__ void __launch_bounds__(T) k_zi2(const float2* __restrict__ gsp,
       const int k2 = H - k;
       const cplx a = mid.ld(b, k), c = mid.ld(b, k2);
       const float2 wa = __ldg(twN + k), wc = __ldg(twN + k2);
+      // i * conj(w) * d  with conj(w) = (w.x, -w.y)
       const cplx sa = {a.x + c.x, a.y - c.y}, da = {a.x - c.x, a.y + c.y};
       const cplx ra = {da.x * wa.x + da.y * wa.y, da.y * wa.x - da.x * wa.y};
       const cplx za = {sa.x - ra.y, sa.y + ra.x};
@@ -630,48 +438,27 @@ struct MeshKernels {
   void (*fz)(const float*, float2*, const float2*, const float2*, double*);
   void (*fyf)(float2*, const float2*);
   void (*fyi)(float2*, const float2*);
-  void (*fx)(const float2*, float2*, float2*, float2*, const float2*, float);
+  void (*fxf)(float2*, const float2*);
+  void (*fxi)(float2*, const float2*);
+  void (*green)(const float2*, float2*, float2*, float2*, const float2*, float);
   void (*zi)(const float2*, float*, const float2*, const float2*);
-  void (*fxpf)(float2*, const float2*);
-  void (*fxpi)(float2*, const float2*);
-  size_t sm_fz, sm_fy, sm_fx, sm_zi, sm_fxp;
-  int tkx;   // ky columns per CTA of the fx (Green) kernel
+  size_t sm_fz, sm_fy, sm_fx, sm_green, sm_zi;
 };
 
 template <int N>
 MeshKernels make_kernels() {
   MeshKernels k;
-  static const bool v1 = getenv("COLAGPU_FFT_V1") && getenv("COLAGPU_FFT_V1")[0] == '1';
-  if (v1) {
-    // shared-memory staged passes (every stage goes through the tile)
-    k.fz = k_fz_r2c<N>;
-    k.fyf = k_fy<N, -1>;
-    k.fyi = k_fy<N, 1>;
-    k.fx = k_fx_green<N>;
-    k.zi = k_zi_c2r<N>;
-    k.fxpf = k_fx_plain<N, -1>;
-    k.fxpi = k_fx_plain<N, 1>;
-    k.sm_fxp = sizeof(cplx) * N * TK;
-    k.sm_fz = sizeof(cplx) * TY * (N / 2 + 1);
-    k.sm_fy = sizeof(cplx) * BY * N;
-    k.sm_fx = sizeof(cplx) * 2 * N * TK;
-    k.sm_zi = sizeof(cplx) * TY * (N / 2 + 1);
-    k.tkx = TK;
-    return k;
-  }
-  k.fz = k_fz2<N>;
-  k.fyf = k_fy2<N, -1>;
-  k.fyi = k_fy2<N, 1>;
-  static const bool green3 = !(getenv("COLAGPU_GREEN3") && getenv("COLAGPU_GREEN3")[0] == '0');
-  k.fx = green3 ? k_fx_green3<N> : k_fx_green2<N>;
-  k.zi = k_zi2<N>;
-  k.fxpf = k_fx_plain2<N, -1>;
-  k.fxpi = k_fx_plain2<N, 1>;
-  k.sm_fxp = sizeof(cplx) * cgfft::col_tile_elems<N, TK>();
+  k.fz = k_fz<N>;
+  k.fyf = k_fy<N, -1>;
+  k.fyi = k_fy<N, 1>;
+  k.fxf = k_fx<N, -1>;
+  k.fxi = k_fx<N, 1>;
+  k.green = k_green<N>;
+  k.zi = k_zi<N>;
   k.sm_fz = sizeof(cplx) * TY * cgfft::line_pitch<N / 2>();
   k.sm_fy = sizeof(cplx) * BY * cgfft::line_pitch<N>();
-  k.sm_fx = sizeof(cplx) * 2 * cgfft::col_tile_elems<N, tk_green(N)>();
-  k.tkx = tk_green(N);
+  k.sm_fx = sizeof(cplx) * cgfft::col_tile_elems<N, TK>();
+  k.sm_green = sizeof(cplx) * 2 * BYG * cgfft::line_pitch<N>();
   k.sm_zi = sizeof(cplx) * TY * cgfft::line_pitch<N / 2 + 1>();
   return k;
 }
@@ -689,6 +476,18 @@ bool get_kernels(int N, MeshKernels* out) {
 
 cudaError_t set_smem(const void* fn, size_t bytes) {
   return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+// Dynamic shared-memory limits of every pass kernel of one mesh size.
+cudaError_t set_all_smem(const MeshKernels& k) {
+  cudaError_t e = set_smem((const void*)k.fz, k.sm_fz);
+  if (e == cudaSuccess) e = set_smem((const void*)k.fyf, k.sm_fy);
+  if (e == cudaSuccess) e = set_smem((const void*)k.fyi, k.sm_fy);
+  if (e == cudaSuccess) e = set_smem((const void*)k.fxf, k.sm_fx);
+  if (e == cudaSuccess) e = set_smem((const void*)k.fxi, k.sm_fx);
+  if (e == cudaSuccess) e = set_smem((const void*)k.green, k.sm_green);
+  if (e == cudaSuccess) e = set_smem((const void*)k.zi, k.sm_zi);
+  return e;
 }
 
 void twiddle_table(float2* h, int L) {
@@ -758,13 +557,7 @@ cudaError_t pm_plan_alloc(PmPlan* p, int N, int factor, float L) {
   }
   CG_TRY(cudaMemset(p->dsum, 0, sizeof(double)));
   CG_TRY(cudaMemset(p->err, 0, sizeof(unsigned)));
-  CG_TRY(set_smem((const void*)k.fz, k.sm_fz));
-  CG_TRY(set_smem((const void*)k.fyf, k.sm_fy));
-  CG_TRY(set_smem((const void*)k.fyi, k.sm_fy));
-  CG_TRY(set_smem((const void*)k.fx, k.sm_fx));
-  CG_TRY(set_smem((const void*)k.zi, k.sm_zi));
-  CG_TRY(set_smem((const void*)k.fxpf, k.sm_fxp));
-  CG_TRY(set_smem((const void*)k.fxpi, k.sm_fxp));
+  CG_TRY(set_all_smem(k));
 #undef CG_TRY
   return cudaSuccess;
 }
@@ -785,12 +578,7 @@ cudaError_t mesh_fft_alloc(MeshFFT* f, int N) {
     if (e == cudaSuccess) e = cudaMemcpy(f->twH, h, sizeof(float2) * (N / 2), cudaMemcpyHostToDevice);
     free(h);
   }
-  if (e == cudaSuccess) e = set_smem((const void*)k.fz, k.sm_fz);
-  if (e == cudaSuccess) e = set_smem((const void*)k.fyf, k.sm_fy);
-  if (e == cudaSuccess) e = set_smem((const void*)k.fyi, k.sm_fy);
-  if (e == cudaSuccess) e = set_smem((const void*)k.zi, k.sm_zi);
-  if (e == cudaSuccess) e = set_smem((const void*)k.fxpf, k.sm_fxp);
-  if (e == cudaSuccess) e = set_smem((const void*)k.fxpi, k.sm_fxp);
+  if (e == cudaSuccess) e = set_all_smem(k);
   if (e != cudaSuccess) mesh_fft_free(f);
   return e;
 }
@@ -808,10 +596,10 @@ cudaError_t mesh_r2c(const MeshFFT* f, const float* real, float2* spec, cudaStre
   const int N = f->N;
   prof_mark(st, CG_ST_FZ);
   k.fz<<<dim3(N / TY, N), T, k.sm_fz, st>>>(real, spec, f->twH, f->twN, f->dsum);
-  prof_mark(st, CG_ST_FY_FWD);
-  k.fyf<<<(N / 2 + 1) * N / BY, T, k.sm_fy, st>>>(spec, f->twN);
   prof_mark(st, CG_ST_OTHER);
-  k.fxpf<<<dim3(N / TK, N / 2 + 1), T, k.sm_fxp, st>>>(spec, f->twN);
+  k.fyf<<<(N / 2 + 1) * N / BY, T, k.sm_fy, st>>>(spec, f->twN);
+  prof_mark(st, CG_ST_FX_FWD);
+  k.fxf<<<dim3(N / TK, N / 2 + 1), T, k.sm_fx, st>>>(spec, f->twN);
   return cudaGetLastError();
 }
 
@@ -819,9 +607,9 @@ cudaError_t mesh_c2r(const MeshFFT* f, float2* spec, float* real, cudaStream_t s
   MeshKernels k;
   if (!get_kernels(f->N, &k)) return cudaErrorInvalidValue;
   const int N = f->N;
+  prof_mark(st, CG_ST_FX_INV);
+  k.fxi<<<dim3(N / TK, N / 2 + 1), T, k.sm_fx, st>>>(spec, f->twN);
   prof_mark(st, CG_ST_OTHER);
-  k.fxpi<<<dim3(N / TK, N / 2 + 1), T, k.sm_fxp, st>>>(spec, f->twN);
-  prof_mark(st, CG_ST_FY_INV);
   k.fyi<<<(N / 2 + 1) * N / BY, T, k.sm_fy, st>>>(spec, f->twN);
   prof_mark(st, CG_ST_ZI);
   k.zi<<<dim3(N / TY, N), T, k.sm_zi, st>>>(spec, real, f->twH, f->twN);
@@ -839,18 +627,31 @@ void pm_plan_free(PmPlan* p) {
   cudaFree(p->twH);
   cudaFree(p->dsum);
   cudaFree(p->pk_acc);
+  cudaFree(p->keys);
+  cudaFree(p->sorted);
+  cudaFree(p->bins);
   cudaFree(p->err);
   memset(p, 0, sizeof(*p));
 }
 
 cudaError_t pm_deposit(PmPlan* p, const float* const x[3], long long n, cudaStream_t st) {
+  // COLAGPU_DEPOSIT=tiled selects the cell-sorted deposit (deposit_tiled.cu);
+  // the default global-atomic scatter measured faster at 256^3 / 768^3.
+  static const bool tiled_deposit =
+      getenv("COLAGPU_DEPOSIT") && getenv("COLAGPU_DEPOSIT")[0] == 't';
+  if (tiled_deposit) {
+    cudaError_t e = pm_deposit_tiled(p, x, n, st);
+    if (e != cudaErrorNotSupported) return e;
+  }
+  // scatter with global float atomics into a mesh filled with -1
   const size_t n4 = (size_t)p->N * p->N * p->N / 4;
   prof_mark(st, CG_ST_FILL);
   k_fill<<<grid_for((long long)n4), T, 0, st>>>(reinterpret_cast<float4*>(p->dens), n4, -1.0f);
-  if (n > 0)
+  if (n > 0) {
     prof_mark(st, CG_ST_DEPOSIT);
     k_deposit<<<grid_for(n), T, 0, st>>>(x[0], x[1], x[2], n, p->dens, p->N, p->scale,
                                          p->wpar, p->x_right, p->shiftx, p->err);
+  }
   return cudaGetLastError();
 }
 
@@ -861,8 +662,8 @@ cudaError_t pm_r2c(PmPlan* p, cudaStream_t st) {
   cudaMemsetAsync(p->dsum, 0, sizeof(double), st);
   prof_mark(st, CG_ST_FZ);
   k.fz<<<dim3(N / TY, N), T, k.sm_fz, st>>>(p->dens, p->spec, p->twH, p->twN, p->dsum);
-  prof_mark(st, CG_ST_FY_FWD);
-  k.fyf<<<(N / 2 + 1) * N / BY, T, k.sm_fy, st>>>(p->spec, p->twN);
+  prof_mark(st, CG_ST_FX_FWD);
+  k.fxf<<<dim3(N / TK, N / 2 + 1), T, k.sm_fx, st>>>(p->spec, p->twN);
   return cudaGetLastError();
 }
 
@@ -870,12 +671,12 @@ cudaError_t pm_green_c2r(PmPlan* p, cudaStream_t st) {
   MeshKernels k;
   get_kernels(p->N, &k);
   const int N = p->N;
-  prof_mark(st, CG_ST_FX_GREEN);
-  k.fx<<<dim3(N / k.tkx, N / 2 + 1), T, k.sm_fx, st>>>(p->spec, p->gsp[0], p->gsp[1], p->gsp[2],
-                                                     p->twN, p->f1);
+  prof_mark(st, CG_ST_GREEN);
+  k.green<<<(N / 2 + 1) * N / BYG, T, k.sm_green, st>>>(p->spec, p->gsp[0], p->gsp[1],
+                                                         p->gsp[2], p->twN, p->f1);
   for (int a = 0; a < 3; a++) {
-    prof_mark(st, CG_ST_FY_INV);
-    k.fyi<<<(N / 2 + 1) * N / BY, T, k.sm_fy, st>>>(p->gsp[a], p->twN);
+    prof_mark(st, CG_ST_FX_INV);
+    k.fxi<<<dim3(N / TK, N / 2 + 1), T, k.sm_fx, st>>>(p->gsp[a], p->twN);
     prof_mark(st, CG_ST_ZI);
     k.zi<<<dim3(N / TY, N), T, k.sm_zi, st>>>(p->gsp[a], p->fmesh[a], p->twH, p->twN);
   }
@@ -884,11 +685,12 @@ cudaError_t pm_green_c2r(PmPlan* p, cudaStream_t st) {
 
 cudaError_t pm_interp(PmPlan* p, const float* const x[3], long long n, float* const f[3],
                       cudaStream_t st) {
-  if (n > 0)
+  if (n > 0) {
     prof_mark(st, CG_ST_INTERP);
     k_interp<<<grid_for(n), T, 0, st>>>(x[0], x[1], x[2], n, p->fmesh[0], p->fmesh[1],
                                         p->fmesh[2], f[0], f[1], f[2], p->N, p->scale,
                                         p->x_right, p->shiftx);
+  }
   return cudaGetLastError();
 }
 
@@ -912,10 +714,10 @@ cudaError_t pm_power_spectrum(PmPlan* p, const float* const x[3], long long n, i
   cudaMemsetAsync(p->dsum, 0, sizeof(double), st);
   prof_mark(st, CG_ST_FZ);
   k.fz<<<dim3(N / TY, N), T, k.sm_fz, st>>>(p->dens, p->spec, p->twH, p->twN, p->dsum);
-  prof_mark(st, CG_ST_FY_FWD);
-  k.fyf<<<(N / 2 + 1) * N / BY, T, k.sm_fy, st>>>(p->spec, p->twN);
+  prof_mark(st, CG_ST_FX_FWD);
+  k.fxf<<<dim3(N / TK, N / 2 + 1), T, k.sm_fx, st>>>(p->spec, p->twN);
   prof_mark(st, CG_ST_OTHER);
-  k.fxpf<<<dim3(N / TK, N / 2 + 1), T, k.sm_fxp, st>>>(p->spec, p->twN);
+  k.fyf<<<(N / 2 + 1) * N / BY, T, k.sm_fy, st>>>(p->spec, p->twN);
   cudaMemsetAsync(acc, 0, sizeof(double) * 3 * nbins, st);
   prof_mark(st, CG_ST_OTHER);
   k_pk_bin<<<grid_for((long long)(N / 2 + 1) * N * N), T, sizeof(double) * 3 * nbins, st>>>(

@@ -27,8 +27,8 @@ struct Profile {
 };
 Profile g_prof;
 
-const char* kNames[CG_ST_COUNT] = {"fill", "deposit", "fz_r2c", "fy_fwd", "fx_green",
-                                    "fy_inv", "zi_c2r", "interp", "wrap", "kick",
+const char* kNames[CG_ST_COUNT] = {"fill", "deposit", "fz_r2c", "fx_fwd", "green_y",
+                                    "fx_inv", "zi_c2r", "interp", "wrap", "kick",
                                     "drift", "snapshot", "lpt", "other"};
 }  // namespace
 

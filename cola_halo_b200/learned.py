@@ -80,3 +80,107 @@ class ConvNet:
 
 def copy_particles(dst, src):
     _lib.check(_lib.load().cg_sim_copy_particles(dst.h, src.h), "cg_sim_copy_particles")
+
+
+def _lpt_particles(nc, boxsize, seed, omega_m, a_init, table):
+    """2LPT particles of one seed from the GPU drop-in lpt_set_displacement."""
+    from .types import HostParticles
+    lib = _lib.load()
+    lib.cg_dropin_set_abort(0)
+    lib.power_init(table.encode(), a_init, 0.81, omega_m, 1 - omega_m)
+    lib.lpt_init(nc, None, 0)
+    hp = HostParticles(nc)
+    rc = lib.lpt_set_displacement(a_init, omega_m, seed, boxsize, hp.ptr)
+    if rc != 0:
+        raise _lib.ColaGpuError(lib.cg_last_error().decode())
+    return hp.local().copy()
+
+
+def train_online(net, coarse, fine, sched, seeds, table, *, lr=2e-3, epochs=1,
+                 steps_per_state=1, omega_m=0.273, log=None):
+    """Train on PM-generated pairs along fine-mesh trajectories: for each
+    seed and each time step, copy the fine run's particles to the coarse
+    realization and take `steps_per_state` optimiser steps on
+    (coarse features, fine - coarse force).  Returns the loss history."""
+    hist = []
+    for ep in range(epochs):
+        for seed in seeds:
+            p = _lpt_particles(fine.nc, fine.boxsize, seed, omega_m, sched.a_init, table)
+            fine.set_particles(p, sched.a_init, sched.a_init)
+            for i in range(1, sched.nloop):
+                _, _, avel1, apos1 = sched.times(i)
+                fine.move()
+                copy_particles(coarse, fine)
+                for _ in range(steps_per_state):
+                    hist.append(net.train_step(coarse, fine, lr))
+                # train_step left the fine forces of these positions in `fine`
+                fine.kick(avel1)
+                fine.drift(apos1)
+            if log:
+                log("epoch %d seed %d loss %.4g" % (ep, seed, hist[-1]))
+    return hist
+
+
+def power_spectrum_on(sim_pk, snap_x, a):
+    """P(k) of snapshot positions measured with realization sim_pk's mesh
+    (CIC window deconvolved, shot noise subtracted)."""
+    from .types import PARTICLE_DTYPE
+    p = np.zeros(len(snap_x), dtype=PARTICLE_DTYPE)
+    p["x"] = snap_x
+    p["id"] = np.arange(1, len(p) + 1)
+    sim_pk.set_particles(p, a, a)
+    sim_pk.move()
+    return sim_pk.power_spectrum(deconvolve_cic=True, subtract_shot=True)
+
+
+def pk_error(k, p, p_ref, kmax):
+    """max over bins with 0 < k <= kmax of |P/P_ref - 1|."""
+    ok = (k > 0) & (k <= kmax) & (p_ref > 0)
+    return float(np.max(np.abs(p[ok] / p_ref[ok] - 1.0)))
+
+
+def evaluate(nc, boxsize, sched, net, train_seeds, eval_seeds, table, *, omega_m=0.273,
+             epochs=1, lr=2e-3, log=None):
+    """Train on PM pairs, then judge plain-coarse and learned-coarse runs
+    against the plain factor-3 run on held-out seeds: P(k) error up to half
+    the particle Nyquist wavenumber, and device wall time per run."""
+    import time
+
+    from .sim import Simulation
+    fine = Simulation(nc, 3 * nc, boxsize, omega_m)
+    coarse = Simulation(nc, nc, boxsize, omega_m)
+    t0 = time.perf_counter()
+    hist = train_online(net, coarse, fine, sched, train_seeds, table, lr=lr, epochs=epochs,
+                        omega_m=omega_m, log=log)
+    train_s = time.perf_counter() - t0
+    kmax = 0.5 * np.pi * nc / boxsize
+    res = {"train_s": train_s, "train_steps": len(hist), "loss_first": float(np.mean(hist[:10])),
+           "loss_last": float(np.mean(hist[-10:])), "seeds": []}
+
+    def timed(fn):
+        fine.sync()
+        coarse.sync()
+        t = time.perf_counter()
+        out = fn()
+        fine.sync()
+        coarse.sync()
+        return out, time.perf_counter() - t
+    for seed in eval_seeds:
+        p = _lpt_particles(nc, boxsize, seed, omega_m, sched.a_init, table)
+        fine.set_particles(p, sched.a_init, sched.a_init)
+        s_f, t_f = timed(lambda: fine.run(sched)[-1][1])
+        coarse.set_particles(p, sched.a_init, sched.a_init)
+        s_c, t_c = timed(lambda: coarse.run(sched)[-1][1])
+        coarse.set_particles(p, sched.a_init, sched.a_init)
+        s_l, t_l = timed(lambda: net.run(coarse, sched)[-1][1])
+        k, pf, _ = power_spectrum_on(fine, s_f["x"], 1.0)
+        _, pc, _ = power_spectrum_on(fine, s_c["x"], 1.0)
+        _, pl, _ = power_spectrum_on(fine, s_l["x"], 1.0)
+        r = {"seed": seed, "fine_s": t_f, "coarse_s": t_c, "learned_s": t_l,
+             "err_coarse": pk_error(k, pc, pf, kmax), "err_learned": pk_error(k, pl, pf, kmax)}
+        res["seeds"].append(r)
+        if log:
+            log(str(r))
+    fine.close()
+    coarse.close()
+    return res

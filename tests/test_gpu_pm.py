@@ -65,7 +65,10 @@ def test_single_particle_mass(gpu_lib):
     nc, factor, L = 16, 3, 48.0
     N = nc * factor
     sim = Simulation(nc, N, L, OM, np_capacity=nc ** 3)
-    for xyz in ([10.3, 20.7, 5.5], [47.6, 0.2, 47.9], [0.0, 47.99, 13.0]):
+    # interior; last x/z cells (buffer copy, periodic z); tile edges (cells
+    # 15/16 of the 16^3 deposit tiles); x = L and y = L exactly
+    for xyz in ([10.3, 20.7, 5.5], [47.6, 0.2, 47.9], [0.0, 47.99, 13.0],
+                [15.5, 15.9, 31.7], [16.0, 31.999, 47.0], [48.0, 3.3, 7.1], [5.0, 48.0, 0.0]):
         p = np.zeros(1, dtype=__import__("cola_halo_b200").PARTICLE_DTYPE)
         p["x"] = xyz
         sim.set_particles(p, 0.1, 0.1)
