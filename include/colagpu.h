@@ -105,6 +105,26 @@ int cg_sim_sync(cg_sim* s);
 #define CG_PK_SUBTRACT_SHOT 2    /* subtract L^3 / np */
 int cg_sim_power_spectrum(cg_sim* s, int nbins, int flags, double* k, double* pk,
                           double* nmodes);
+/* The shell sums of cg_sim_power_spectrum for a half spectrum the caller
+ * already holds in device memory, without allocating anything (no reference
+ * counterpart).  For callers that cannot allocate device memory where they
+ * measure P(k): a caller whose memory pool or arena owns the whole device, a
+ * stream-ordered pipeline that must not call cudaMalloc (it synchronises the
+ * device), or a program that has given all of HBM to its meshes.
+ * d_spec: device, n*n*(n/2+1) interleaved complex [x][y][kz], unnormalised
+ * r2c of delta (the cg_fft_r2c layout); n even.  Same bins, flags and units
+ * as cg_sim_power_spectrum; np is the particle count for
+ * CG_PK_SUBTRACT_SHOT.  stream: a cudaStream_t, or NULL for the default
+ * stream; synchronous on it.
+ * Scratch is a fixed device array compiled into the library: at most
+ * CG_PK_NOALLOC_MAX_BINS bins (larger nbins returns CG_EINVAL).  Every call
+ * on a device shares that one array, so calls that overlap (from two host
+ * threads, or on two streams at once) race and must not be made.  The first
+ * call on each device, made with that device current, looks the array's
+ * device address up; make it before any stream capture. */
+#define CG_PK_NOALLOC_MAX_BINS 1024
+int cg_pk_bins_noalloc(const void* d_spec, int n, float boxsize, int nbins, int flags,
+                       double* k, double* pk, double* nmodes, long long np, void* stream);
 /* Copy one mesh to host: which = 0 density (delta), 1..3 force x, y, z;
  * ngrid^3 floats, [x][y][z] order. */
 int cg_sim_get_mesh(cg_sim* s, int which, float* out);
