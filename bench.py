@@ -469,11 +469,15 @@ def run_b200(args, cfg):
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "particle-steps/s",
-                    "h2d_bytes_per_step": 56 * npart, "d2h_bytes_per_step": snap_bytes,
-                    "what": "one realization per step: drop-in C ABI (cg_particles_upload, "
-                            "move_particles2, pm_calculate_forces, cola_kick, cola_drift, "
-                            "cola_set_snapshot) from pinned host Particle[] to a host "
-                            "Snapshot; %d force evaluations" % sched.nloop},
+                    "h2d_bytes_per_step": 56 * npart // sched.nloop,
+                    "d2h_bytes_per_step": snap_bytes // sched.nloop,
+                    "what": "whole realizations through the drop-in C ABI "
+                            "(cg_particles_upload, then per step move_particles2, "
+                            "pm_calculate_forces, cola_kick, cola_drift, and "
+                            "cola_set_snapshot) from a pinned host Particle[] (56 B per "
+                            "particle up) to a host Snapshot (32 B per particle down); "
+                            "%d force evaluations per realization, bytes averaged per "
+                            "step" % sched.nloop},
             "gpu_launches": int(launches),
             "clocks": clk,
             "stages_ms": {k: round(v["ms"] / args.steps, 4) for k, v in stages.items()},

@@ -82,21 +82,41 @@ __device__ __forceinline__ size_t cell(int i, int j, int k, int N) {
   return ((size_t)i * N + j) * N + k;
 }
 
+// The two z cells k0, k1 of one (x, y) column of the cloud.  When they lie
+// in one 16-byte-aligned group of four floats they take a single float4
+// atomic (zeros in the other two lanes leave those cells unchanged); else
+// (k0 = 3 mod 4, or k1 wrapped to 0) two scalar atomics.  `col` is the
+// cell (i, j, 0): a multiple of 4 floats since N is.
+__device__ __forceinline__ void add_z_pair(float* __restrict__ d, size_t col, int k0, int k1,
+                                           float w0, float w1) {
+  const int q = k0 & 3;
+  if (k1 == k0 + 1 && q != 3) {
+    float4 v = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    if (q == 0) { v.x = w0; v.y = w1; }
+    else if (q == 1) { v.y = w0; v.z = w1; }
+    else { v.z = w0; v.w = w1; }
+    atomicAdd(reinterpret_cast<float4*>(d + col + (k0 - q)), v);
+  } else {
+    atomicAdd(d + col + k0, w0);
+    atomicAdd(d + col + k1, w1);
+  }
+}
+
 __device__ __forceinline__ void deposit_one(float* __restrict__ d, const Cic& c, int N,
                                             float wpar) {
   const float T2W = __fmul_rn(c.t2, wpar);
   const float D2W = __fmul_rn(c.d2, wpar);
   if (0 <= c.i0 && c.i0 < N) {
-    atomicAdd(d + cell(c.i0, c.j0, c.k0, N), __fmul_rn(__fmul_rn(c.t3, c.t1), T2W));
-    atomicAdd(d + cell(c.i0, c.j0, c.k1, N), __fmul_rn(__fmul_rn(c.d3, c.t1), T2W));
-    atomicAdd(d + cell(c.i0, c.j1, c.k0, N), __fmul_rn(__fmul_rn(c.t3, c.t1), D2W));
-    atomicAdd(d + cell(c.i0, c.j1, c.k1, N), __fmul_rn(__fmul_rn(c.d3, c.t1), D2W));
+    add_z_pair(d, cell(c.i0, c.j0, 0, N), c.k0, c.k1, __fmul_rn(__fmul_rn(c.t3, c.t1), T2W),
+               __fmul_rn(__fmul_rn(c.d3, c.t1), T2W));
+    add_z_pair(d, cell(c.i0, c.j1, 0, N), c.k0, c.k1, __fmul_rn(__fmul_rn(c.t3, c.t1), D2W),
+               __fmul_rn(__fmul_rn(c.d3, c.t1), D2W));
   }
   if (0 <= c.i1 && c.i1 < N) {
-    atomicAdd(d + cell(c.i1, c.j0, c.k0, N), __fmul_rn(__fmul_rn(c.t3, c.d1), T2W));
-    atomicAdd(d + cell(c.i1, c.j0, c.k1, N), __fmul_rn(__fmul_rn(c.d3, c.d1), T2W));
-    atomicAdd(d + cell(c.i1, c.j1, c.k0, N), __fmul_rn(__fmul_rn(c.t3, c.d1), D2W));
-    atomicAdd(d + cell(c.i1, c.j1, c.k1, N), __fmul_rn(__fmul_rn(c.d3, c.d1), D2W));
+    add_z_pair(d, cell(c.i1, c.j0, 0, N), c.k0, c.k1, __fmul_rn(__fmul_rn(c.t3, c.d1), T2W),
+               __fmul_rn(__fmul_rn(c.d3, c.d1), T2W));
+    add_z_pair(d, cell(c.i1, c.j1, 0, N), c.k0, c.k1, __fmul_rn(__fmul_rn(c.t3, c.d1), D2W),
+               __fmul_rn(__fmul_rn(c.d3, c.d1), D2W));
   }
 }
 
@@ -188,11 +208,12 @@ using cgfft::Gmem;
 using cgfft::SmemCol;
 using cgfft::SmemLine;
 
-// Maximum radix of the strided x passes and of the fused y pass: radix 8
-// keeps these kernels at two CTAs per SM from 768 up.
+// Maximum radix of the strided x passes (radix 8 measured faster from 768
+// up) and the tile of the fused y pass: 4 lines per CTA, three CTAs per SM
+// (the fastest of the tile / thread / radix shapes measured at 384 and 768).
 __host__ __device__ constexpr int rm_x(int N) { return N >= 768 ? 8 : 16; }
-__host__ __device__ constexpr int rm_green(int N) { return N >= 768 ? 8 : 16; }
-constexpr int BYG = 8;   // lines per CTA of the fused y pass
+constexpr int BYG = 4;        // lines per CTA of the fused y pass
+constexpr int GREEN_MINB = 3; // resident CTAs per SM the fused pass is built for
 
 // FZ: r2c along z of R (TY z-lines (x, y0..y0+TY-1) per CTA) through a
 // complex FFT of length H = N/2 on (x_2m + i x_2m+1):
@@ -297,11 +318,12 @@ struct GmemXZ {
 };
 
 // The three transforms of the fused pass as separate (not inlined) calls:
-// each keeps its own register live range, so the kernel fits two CTAs per SM.
+// each keeps its own register live range, so the kernel fits GREEN_MINB CTAs
+// per SM without spilling.
 template <int N, int DIR, class First, class Mid, class Last>
 __device__ __noinline__ void fft_tile_y(const First f, const Mid m, const Last l,
                                         const float2* __restrict__ tw) {
-  cgfft::fft_io<N, BYG, T, true, DIR, rm_green(N)>(f, m, l, tw);
+  cgfft::fft_io<N, BYG, T, true, DIR>(f, m, l, tw);
 }
 
 // GREEN: forward c2c along ky, Green/gradient, inverse c2c along ky for the
@@ -309,7 +331,7 @@ __device__ __noinline__ void fft_tile_y(const First f, const Mid m, const Last l
 // BYG lines (kz, kx0 .. kx0+BYG-1) per CTA; N is a multiple of BYG so the
 // lines of a CTA share kz.
 template <int N>
-__global__ void __launch_bounds__(T, 2) k_green(const float2* __restrict__ spec,
+__global__ void __launch_bounds__(T, GREEN_MINB) k_green(const float2* __restrict__ spec,
                                                 float2* __restrict__ g0,
                                                 float2* __restrict__ g1,
                                                 float2* __restrict__ g2,
