@@ -174,7 +174,7 @@ def algorithmic_bytes(stage, N, npart):
         "deposit": 12.0 * npart,
         "fz_r2c": Mr + Ms,
         "fx_fwd": 2 * Ms,
-        "green_y": 4 * Ms,
+        "green_y": 3 * Ms,
         "fx_inv": 2 * Ms,
         "zi_c2r": Ms + Mr,
         "interp": 12.0 * npart + 3 * Mr + 12.0 * npart,

@@ -14,8 +14,10 @@
 //   FZ     r2c along z of R, transposed store into S      (+ density sum)
 //   FX     forward c2c along kx (stride N), in place
 //   GREEN  forward c2c along ky (contiguous lines), Green/gradient, inverse
-//          c2c along ky -> three spectra G_a (one read, three writes)
-//   FX     inverse c2c along kx on each G_a, in place
+//          c2c along ky -> the y spectrum and the shared x/z spectrum
+//          (one read, two writes)
+//   FX     inverse c2c along kx per component (x and z scale the shared
+//          spectrum by n_x / n_z as they load it)
 //   ZI     c2r along z of G_a, transposed load, store R_a
 // The plain 3-D transforms (mesh_r2c / mesh_c2r) run FZ, FY, FX and back.
 #include <cuda_runtime.h>
@@ -264,14 +266,40 @@ __global__ void __launch_bounds__(T) k_fy(float2* __restrict__ spec,
   cgfft::fft_io<N, BY, T, true, DIR>(g, mid, g, twN);
 }
 
-// FX: c2c along kx (stride N), TK ky columns per CTA, in place.
-template <int N, int DIR>
-__global__ void __launch_bounds__(T) k_fx(float2* __restrict__ spec,
+// Load of a kx column scaled by the force component's wavenumber index:
+// SCALE 1 by n_x = I0 (signed, Nyquist at +N/2; the position n along the
+// column), SCALE 2 by n_z = kz (the plane, constant over the CTA).
+template <int SCALE>
+struct GmemScaled {
+  const float2* p;
+  size_t es;
+  int N;
+  float fz;
+  __device__ __forceinline__ cplx ld(int b, int n) const {
+    const float2 v = __ldg(p + b + (size_t)n * es);
+    const float f = SCALE == 1 ? (float)(n <= N / 2 ? n : n - N) : fz;
+    return cplx{v.x * f, v.y * f};
+  }
+  static constexpr bool kShared = false;
+};
+
+// FX: c2c along kx (stride N), TK ky columns per CTA, from `in` to `out`
+// (the same array for an in-place pass).  SCALE 0: plain; 1 / 2: the input
+// is first multiplied by n_x / n_z (GmemScaled).
+template <int N, int DIR, int SCALE>
+__global__ void __launch_bounds__(T) k_fx(const float2* in, float2* out,
                                           const float2* __restrict__ twN) {
   extern __shared__ __align__(16) unsigned char smraw[];
   const SmemCol<TK> mid{reinterpret_cast<cplx*>(smraw)};
-  const Gmem g{spec + (size_t)blockIdx.y * N * N + blockIdx.x * TK, 1, (size_t)N};
-  cgfft::fft_io<N, TK, T, false, DIR, rm_x(N)>(g, mid, g, twN);
+  const size_t off = (size_t)blockIdx.y * N * N + blockIdx.x * TK;
+  const Gmem go{out + off, 1, (size_t)N};
+  if constexpr (SCALE == 0) {
+    const Gmem gi{const_cast<float2*>(in) + off, 1, (size_t)N};
+    cgfft::fft_io<N, TK, T, false, DIR, rm_x(N)>(gi, mid, go, twN);
+  } else {
+    const GmemScaled<SCALE> gi{in + off, (size_t)N, N, (float)blockIdx.y};
+    cgfft::fft_io<N, TK, T, false, DIR, rm_x(N)>(gi, mid, go, twN);
+  }
 }
 
 // compute_force_mesh (pm.c:304-346) on lines (kz, kx) that are already
@@ -300,23 +328,6 @@ struct GreenLoad {
   static constexpr bool kShared = true;
 };
 
-// n_x = I0 and n_z = kz are constant along a y line, so
-// IFFT_y(i f1 n_a/|n|^2 delta) = n_a IFFT_y(i f1/|n|^2 delta) for a = x, z:
-// one inverse transform serves both components.
-struct GmemXZ {
-  float2* gx;
-  float2* gz;
-  int kx0, N;
-  float fz;
-  __device__ __forceinline__ void st(int b, int n, cplx v) const {
-    const int kx = kx0 + b;
-    const float fx = (float)(kx <= N / 2 ? kx : kx - N);
-    gx[(size_t)b * N + n] = make_float2(v.x * fx, v.y * fx);
-    gz[(size_t)b * N + n] = make_float2(v.x * fz, v.y * fz);
-  }
-  static constexpr bool kShared = false;
-};
-
 // The three transforms of the fused pass as separate (not inlined) calls:
 // each keeps its own register live range, so the kernel fits GREEN_MINB CTAs
 // per SM without spilling.
@@ -326,16 +337,19 @@ __device__ __noinline__ void fft_tile_y(const First f, const Mid m, const Last l
   cgfft::fft_io<N, BYG, T, true, DIR>(f, m, l, tw);
 }
 
-// GREEN: forward c2c along ky, Green/gradient, inverse c2c along ky for the
-// y component and for the shared x/z factor: spec -> g0 (x), g1 (y), g2 (z).
-// BYG lines (kz, kx0 .. kx0+BYG-1) per CTA; N is a multiple of BYG so the
-// lines of a CTA share kz.
+// GREEN: forward c2c along ky, Green/gradient, inverse c2c along ky:
+//   g1 = IFFT_y(i f1 n_y/|n|^2 delta)       the y component
+//   g2 = IFFT_y(i f1/|n|^2 delta)           the x and z components before
+// their factor n_x / n_z, which is constant along a y line and is applied
+// by the inverse x pass as it loads g2 (k_fx, SCALE 1 and 2): one inverse
+// transform serves both components.  BYG lines (kz, kx0 .. kx0+BYG-1) per
+// CTA; N is a multiple of BYG so the lines of a CTA share kz.
 template <int N>
 __global__ void __launch_bounds__(T, GREEN_MINB) k_green(const float2* __restrict__ spec,
-                                                float2* __restrict__ g0,
-                                                float2* __restrict__ g1,
-                                                float2* __restrict__ g2,
-                                                const float2* __restrict__ twN, float f1) {
+                                                         float2* __restrict__ g1,
+                                                         float2* __restrict__ g2,
+                                                         const float2* __restrict__ twN,
+                                                         float f1) {
   constexpr int P = cgfft::line_pitch<N>();
   extern __shared__ __align__(16) unsigned char smraw[];
   cplx* D = reinterpret_cast<cplx*>(smraw);
@@ -352,8 +366,8 @@ __global__ void __launch_bounds__(T, GREEN_MINB) k_green(const float2* __restric
   fft_tile_y<N, 1>(gy, w, oy, twN);
   __syncthreads();
   const GreenLoad<P, 1> gs{D, kz, kx0, N, f1};
-  const GmemXZ oxz{g0 + off, g2 + off, kx0, N, (float)kz};
-  fft_tile_y<N, 1>(gs, d, oxz, twN);
+  const Gmem os{g2 + off, (size_t)N, 1};
+  fft_tile_y<N, 1>(gs, d, os, twN);
 }
 
 // ZI: c2r along z of S (lines (x, y0..y0+TY-1) per CTA) into R.  The
@@ -460,9 +474,11 @@ struct MeshKernels {
   void (*fz)(const float*, float2*, const float2*, const float2*, double*);
   void (*fyf)(float2*, const float2*);
   void (*fyi)(float2*, const float2*);
-  void (*fxf)(float2*, const float2*);
-  void (*fxi)(float2*, const float2*);
-  void (*green)(const float2*, float2*, float2*, float2*, const float2*, float);
+  void (*fxf)(const float2*, float2*, const float2*);
+  void (*fxi)(const float2*, float2*, const float2*);
+  void (*fxi_x)(const float2*, float2*, const float2*);   // inverse, input times n_x
+  void (*fxi_z)(const float2*, float2*, const float2*);   // inverse, input times n_z
+  void (*green)(const float2*, float2*, float2*, const float2*, float);
   void (*zi)(const float2*, float*, const float2*, const float2*);
   size_t sm_fz, sm_fy, sm_fx, sm_green, sm_zi;
 };
@@ -473,8 +489,10 @@ MeshKernels make_kernels() {
   k.fz = k_fz<N>;
   k.fyf = k_fy<N, -1>;
   k.fyi = k_fy<N, 1>;
-  k.fxf = k_fx<N, -1>;
-  k.fxi = k_fx<N, 1>;
+  k.fxf = k_fx<N, -1, 0>;
+  k.fxi = k_fx<N, 1, 0>;
+  k.fxi_x = k_fx<N, 1, 1>;
+  k.fxi_z = k_fx<N, 1, 2>;
   k.green = k_green<N>;
   k.zi = k_zi<N>;
   k.sm_fz = sizeof(cplx) * TY * cgfft::line_pitch<N / 2>();
@@ -507,6 +525,8 @@ cudaError_t set_all_smem(const MeshKernels& k) {
   if (e == cudaSuccess) e = set_smem((const void*)k.fyi, k.sm_fy);
   if (e == cudaSuccess) e = set_smem((const void*)k.fxf, k.sm_fx);
   if (e == cudaSuccess) e = set_smem((const void*)k.fxi, k.sm_fx);
+  if (e == cudaSuccess) e = set_smem((const void*)k.fxi_x, k.sm_fx);
+  if (e == cudaSuccess) e = set_smem((const void*)k.fxi_z, k.sm_fx);
   if (e == cudaSuccess) e = set_smem((const void*)k.green, k.sm_green);
   if (e == cudaSuccess) e = set_smem((const void*)k.zi, k.sm_zi);
   return e;
@@ -621,7 +641,7 @@ cudaError_t mesh_r2c(const MeshFFT* f, const float* real, float2* spec, cudaStre
   prof_mark(st, CG_ST_OTHER);
   k.fyf<<<(N / 2 + 1) * N / BY, T, k.sm_fy, st>>>(spec, f->twN);
   prof_mark(st, CG_ST_FX_FWD);
-  k.fxf<<<dim3(N / TK, N / 2 + 1), T, k.sm_fx, st>>>(spec, f->twN);
+  k.fxf<<<dim3(N / TK, N / 2 + 1), T, k.sm_fx, st>>>(spec, spec, f->twN);
   return cudaGetLastError();
 }
 
@@ -630,7 +650,7 @@ cudaError_t mesh_c2r(const MeshFFT* f, float2* spec, float* real, cudaStream_t s
   if (!get_kernels(f->N, &k)) return cudaErrorInvalidValue;
   const int N = f->N;
   prof_mark(st, CG_ST_FX_INV);
-  k.fxi<<<dim3(N / TK, N / 2 + 1), T, k.sm_fx, st>>>(spec, f->twN);
+  k.fxi<<<dim3(N / TK, N / 2 + 1), T, k.sm_fx, st>>>(spec, spec, f->twN);
   prof_mark(st, CG_ST_OTHER);
   k.fyi<<<(N / 2 + 1) * N / BY, T, k.sm_fy, st>>>(spec, f->twN);
   prof_mark(st, CG_ST_ZI);
@@ -685,7 +705,7 @@ cudaError_t pm_r2c(PmPlan* p, cudaStream_t st) {
   prof_mark(st, CG_ST_FZ);
   k.fz<<<dim3(N / TY, N), T, k.sm_fz, st>>>(p->dens, p->spec, p->twH, p->twN, p->dsum);
   prof_mark(st, CG_ST_FX_FWD);
-  k.fxf<<<dim3(N / TK, N / 2 + 1), T, k.sm_fx, st>>>(p->spec, p->twN);
+  k.fxf<<<dim3(N / TK, N / 2 + 1), T, k.sm_fx, st>>>(p->spec, p->spec, p->twN);
   return cudaGetLastError();
 }
 
@@ -693,15 +713,26 @@ cudaError_t pm_green_c2r(PmPlan* p, cudaStream_t st) {
   MeshKernels k;
   get_kernels(p->N, &k);
   const int N = p->N;
+  // gsp[1] <- y component, gsp[2] <- the shared x/z spectrum
   prof_mark(st, CG_ST_GREEN);
-  k.green<<<(N / 2 + 1) * N / BYG, T, k.sm_green, st>>>(p->spec, p->gsp[0], p->gsp[1],
-                                                         p->gsp[2], p->twN, p->f1);
-  for (int a = 0; a < 3; a++) {
-    prof_mark(st, CG_ST_FX_INV);
-    k.fxi<<<dim3(N / TK, N / 2 + 1), T, k.sm_fx, st>>>(p->gsp[a], p->twN);
-    prof_mark(st, CG_ST_ZI);
-    k.zi<<<dim3(N / TY, N), T, k.sm_zi, st>>>(p->gsp[a], p->fmesh[a], p->twH, p->twN);
-  }
+  k.green<<<(N / 2 + 1) * N / BYG, T, k.sm_green, st>>>(p->spec, p->gsp[1], p->gsp[2], p->twN,
+                                                         p->f1);
+  const dim3 gx(N / TK, N / 2 + 1), gz(N / TY, N);
+  // x: n_x * gsp[2] -> gsp[0] (gsp[2] is still needed for z)
+  prof_mark(st, CG_ST_FX_INV);
+  k.fxi_x<<<gx, T, k.sm_fx, st>>>(p->gsp[2], p->gsp[0], p->twN);
+  prof_mark(st, CG_ST_ZI);
+  k.zi<<<gz, T, k.sm_zi, st>>>(p->gsp[0], p->fmesh[0], p->twH, p->twN);
+  // y: in place
+  prof_mark(st, CG_ST_FX_INV);
+  k.fxi<<<gx, T, k.sm_fx, st>>>(p->gsp[1], p->gsp[1], p->twN);
+  prof_mark(st, CG_ST_ZI);
+  k.zi<<<gz, T, k.sm_zi, st>>>(p->gsp[1], p->fmesh[1], p->twH, p->twN);
+  // z: n_z * gsp[2], in place
+  prof_mark(st, CG_ST_FX_INV);
+  k.fxi_z<<<gx, T, k.sm_fx, st>>>(p->gsp[2], p->gsp[2], p->twN);
+  prof_mark(st, CG_ST_ZI);
+  k.zi<<<gz, T, k.sm_zi, st>>>(p->gsp[2], p->fmesh[2], p->twH, p->twN);
   return cudaGetLastError();
 }
 
@@ -737,7 +768,7 @@ cudaError_t pm_power_spectrum(PmPlan* p, const float* const x[3], long long n, i
   prof_mark(st, CG_ST_FZ);
   k.fz<<<dim3(N / TY, N), T, k.sm_fz, st>>>(p->dens, p->spec, p->twH, p->twN, p->dsum);
   prof_mark(st, CG_ST_FX_FWD);
-  k.fxf<<<dim3(N / TK, N / 2 + 1), T, k.sm_fx, st>>>(p->spec, p->twN);
+  k.fxf<<<dim3(N / TK, N / 2 + 1), T, k.sm_fx, st>>>(p->spec, p->spec, p->twN);
   prof_mark(st, CG_ST_OTHER);
   k.fyf<<<(N / 2 + 1) * N / BY, T, k.sm_fy, st>>>(p->spec, p->twN);
   cudaMemsetAsync(acc, 0, sizeof(double) * 3 * nbins, st);
