@@ -331,6 +331,12 @@ def run_b200(args, cfg):
     assert rc == 0, lib.cg_last_error()
     ics = host_parts.copy()
 
+    # ---- FFT schedule for this mesh size (untimed; cached across runs when
+    # COLAGPU_TUNE_CACHE names a file)
+    _lib.check(lib.cg_autotune(N, 0, None, None), "cg_autotune")
+    sg, sf = ctypes.c_int(), ctypes.c_int()
+    _lib.check(lib.cg_get_schedule(N, ctypes.byref(sg), ctypes.byref(sf)), "cg_get_schedule")
+
     # ---- device-resident step loop (value)
     sim = Simulation(nc, N, L, om)
     stream = lib.cg_sim_stream(sim.h)
@@ -465,7 +471,9 @@ def run_b200(args, cfg):
             "config": {"workload": args.config_desc, "particles": npart, "mesh": N,
                        "boxsize": L, "schedule": "10 COLA steps linear in a, z=49 -> 0",
                        "parallelism": "replicas x%d (one realization per GPU)" % world,
-                       "l2": "inputs larger than L2 (%.2f GB per mesh)" % (4.0 * N ** 3 / 1e9)},
+                       "l2": "inputs larger than L2 (%.2f GB per mesh)" % (4.0 * N ** 3 / 1e9),
+                       "fft_schedule": {"green_variant": sg.value, "x_variant": sf.value,
+                                        "chosen_by": "cg_autotune"}},
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "particle-steps/s",
@@ -505,17 +513,88 @@ def main():
     ap.add_argument("--train-seeds", type=int, default=16)
     ap.add_argument("--eval-seeds", type=int, default=8)
     ap.add_argument("--epochs", type=int, default=1)
+    ap.add_argument("--batch", action="store_true",
+                    help="batched realizations: 32 x 128^3 particles / 384^3 meshes, uneven "
+                         "boxes and step counts, one CUDA graph per run")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "b200":
         args.warmup = 3
     if args.learned:
         return run_learned(args)
+    if args.batch:
+        return run_batch(args)
     cfg = CONFIGS[args.config]
     args.config_desc = "%d^3 particles, %d^3 mesh, L=%g Mpc/h, BBKS, 2LPT z=49, 10 steps" % (
         cfg["nc"], cfg["nc"] * cfg["factor"], cfg["L"])
     if args.impl == "reference":
         return run_reference(args, cfg)
     return run_b200(args, cfg)
+
+
+def run_batch(args):
+    """Throughput of batched realizations: 32 realizations of 128^3
+    particles on 384^3 meshes with box sizes L ~ U[250, 400] Mpc/h and step
+    counts ~ U[5, 20] drawn from a fixed meta-seed, 2LPT at z = 49, recorded
+    into one CUDA graph over 4 streams; a particle-step is one COLA step of
+    one particle.  Device time from CUDA events around each graph launch."""
+    rank, world, local = dist_setup(args)
+    if rank != 0:
+        return 0
+    from cola_halo_b200 import _lib
+    from cola_halo_b200.batch import Batch
+    from cola_halo_b200.bbks import write_bbks_table
+    from cola_halo_b200.types import PARTICLE_DTYPE, Particles
+    lib = _lib.load()
+    _lib.check(lib.cg_set_device(local), "cg_set_device")
+    nreal, nc, N, om, a_init = 32, 128, 384, 0.273, 0.02
+    meta = np.random.default_rng(2024)
+    specs = [dict(nc=nc, ngrid=N, boxsize=float(meta.uniform(250.0, 400.0)), a_init=a_init,
+                  nsteps=int(meta.integers(5, 21)), aout=1.0) for _ in range(nreal)]
+    table = write_bbks_table(os.path.join(tempfile.mkdtemp(), "bbks.dat"))
+    _lib.check(lib.cg_autotune(N, 0, None, None), "cg_autotune")
+    npart = nc ** 3
+    nbytes = 56 * npart
+    hp_ptr = lib.cg_host_alloc(nbytes)
+    host = np.ctypeslib.as_array((ctypes.c_uint8 * nbytes).from_address(hp_ptr)).view(
+        PARTICLE_DTYPE)
+    P = Particles()
+    P.p = hp_ptr
+    P.force = None
+    P.np_allocated = npart
+    P.np_total = npart
+    P.np_average = float(npart)
+    lib.cg_dropin_set_abort(0)
+    lib.power_init(table.encode(), a_init, 0.81, om, 1 - om)
+    lib.lpt_init(nc, None, 0)
+    b = Batch(specs, om, nstreams=4)
+    for i, sp in enumerate(specs):
+        rc = lib.lpt_set_displacement(a_init, om, 1000 + i, sp["boxsize"], ctypes.byref(P))
+        assert rc == 0, lib.cg_last_error()
+        b.set_particles(i, host)
+    for _ in range(args.warmup):
+        b.run()
+    times = []
+    for _ in range(args.steps):
+        b.run()
+        times.append(b.last_ms())
+    ms = sum(times)
+    psteps = sum(npart * sp["nsteps"] for sp in specs)
+    value = psteps * len(times) / (ms / 1e3)
+    out = {"metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": 1,
+           "steps": len(times), "warmup": args.warmup, "ms_per_step": ms / len(times),
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+           "data": "synthetic (seeded 2LPT initial conditions, BBKS P(k))",
+           "config": {"workload": "batch: 32 x 128^3 particles, 384^3 meshes, L ~ U[250,400] "
+                                  "Mpc/h, nsteps ~ U[5,20] (meta-seed 2024), one CUDA graph",
+                      "realizations": nreal, "particle_steps_per_launch": psteps,
+                      "graph_nodes": b.num_nodes(), "streams": 4,
+                      "l2": "inputs larger than L2 (0.23 GB per mesh, 32 realizations)"},
+           "ms_per_launch": [round(t, 3) for t in times],
+           "note": "a step of this line is one graph launch running all 32 realizations"}
+    print(json.dumps(out))
+    b.close()
+    lib.cg_host_free(hp_ptr)
+    return 0
 
 
 def run_learned(args):

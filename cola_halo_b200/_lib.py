@@ -69,6 +69,11 @@ SIGNATURES = {
     "cg_batch_get_snapshot": (i32, [P, i32, P]),
     "cg_batch_power_spectrum": (i32, [P, i32, P, P, P]),
     "cg_batch_num_nodes": (i32, [P, ctypes.POINTER(sz)]),
+    "cg_batch_last_ms": (i32, [P, fptr]),
+    "cg_autotune": (i32, [i32, i32, P, P]),
+    "cg_schedule_variants": (i32, [i32, ctypes.POINTER(i32), ctypes.POINTER(i32)]),
+    "cg_get_schedule": (i32, [i32, ctypes.POINTER(i32), ctypes.POINTER(i32)]),
+    "cg_set_schedule": (i32, [i32, i32, i32]),
     "cg_fft_r2c": (i32, [i32, P, P]),
     "cg_fft_c2r": (i32, [i32, P, P]),
     "cg_launch_count": (i64, []),

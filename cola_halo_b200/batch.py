@@ -47,6 +47,12 @@ class Batch:
                                                     m.ctypes.data), "power_spectrum")
         return k, p, m
 
+    def last_ms(self):
+        """Device time of the last run (CUDA events around the graph launch)."""
+        t = ctypes.c_float()
+        _lib.check(self.lib.cg_batch_last_ms(self.h, ctypes.byref(t)), "last_ms")
+        return t.value
+
     def num_nodes(self):
         n = ctypes.c_size_t()
         _lib.check(self.lib.cg_batch_num_nodes(self.h, ctypes.byref(n)), "num_nodes")

@@ -59,6 +59,8 @@ struct cg_batch {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   std::vector<cudaEvent_t> events;
+  cudaEvent_t t0 = nullptr, t1 = nullptr;   // timing of the last graph launch
+  float last_ms = 0.0f;
 };
 
 namespace {
@@ -173,6 +175,8 @@ void free_batch(cg_batch* b) {
   }
   for (auto& t : b->tables) mesh_fft_free(&t.second);
   for (auto e : b->events) cudaEventDestroy(e);
+  if (b->t0) cudaEventDestroy(b->t0);
+  if (b->t1) cudaEventDestroy(b->t1);
   if (b->main) cudaStreamDestroy(b->main);
   delete b;
 }
@@ -301,9 +305,16 @@ extern "C" int cg_batch_run(cg_batch* b) {
     e = cudaGraphInstantiate(&b->exec, g, 0);
     if (e != cudaSuccess) return fail(CG_ECUDA, "cg_batch_run: instantiate", e);
   }
+  if (!b->t0) {
+    if ((e = cudaEventCreate(&b->t0)) != cudaSuccess || (e = cudaEventCreate(&b->t1)) != cudaSuccess)
+      return fail(CG_ECUDA, "cg_batch_run: event", e);
+  }
   prof_mark(b->main, CG_ST_OTHER);
+  cudaEventRecord(b->t0, b->main);
   e = cudaGraphLaunch(b->exec, b->main);
+  if (e == cudaSuccess) e = cudaEventRecord(b->t1, b->main);
   if (e == cudaSuccess) e = cudaStreamSynchronize(b->main);
+  if (e == cudaSuccess) e = cudaEventElapsedTime(&b->last_ms, b->t0, b->t1);
   if (e != cudaSuccess) return fail(CG_ECUDA, "cg_batch_run: launch", e);
   // density checks of every force evaluation (pm.c:548-553)
   for (auto& r : b->reals) {
@@ -350,4 +361,10 @@ extern "C" int cg_batch_num_nodes(cg_batch* b, size_t* nodes) {
   if (!b || !b->graph || !nodes) return fail(CG_EINVAL, "cg_batch_num_nodes: not recorded");
   cudaError_t e = cudaGraphGetNodes(b->graph, nullptr, nodes);
   return e == cudaSuccess ? CG_OK : fail(CG_ECUDA, "cg_batch_num_nodes", e);
+}
+
+extern "C" int cg_batch_last_ms(cg_batch* b, float* ms) {
+  if (!b || !ms) return fail(CG_EINVAL, "cg_batch_last_ms: NULL");
+  *ms = b->last_ms;
+  return CG_OK;
 }

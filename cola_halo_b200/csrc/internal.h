@@ -62,8 +62,28 @@ void mesh_fft_free(MeshFFT* f);
 cudaError_t mesh_r2c(const MeshFFT* f, const float* real, float2* spec, cudaStream_t st);
 cudaError_t mesh_c2r(const MeshFFT* f, float2* spec, float* real, cudaStream_t st);
 
+// Schedule of the FFT passes of one mesh size: which compiled variant of the
+// strided x pass and of the fused Green pass runs (pm_kernels.cu kFxCfg,
+// kGreenCfg).  Variants other than 0 exist from 256 up (Green: up to 768).
+#define PM_NUM_FX_VARIANTS 3
+#define PM_NUM_GREEN_VARIANTS 3
+struct MeshSched {
+  int green = 0;
+  int fx = 0;
+};
+
 // pm_kernels.cu
 bool pm_supported_mesh(int N);
+// Number of schedule variants compiled for mesh size N (1 below 256).
+int pm_num_variants(int N, int* n_green, int* n_fx);
+MeshSched pm_get_schedule(int N);
+void pm_set_schedule(int N, MeshSched s);
+// Time every Green and x-pass variant of the plan's mesh size on its own
+// buffers (their contents are overwritten) and return the fastest of each;
+// ms_green / ms_fx receive the best time of each variant (may be NULL).
+// Does not install the result.
+cudaError_t pm_autotune(PmPlan* p, cudaStream_t st, MeshSched* best, float* ms_green,
+                        float* ms_fx);
 cudaError_t pm_plan_alloc(PmPlan* p, int N, int factor, float L);
 void pm_plan_free(PmPlan* p);
 // Full PM force: deposit -> r2c -> Green/gradient -> 3 c2r -> interpolation.

@@ -26,6 +26,9 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <map>
+#include <mutex>
+
 #include "fft_core.cuh"
 #include "internal.h"
 
@@ -36,7 +39,6 @@ namespace {
 constexpr int T = CG_THREADS;
 constexpr int TY = 16;   // z-lines per CTA in FZ / ZI
 constexpr int BY = 8;    // y-lines per CTA in FY
-constexpr int TK = 8;    // ky columns per CTA in FX
 
 // ------------------------------------------------------------------ fill
 __global__ void k_fill(float4* __restrict__ p, size_t n4, float v) {
@@ -210,12 +212,32 @@ using cgfft::Gmem;
 using cgfft::SmemCol;
 using cgfft::SmemLine;
 
-// Maximum radix of the strided x passes (radix 8 measured faster from 768
-// up) and the tile of the fused y pass: 4 lines per CTA, three CTAs per SM
-// (the fastest of the tile / thread / radix shapes measured at 384 and 768).
-__host__ __device__ constexpr int rm_x(int N) { return N >= 768 ? 8 : 16; }
-constexpr int BYG = 4;        // lines per CTA of the fused y pass
-constexpr int GREEN_MINB = 3; // resident CTAs per SM the fused pass is built for
+// Schedules of the strided x pass and the fused y Green pass.  Variant 0
+// is the default; the others are compiled for meshes from MIN_TUNED_N up
+// and chosen per mesh size by the autotuner (pm_autotune) or set
+// explicitly.  x pass: ky columns per CTA and maximum radix (0: radix 8
+// from 768 up, else 16; -1: the other of the two).  Green pass: lines per
+// CTA, maximum radix and the resident CTAs per SM the kernel is
+// register-limited to.  The defaults are the fastest shapes measured at
+// 384 and 768.
+constexpr int MIN_TUNED_N = 256;
+// Variants compiled at size N.  The 8-line Green variants stop at 768: at
+// 1024 they would spill registers.
+__host__ __device__ constexpr int n_fx_variants(int N) {
+  return N >= MIN_TUNED_N ? PM_NUM_FX_VARIANTS : 1;
+}
+__host__ __device__ constexpr int n_green_variants(int N) {
+  return N >= MIN_TUNED_N && N <= 768 ? PM_NUM_GREEN_VARIANTS : 1;
+}
+struct FxCfg { int tk, rm; };
+struct GreenCfg { int byg, rm, minb; };
+constexpr FxCfg kFxCfg[PM_NUM_FX_VARIANTS] = {{8, 0}, {8, -1}, {16, 16}};
+constexpr GreenCfg kGreenCfg[PM_NUM_GREEN_VARIANTS] = {{4, 16, 3}, {8, 8, 2}, {8, 16, 2}};
+__host__ __device__ constexpr int rm_x_default(int N) { return N >= 768 ? 8 : 16; }
+__host__ __device__ constexpr int fx_rm(int N, int v) {
+  return kFxCfg[v].rm == 0 ? rm_x_default(N)
+                           : (kFxCfg[v].rm < 0 ? 24 - rm_x_default(N) : kFxCfg[v].rm);
+}
 
 // FZ: r2c along z of R (TY z-lines (x, y0..y0+TY-1) per CTA) through a
 // complex FFT of length H = N/2 on (x_2m + i x_2m+1):
@@ -283,22 +305,22 @@ struct GmemScaled {
   static constexpr bool kShared = false;
 };
 
-// FX: c2c along kx (stride N), TK ky columns per CTA, from `in` to `out`
+// FX: c2c along kx (stride N), TKV ky columns per CTA, from `in` to `out`
 // (the same array for an in-place pass).  SCALE 0: plain; 1 / 2: the input
 // is first multiplied by n_x / n_z (GmemScaled).
-template <int N, int DIR, int SCALE>
+template <int N, int DIR, int SCALE, int TKV, int RMX>
 __global__ void __launch_bounds__(T) k_fx(const float2* in, float2* out,
                                           const float2* __restrict__ twN) {
   extern __shared__ __align__(16) unsigned char smraw[];
-  const SmemCol<TK> mid{reinterpret_cast<cplx*>(smraw)};
-  const size_t off = (size_t)blockIdx.y * N * N + blockIdx.x * TK;
+  const SmemCol<TKV> mid{reinterpret_cast<cplx*>(smraw)};
+  const size_t off = (size_t)blockIdx.y * N * N + blockIdx.x * TKV;
   const Gmem go{out + off, 1, (size_t)N};
   if constexpr (SCALE == 0) {
     const Gmem gi{const_cast<float2*>(in) + off, 1, (size_t)N};
-    cgfft::fft_io<N, TK, T, false, DIR, rm_x(N)>(gi, mid, go, twN);
+    cgfft::fft_io<N, TKV, T, false, DIR, RMX>(gi, mid, go, twN);
   } else {
     const GmemScaled<SCALE> gi{in + off, (size_t)N, N, (float)blockIdx.y};
-    cgfft::fft_io<N, TK, T, false, DIR, rm_x(N)>(gi, mid, go, twN);
+    cgfft::fft_io<N, TKV, T, false, DIR, RMX>(gi, mid, go, twN);
   }
 }
 
@@ -329,12 +351,12 @@ struct GreenLoad {
 };
 
 // The three transforms of the fused pass as separate (not inlined) calls:
-// each keeps its own register live range, so the kernel fits GREEN_MINB CTAs
-// per SM without spilling.
-template <int N, int DIR, class First, class Mid, class Last>
+// each keeps its own register live range, so the kernel fits MINB CTAs per
+// SM without spilling.
+template <int N, int BG, int RMG, int DIR, class First, class Mid, class Last>
 __device__ __noinline__ void fft_tile_y(const First f, const Mid m, const Last l,
                                         const float2* __restrict__ tw) {
-  cgfft::fft_io<N, BYG, T, true, DIR>(f, m, l, tw);
+  cgfft::fft_io<N, BG, T, true, DIR, RMG>(f, m, l, tw);
 }
 
 // GREEN: forward c2c along ky, Green/gradient, inverse c2c along ky:
@@ -342,10 +364,10 @@ __device__ __noinline__ void fft_tile_y(const First f, const Mid m, const Last l
 //   g2 = IFFT_y(i f1/|n|^2 delta)           the x and z components before
 // their factor n_x / n_z, which is constant along a y line and is applied
 // by the inverse x pass as it loads g2 (k_fx, SCALE 1 and 2): one inverse
-// transform serves both components.  BYG lines (kz, kx0 .. kx0+BYG-1) per
-// CTA; N is a multiple of BYG so the lines of a CTA share kz.
-template <int N>
-__global__ void __launch_bounds__(T, GREEN_MINB) k_green(const float2* __restrict__ spec,
+// transform serves both components.  BG lines (kz, kx0 .. kx0+BG-1) per
+// CTA; N is a multiple of BG so the lines of a CTA share kz.
+template <int N, int BG, int RMG, int MINB>
+__global__ void __launch_bounds__(T, MINB) k_green(const float2* __restrict__ spec,
                                                          float2* __restrict__ g1,
                                                          float2* __restrict__ g2,
                                                          const float2* __restrict__ twN,
@@ -353,21 +375,21 @@ __global__ void __launch_bounds__(T, GREEN_MINB) k_green(const float2* __restric
   constexpr int P = cgfft::line_pitch<N>();
   extern __shared__ __align__(16) unsigned char smraw[];
   cplx* D = reinterpret_cast<cplx*>(smraw);
-  cplx* W = D + BYG * P;
-  const size_t l0 = (size_t)blockIdx.x * BYG;
+  cplx* W = D + BG * P;
+  const size_t l0 = (size_t)blockIdx.x * BG;
   const int kz = (int)(l0 / N);
   const int kx0 = (int)(l0 % N);
   const size_t off = l0 * N;
   const Gmem gin{const_cast<float2*>(spec) + off, (size_t)N, 1};
   const SmemLine<P> d{D}, w{W};
-  fft_tile_y<N, -1>(gin, d, d, twN);
+  fft_tile_y<N, BG, RMG, -1>(gin, d, d, twN);
   const GreenLoad<P, 0> gy{D, kz, kx0, N, f1};
   const Gmem oy{g1 + off, (size_t)N, 1};
-  fft_tile_y<N, 1>(gy, w, oy, twN);
+  fft_tile_y<N, BG, RMG, 1>(gy, w, oy, twN);
   __syncthreads();
   const GreenLoad<P, 1> gs{D, kz, kx0, N, f1};
   const Gmem os{g2 + off, (size_t)N, 1};
-  fft_tile_y<N, 1>(gs, d, os, twN);
+  fft_tile_y<N, BG, RMG, 1>(gs, d, os, twN);
 }
 
 // ZI: c2r along z of S (lines (x, y0..y0+TY-1) per CTA) into R.  The
@@ -481,54 +503,107 @@ struct MeshKernels {
   void (*green)(const float2*, float2*, float2*, const float2*, float);
   void (*zi)(const float2*, float*, const float2*, const float2*);
   size_t sm_fz, sm_fy, sm_fx, sm_green, sm_zi;
+  int tk;    // ky columns per CTA of the x pass
+  int byg;   // lines per CTA of the Green pass
 };
 
+template <int N, int V>
+void set_fx(MeshKernels* k) {
+  constexpr int TKV = kFxCfg[V].tk, RMX = fx_rm(N, V);
+  k->fxf = k_fx<N, -1, 0, TKV, RMX>;
+  k->fxi = k_fx<N, 1, 0, TKV, RMX>;
+  k->fxi_x = k_fx<N, 1, 1, TKV, RMX>;
+  k->fxi_z = k_fx<N, 1, 2, TKV, RMX>;
+  k->sm_fx = sizeof(cplx) * cgfft::col_tile_elems<N, TKV>();
+  k->tk = TKV;
+}
+
+template <int N, int V>
+void set_green(MeshKernels* k) {
+  constexpr GreenCfg c = kGreenCfg[V];
+  k->green = k_green<N, c.byg, c.rm, c.minb>;
+  k->sm_green = sizeof(cplx) * 2 * c.byg * cgfft::line_pitch<N>();
+  k->byg = c.byg;
+}
+
 template <int N>
-MeshKernels make_kernels() {
+MeshKernels make_kernels(MeshSched s) {
   MeshKernels k;
   k.fz = k_fz<N>;
   k.fyf = k_fy<N, -1>;
   k.fyi = k_fy<N, 1>;
-  k.fxf = k_fx<N, -1, 0>;
-  k.fxi = k_fx<N, 1, 0>;
-  k.fxi_x = k_fx<N, 1, 1>;
-  k.fxi_z = k_fx<N, 1, 2>;
-  k.green = k_green<N>;
   k.zi = k_zi<N>;
   k.sm_fz = sizeof(cplx) * TY * cgfft::line_pitch<N / 2>();
   k.sm_fy = sizeof(cplx) * BY * cgfft::line_pitch<N>();
-  k.sm_fx = sizeof(cplx) * cgfft::col_tile_elems<N, TK>();
-  k.sm_green = sizeof(cplx) * 2 * BYG * cgfft::line_pitch<N>();
   k.sm_zi = sizeof(cplx) * TY * cgfft::line_pitch<N / 2 + 1>();
+  if constexpr (n_fx_variants(N) > 1) {
+    switch (s.fx) {
+      case 1: set_fx<N, 1>(&k); break;
+      case 2: set_fx<N, 2>(&k); break;
+      default: set_fx<N, 0>(&k);
+    }
+  } else {
+    set_fx<N, 0>(&k);
+  }
+  if constexpr (n_green_variants(N) > 1) {
+    switch (s.green) {
+      case 1: set_green<N, 1>(&k); break;
+      case 2: set_green<N, 2>(&k); break;
+      default: set_green<N, 0>(&k);
+    }
+  } else {
+    set_green<N, 0>(&k);
+  }
   return k;
 }
 
 #define CG_MESH_SIZES(X) X(16) X(32) X(48) X(64) X(96) X(128) X(192) X(256) X(384) X(512) X(768) X(1024)
 
-bool get_kernels(int N, MeshKernels* out) {
+bool kernels_with(int N, MeshSched s, MeshKernels* out) {
   switch (N) {
-#define CG_CASE(n) case n: *out = make_kernels<n>(); return true;
+#define CG_CASE(n) case n: *out = make_kernels<n>(s); return true;
     CG_MESH_SIZES(CG_CASE)
 #undef CG_CASE
     default: return false;
   }
 }
 
+// The schedule in use per mesh size (variant 0 unless tuned or set).
+std::mutex g_sched_mu;
+std::map<int, MeshSched> g_sched;
+
+MeshSched sched_for(int N) {
+  std::lock_guard<std::mutex> lk(g_sched_mu);
+  auto it = g_sched.find(N);
+  return it == g_sched.end() ? MeshSched{} : it->second;
+}
+
+bool get_kernels(int N, MeshKernels* out) { return kernels_with(N, sched_for(N), out); }
+
 cudaError_t set_smem(const void* fn, size_t bytes) {
   return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
-// Dynamic shared-memory limits of every pass kernel of one mesh size.
-cudaError_t set_all_smem(const MeshKernels& k) {
-  cudaError_t e = set_smem((const void*)k.fz, k.sm_fz);
-  if (e == cudaSuccess) e = set_smem((const void*)k.fyf, k.sm_fy);
-  if (e == cudaSuccess) e = set_smem((const void*)k.fyi, k.sm_fy);
-  if (e == cudaSuccess) e = set_smem((const void*)k.fxf, k.sm_fx);
-  if (e == cudaSuccess) e = set_smem((const void*)k.fxi, k.sm_fx);
-  if (e == cudaSuccess) e = set_smem((const void*)k.fxi_x, k.sm_fx);
-  if (e == cudaSuccess) e = set_smem((const void*)k.fxi_z, k.sm_fx);
-  if (e == cudaSuccess) e = set_smem((const void*)k.green, k.sm_green);
-  if (e == cudaSuccess) e = set_smem((const void*)k.zi, k.sm_zi);
+// Dynamic shared-memory limits of the pass kernels of one mesh size, for
+// every schedule variant (a schedule may change after a plan exists).
+cudaError_t set_all_smem(int N) {
+  cudaError_t e = cudaSuccess;
+  const int nv = n_fx_variants(N);
+  const int ng = n_green_variants(N);
+  for (int v = 0; v < (nv > ng ? nv : ng) && e == cudaSuccess; v++) {
+    MeshKernels k;
+    if (!kernels_with(N, MeshSched{v < ng ? v : 0, v < nv ? v : 0}, &k))
+      return cudaErrorInvalidValue;
+    if (e == cudaSuccess) e = set_smem((const void*)k.fz, k.sm_fz);
+    if (e == cudaSuccess) e = set_smem((const void*)k.fyf, k.sm_fy);
+    if (e == cudaSuccess) e = set_smem((const void*)k.fyi, k.sm_fy);
+    if (e == cudaSuccess) e = set_smem((const void*)k.fxf, k.sm_fx);
+    if (e == cudaSuccess) e = set_smem((const void*)k.fxi, k.sm_fx);
+    if (e == cudaSuccess) e = set_smem((const void*)k.fxi_x, k.sm_fx);
+    if (e == cudaSuccess) e = set_smem((const void*)k.fxi_z, k.sm_fx);
+    if (e == cudaSuccess) e = set_smem((const void*)k.green, k.sm_green);
+    if (e == cudaSuccess) e = set_smem((const void*)k.zi, k.sm_zi);
+  }
   return e;
 }
 
@@ -552,6 +627,97 @@ int grid_for(long long n) {
 bool pm_supported_mesh(int N) {
   MeshKernels k;
   return get_kernels(N, &k);
+}
+
+int pm_num_variants(int N, int* n_green, int* n_fx) {
+  MeshKernels k;
+  if (!get_kernels(N, &k)) return 0;
+  if (n_green) *n_green = n_green_variants(N);
+  if (n_fx) *n_fx = n_fx_variants(N);
+  return 1;
+}
+
+MeshSched pm_get_schedule(int N) { return sched_for(N); }
+
+void pm_set_schedule(int N, MeshSched s) {
+  std::lock_guard<std::mutex> lk(g_sched_mu);
+  g_sched[N] = s;
+}
+
+// Best of `reps` timed launches (after one untimed) of `launch` on stream st.
+template <class F>
+static cudaError_t best_time(cudaStream_t st, int reps, F launch, float* ms) {
+  cudaEvent_t a, b;
+  cudaError_t e = cudaEventCreate(&a);
+  if (e != cudaSuccess) return e;
+  if ((e = cudaEventCreate(&b)) != cudaSuccess) {
+    cudaEventDestroy(a);
+    return e;
+  }
+  launch();
+  float best = 1e30f;
+  for (int r = 0; r < reps && e == cudaSuccess; r++) {
+    cudaEventRecord(a, st);
+    launch();
+    cudaEventRecord(b, st);
+    e = cudaEventSynchronize(b);
+    float t = 0.0f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&t, a, b);
+    if (e == cudaSuccess && t < best) best = t;
+  }
+  if (e == cudaSuccess) e = cudaGetLastError();
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  *ms = best;
+  return e;
+}
+
+cudaError_t pm_autotune(PmPlan* p, cudaStream_t st, MeshSched* best, float* ms_green,
+                        float* ms_fx) {
+  const int N = p->N;
+  int ng = 0, nf = 0;
+  if (!pm_num_variants(N, &ng, &nf)) return cudaErrorInvalidValue;
+  cudaError_t e = set_all_smem(N);
+  // defined contents for the timed passes (the values do not change the work)
+  if (e == cudaSuccess) e = cudaMemsetAsync(p->spec, 0, p->spec_bytes, st);
+  for (int a = 0; a < 3 && e == cudaSuccess; a++)
+    e = cudaMemsetAsync(p->gsp[a], 0, p->spec_bytes, st);
+  if (e != cudaSuccess) return e;
+  constexpr int kReps = 3;
+  MeshSched out;
+  float tbest = 1e30f;
+  for (int v = 0; v < ng && e == cudaSuccess; v++) {
+    MeshKernels k;
+    kernels_with(N, MeshSched{v, 0}, &k);
+    float t = 0.0f;
+    e = best_time(st, kReps, [&] {
+      prof_mark(st, CG_ST_OTHER);
+      k.green<<<(N / 2 + 1) * N / k.byg, T, k.sm_green, st>>>(p->spec, p->gsp[1], p->gsp[2],
+                                                               p->twN, p->f1);
+    }, &t);
+    if (ms_green) ms_green[v] = t;
+    if (e == cudaSuccess && t < tbest) {
+      tbest = t;
+      out.green = v;
+    }
+  }
+  tbest = 1e30f;
+  for (int v = 0; v < nf && e == cudaSuccess; v++) {
+    MeshKernels k;
+    kernels_with(N, MeshSched{0, v}, &k);
+    float t = 0.0f;
+    e = best_time(st, kReps, [&] {
+      prof_mark(st, CG_ST_OTHER);
+      k.fxi_x<<<dim3(N / k.tk, N / 2 + 1), T, k.sm_fx, st>>>(p->gsp[2], p->gsp[0], p->twN);
+    }, &t);
+    if (ms_fx) ms_fx[v] = t;
+    if (e == cudaSuccess && t < tbest) {
+      tbest = t;
+      out.fx = v;
+    }
+  }
+  if (e == cudaSuccess) *best = out;
+  return e;
 }
 
 cudaError_t pm_plan_alloc(PmPlan* p, int N, int factor, float L) {
@@ -599,7 +765,7 @@ cudaError_t pm_plan_alloc(PmPlan* p, int N, int factor, float L) {
   }
   CG_TRY(cudaMemset(p->dsum, 0, sizeof(double)));
   CG_TRY(cudaMemset(p->err, 0, sizeof(unsigned)));
-  CG_TRY(set_all_smem(k));
+  CG_TRY(set_all_smem(N));
 #undef CG_TRY
   return cudaSuccess;
 }
@@ -620,7 +786,7 @@ cudaError_t mesh_fft_alloc(MeshFFT* f, int N) {
     if (e == cudaSuccess) e = cudaMemcpy(f->twH, h, sizeof(float2) * (N / 2), cudaMemcpyHostToDevice);
     free(h);
   }
-  if (e == cudaSuccess) e = set_all_smem(k);
+  if (e == cudaSuccess) e = set_all_smem(N);
   if (e != cudaSuccess) mesh_fft_free(f);
   return e;
 }
@@ -641,7 +807,7 @@ cudaError_t mesh_r2c(const MeshFFT* f, const float* real, float2* spec, cudaStre
   prof_mark(st, CG_ST_OTHER);
   k.fyf<<<(N / 2 + 1) * N / BY, T, k.sm_fy, st>>>(spec, f->twN);
   prof_mark(st, CG_ST_FX_FWD);
-  k.fxf<<<dim3(N / TK, N / 2 + 1), T, k.sm_fx, st>>>(spec, spec, f->twN);
+  k.fxf<<<dim3(N / k.tk, N / 2 + 1), T, k.sm_fx, st>>>(spec, spec, f->twN);
   return cudaGetLastError();
 }
 
@@ -650,7 +816,7 @@ cudaError_t mesh_c2r(const MeshFFT* f, float2* spec, float* real, cudaStream_t s
   if (!get_kernels(f->N, &k)) return cudaErrorInvalidValue;
   const int N = f->N;
   prof_mark(st, CG_ST_FX_INV);
-  k.fxi<<<dim3(N / TK, N / 2 + 1), T, k.sm_fx, st>>>(spec, spec, f->twN);
+  k.fxi<<<dim3(N / k.tk, N / 2 + 1), T, k.sm_fx, st>>>(spec, spec, f->twN);
   prof_mark(st, CG_ST_OTHER);
   k.fyi<<<(N / 2 + 1) * N / BY, T, k.sm_fy, st>>>(spec, f->twN);
   prof_mark(st, CG_ST_ZI);
@@ -705,7 +871,7 @@ cudaError_t pm_r2c(PmPlan* p, cudaStream_t st) {
   prof_mark(st, CG_ST_FZ);
   k.fz<<<dim3(N / TY, N), T, k.sm_fz, st>>>(p->dens, p->spec, p->twH, p->twN, p->dsum);
   prof_mark(st, CG_ST_FX_FWD);
-  k.fxf<<<dim3(N / TK, N / 2 + 1), T, k.sm_fx, st>>>(p->spec, p->spec, p->twN);
+  k.fxf<<<dim3(N / k.tk, N / 2 + 1), T, k.sm_fx, st>>>(p->spec, p->spec, p->twN);
   return cudaGetLastError();
 }
 
@@ -715,9 +881,9 @@ cudaError_t pm_green_c2r(PmPlan* p, cudaStream_t st) {
   const int N = p->N;
   // gsp[1] <- y component, gsp[2] <- the shared x/z spectrum
   prof_mark(st, CG_ST_GREEN);
-  k.green<<<(N / 2 + 1) * N / BYG, T, k.sm_green, st>>>(p->spec, p->gsp[1], p->gsp[2], p->twN,
-                                                         p->f1);
-  const dim3 gx(N / TK, N / 2 + 1), gz(N / TY, N);
+  k.green<<<(N / 2 + 1) * N / k.byg, T, k.sm_green, st>>>(p->spec, p->gsp[1], p->gsp[2],
+                                                           p->twN, p->f1);
+  const dim3 gx(N / k.tk, N / 2 + 1), gz(N / TY, N);
   // x: n_x * gsp[2] -> gsp[0] (gsp[2] is still needed for z)
   prof_mark(st, CG_ST_FX_INV);
   k.fxi_x<<<gx, T, k.sm_fx, st>>>(p->gsp[2], p->gsp[0], p->twN);
@@ -768,7 +934,7 @@ cudaError_t pm_power_spectrum(PmPlan* p, const float* const x[3], long long n, i
   prof_mark(st, CG_ST_FZ);
   k.fz<<<dim3(N / TY, N), T, k.sm_fz, st>>>(p->dens, p->spec, p->twH, p->twN, p->dsum);
   prof_mark(st, CG_ST_FX_FWD);
-  k.fxf<<<dim3(N / TK, N / 2 + 1), T, k.sm_fx, st>>>(p->spec, p->spec, p->twN);
+  k.fxf<<<dim3(N / k.tk, N / 2 + 1), T, k.sm_fx, st>>>(p->spec, p->spec, p->twN);
   prof_mark(st, CG_ST_OTHER);
   k.fyf<<<(N / 2 + 1) * N / BY, T, k.sm_fy, st>>>(p->spec, p->twN);
   cudaMemsetAsync(acc, 0, sizeof(double) * 3 * nbins, st);

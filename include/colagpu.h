@@ -47,7 +47,7 @@ typedef struct cg_sim cg_sim;
 const char* cg_last_error(void);
 int cg_version(void);
 /* 1 if mesh size n (cells per dimension) is supported: n in
- * {32, 48, 64, 96, 128, 192, 256, 384, 512, 768, 1024}. */
+ * {16, 32, 48, 64, 96, 128, 192, 256, 384, 512, 768, 1024}. */
 int cg_mesh_supported(int n);
 /* Number of visible CUDA devices (0 when there is none or no driver). */
 int cg_device_count(void);
@@ -192,6 +192,9 @@ int cg_batch_get_snapshot(cg_batch* b, int i, void* pmin_out);
 int cg_batch_power_spectrum(cg_batch* b, int i, double* k, double* pk, double* nmodes);
 /* Number of nodes of the recorded graph (after the first run). */
 int cg_batch_num_nodes(cg_batch* b, size_t* nodes);
+/* Device time (CUDA events around the graph launch) of the last
+ * cg_batch_run, in milliseconds. */
+int cg_batch_last_ms(cg_batch* b, float* ms);
 
 /* Unnormalised 3-D real transforms of host arrays on the device, FFTW sign
  * convention (replaces the fftwf_mpi r2c / c2r plans of pm.c:141-147 and
@@ -201,6 +204,25 @@ int cg_batch_num_nodes(cg_batch* b, size_t* nodes);
  * FFTW's c2r does.  Synchronous; allocates its own scratch. */
 int cg_fft_r2c(int n, const float* real_in, float* spec_out);
 int cg_fft_c2r(int n, const float* spec_in, float* real_out);
+
+/* FFT schedule autotuner (no reference counterpart).  From 256 up each
+ * mesh size has several compiled variants of the strided x pass (ky columns
+ * per CTA, maximum radix) and, up to 768, of the fused y Green pass (lines
+ * per CTA, maximum radix, CTAs per SM).  cg_autotune times them on a
+ * temporary plan of that size on the current device, installs the fastest
+ * of each for the process, and appends the choice to the file named by
+ * COLAGPU_TUNE_CACHE (if set), which later calls read instead of timing.
+ * ms_green / ms_fx (may be NULL; cg_schedule_variants entries each) receive
+ * the best time of every variant when they were timed.  CG_TUNE_FORCE
+ * re-times.  The variants agree to float rounding; a fixed schedule
+ * (cached, or set with cg_set_schedule) makes runs bit-reproducible.
+ * Variant 0 is the default; sizes below 256 have only variant 0.  Tune
+ * outside stream capture. */
+#define CG_TUNE_FORCE 1
+int cg_autotune(int ngrid, int flags, float* ms_green, float* ms_fx);
+int cg_schedule_variants(int ngrid, int* n_green, int* n_fx);
+int cg_get_schedule(int ngrid, int* green_variant, int* fx_variant);
+int cg_set_schedule(int ngrid, int green_variant, int fx_variant);
 
 /* Kernel accounting (no reference counterpart; the reference's wall-clock
  * timers are timer.c).  cg_launch_count: kernels launched by this library
