@@ -512,7 +512,7 @@ def main():
                     help="second metric: learned coarse mesh vs plain factor-3 PM")
     ap.add_argument("--train-seeds", type=int, default=16)
     ap.add_argument("--eval-seeds", type=int, default=8)
-    ap.add_argument("--epochs", type=int, default=1)
+    ap.add_argument("--epochs", type=int, default=3)
     ap.add_argument("--batch", action="store_true",
                     help="batched realizations: 32 x 128^3 particles / 384^3 meshes, uneven "
                          "boxes and step counts, one CUDA graph per run")
@@ -618,8 +618,15 @@ def run_learned(args):
     fine_s = float(np.mean([r["fine_s"] for r in seeds]))
     learned_s = float(np.mean([r["learned_s"] for r in seeds]))
     coarse_s = float(np.mean([r["coarse_s"] for r in seeds]))
+    err_l = float(np.mean([r["err_learned"] for r in seeds]))
     out = {"metric": "wall time to 1% P(k) error, learned vs plain PM",
            "value": fine_s / learned_s, "unit": "x (plain factor-3 time / learned time)",
+           "reaches_1pct": bool(err_l <= 0.01),
+           "timing": "device time of each realization's time loop (11 force evaluations) "
+                     "from the library's CUDA-event profile; host wall times beside it",
+           "plain_fine_wall_s": float(np.mean([r["fine_wall_s"] for r in seeds])),
+           "learned_wall_s": float(np.mean([r["learned_wall_s"] for r in seeds])),
+           "plain_coarse_wall_s": float(np.mean([r["coarse_wall_s"] for r in seeds])),
            "higher_is_better": True, "n_gpus": 1, "dtype": "f32 PM, bf16 net (fp32 accum)",
            "data": "synthetic (seeded 2LPT initial conditions, BBKS P(k))",
            "config": {"workload": "128^3 particles, L=300 Mpc/h, coarse 128^3 (factor 1) + "
@@ -628,7 +635,7 @@ def run_learned(args):
                       "train_seeds": args.train_seeds, "eval_seeds": args.eval_seeds,
                       "epochs": args.epochs, "kmax": "0.5 k_Nyq = %.4f h/Mpc" % (0.5 * math.pi * nc / L)},
            "plain_fine_s": fine_s, "learned_s": learned_s, "plain_coarse_s": coarse_s,
-           "pk_err_learned": float(np.mean([r["err_learned"] for r in seeds])),
+           "pk_err_learned": err_l,
            "pk_err_coarse": float(np.mean([r["err_coarse"] for r in seeds])),
            "pk_err_learned_max": float(np.max([r["err_learned"] for r in seeds])),
            "train_s": res["train_s"], "train_steps": res["train_steps"],

@@ -3,14 +3,22 @@
 //
 // Implicit GEMM per tile of 128 consecutive z voxels of one (x, y) line:
 //   D[128 voxels][16 co] = sum over 27 taps of A_t[128][16 ci] . B_t[16 ci][16 co]
-// A_t are the tile's neighbour voxels for tap t, copied from HBM/L2 into
-// shared memory in the no-swizzle K-major core-matrix layout (8 rows x 16 B
-// per core matrix; the two 8-channel halves 128 B apart (LBO), 8-row groups
-// 256 B apart (SBO)).  B_t are the tap weights in the same layout.  One
-// thread issues the 27 MMAs (M=128, N=16, K=16 each), tcgen05.commit
-// arrives on an mbarrier, the four warps read their 32 accumulator lanes
-// with tcgen05.ld and apply bias + activation.  CTAs are persistent over
-// tiles; every mbarrier wait is bounded and reports through an error word.
+// The 27 taps read only 9 input lines -- the (x +- 1, y +- 1) neighbours --
+// each over z0 - 1 .. z0 + 128.  A CTA copies those 9 lines (130 rows of
+// 32 bytes) into shared memory once, in a row-contiguous K-major layout:
+// per line, the 8-channel half h of row j sits at h * 2080 + j * 16 bytes.
+// Read with core-matrix strides SBO = 128 B (8-row groups) and LBO = 2080 B
+// (the two 8-channel halves), the operand of tap (dx, dy, dz) is the same
+// buffer started dz rows further on: the z shift costs no copy.  B_t are the
+// tap weights in the no-swizzle core-matrix layout (LBO 128 B, SBO 256 B).
+//
+// CTAs are persistent over tiles with two line buffers: the cp.async gather
+// of the next tile runs while one thread issues the current tile's 27 MMAs
+// (M=128, N=16, K=16), tcgen05.commit arrives on an mbarrier, and the four
+// warps read their 32 accumulator lanes with tcgen05.ld for bias +
+// activation.  Every mbarrier wait is bounded and reports through an error
+// word; on a timeout the CTA drains its copies, frees its tensor memory and
+// returns.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -21,10 +29,14 @@ namespace {
 
 constexpr int C = CNET_C;
 constexpr int TILE_M = 128;
-constexpr int A_BYTES = TILE_M * C * 2;          // 4096: one tap's A operand
+constexpr int ROWS = TILE_M + 2;                 // z0 - 1 .. z0 + 128
+constexpr int HALF_BYTES = ROWS * 16;            // 2080: one 8-channel half of a line
+constexpr int LINE_BYTES = 2 * HALF_BYTES;       // 4160
+constexpr int STAGE_BYTES = 9 * LINE_BYTES;      // 37440: the 9 neighbour lines
 constexpr int B_BYTES = C * C * 2;               // 512: one tap's B operand
-constexpr int SMEM = 27 * A_BYTES + 27 * B_BYTES + 64;
+constexpr int SMEM = 2 * STAGE_BYTES + 27 * B_BYTES + 64;
 constexpr int THREADS = 128;
+constexpr int CTAS_PER_SM = 2;
 constexpr long long kWaitLimit = 1LL << 24;
 
 __device__ unsigned g_tc_err = 0;
@@ -33,11 +45,12 @@ __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return (uint32_t)__cvta_generic_to_shared(p);
 }
 
-// Shared-memory matrix descriptor: no swizzle, K-major, LBO = 128 B between
-// the two K halves, SBO = 256 B between 8-row groups, version 1.
-__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr) {
-  return (uint64_t)((saddr & 0x3FFFF) >> 4) | ((uint64_t)(128 >> 4) << 16) |
-         ((uint64_t)(256 >> 4) << 32) | (1ULL << 46);
+// Shared-memory matrix descriptor: no swizzle, K-major, version 1.  LBO is
+// the byte offset between the core matrices of the two K halves, SBO the
+// offset between 8-row groups; the start address is 16-byte aligned.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((saddr & 0x3FFFF) >> 4) | ((uint64_t)(lbo >> 4) << 16) |
+         ((uint64_t)(sbo >> 4) << 32) | (1ULL << 46);
 }
 
 // Instruction descriptor, kind::f16: D f32, A bf16, B bf16, both K-major,
@@ -65,15 +78,36 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase) {
   return false;
 }
 
+// cp.async of the 9 neighbour lines of tile `tile` into stage buffer `st`:
+// element (line L, row j, half h) <- voxel (x + L/3 - 1, y + L%3 - 1,
+// z0 - 1 + j), channels 8h .. 8h+7 (periodic).
+__device__ __forceinline__ void gather(const __nv_bfloat16* __restrict__ in, int N, int tile,
+                                       uint8_t* stage) {
+  const int tiles_per_line = N / TILE_M;
+  const int line = tile / tiles_per_line;
+  const int z0 = (tile % tiles_per_line) * TILE_M;
+  const int x = line / N, y = line % N;
+  for (int i = threadIdx.x; i < 9 * ROWS * 2; i += THREADS) {
+    const int h = i & 1, j = (i >> 1) % ROWS, L = (i >> 1) / ROWS;
+    int xx = x + L / 3 - 1, yy = y + L % 3 - 1, zz = z0 - 1 + j;
+    xx = xx < 0 ? xx + N : (xx >= N ? xx - N : xx);
+    yy = yy < 0 ? yy + N : (yy >= N ? yy - N : yy);
+    zz = zz < 0 ? zz + N : (zz >= N ? zz - N : zz);
+    const __nv_bfloat16* src = in + (((size_t)xx * N + yy) * N + zz) * C + h * 8;
+    const uint32_t dst = smem_u32(stage + L * LINE_BYTES + h * HALF_BYTES + j * 16);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" :: "r"(dst), "l"(src) : "memory");
+  }
+}
+
 template <bool FLIP>
-__global__ void __launch_bounds__(THREADS, 1) k_conv_tc(const __nv_bfloat16* __restrict__ in, int N,
-                                                        const __nv_bfloat16* __restrict__ w,
-                                                        const float* __restrict__ bias, int act,
-                                                        float* __restrict__ out_f,
-                                                        __nv_bfloat16* __restrict__ out_b) {
+__global__ void __launch_bounds__(THREADS, CTAS_PER_SM)
+    k_conv_tc(const __nv_bfloat16* __restrict__ in, int N, const __nv_bfloat16* __restrict__ w,
+              const float* __restrict__ bias, int act, float* __restrict__ out_f,
+              __nv_bfloat16* __restrict__ out_b) {
   extern __shared__ __align__(1024) uint8_t sm[];
-  uint8_t* sA = sm;
-  uint8_t* sB = sm + 27 * A_BYTES;
+  uint8_t* const stage0 = sm;
+  uint8_t* const stage1 = sm + STAGE_BYTES;
+  uint8_t* sB = sm + 2 * STAGE_BYTES;
   uint64_t* mbar = reinterpret_cast<uint64_t*>(sB + 27 * B_BYTES);
   uint32_t* tslot = reinterpret_cast<uint32_t*>(mbar + 1);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -105,30 +139,26 @@ __global__ void __launch_bounds__(THREADS, 1) k_conv_tc(const __nv_bfloat16* __r
   uint32_t phase = 0;
   bool ok = true;
 
-  for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
-    const int line = tile / tiles_per_line;
-    const int z0 = (tile % tiles_per_line) * TILE_M;
-    const int x = line / N, y = line % N;
-    // A_t: 27 taps x 128 rows x 2 halves of 16 bytes
-    for (int i = tid; i < 27 * TILE_M * 2; i += THREADS) {
-      const int t = i / (TILE_M * 2), r = (i >> 1) % TILE_M, h = i & 1;
-      int xx = x + t / 9 - 1, yy = y + (t / 3) % 3 - 1, zz = z0 + r + t % 3 - 1;
-      xx = xx < 0 ? xx + N : (xx >= N ? xx - N : xx);
-      yy = yy < 0 ? yy + N : (yy >= N ? yy - N : yy);
-      zz = zz < 0 ? zz + N : (zz >= N ? zz - N : zz);
-      const __nv_bfloat16* src = in + (((size_t)xx * N + yy) * N + zz) * C + h * 8;
-      const uint32_t dst = smem_u32(sA + t * A_BYTES + cm_off(r, h * 8));
-      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" :: "r"(dst), "l"(src) : "memory");
-    }
+  int tile = blockIdx.x;
+  if (tile < ntiles) gather(in, N, tile, stage0);
+  asm volatile("cp.async.commit_group;" ::: "memory");
+  for (int it = 0; tile < ntiles && ok; tile += gridDim.x, it++) {
+    // the next tile's lines load while this tile multiplies; that buffer's
+    // previous MMAs completed before the last iteration's epilogue
+    const int next = tile + gridDim.x;
+    if (next < ntiles) gather(in, N, next, (it & 1) ? stage0 : stage1);
     asm volatile("cp.async.commit_group;" ::: "memory");
-    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    asm volatile("cp.async.wait_group 1;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     if (tid == 0) {
+      const uint8_t* s = (it & 1) ? stage1 : stage0;
       for (int t = 0; t < 27; t++) {
-        const uint64_t da = umma_desc(smem_u32(sA + t * A_BYTES));
-        const uint64_t db = umma_desc(smem_u32(sB + t * B_BYTES));
+        // tap (dx, dy, dz): line t / 3, started dz = t % 3 rows on
+        const uint64_t da =
+            umma_desc(smem_u32(s + (t / 3) * LINE_BYTES + (t % 3) * 16), HALF_BYTES, 128);
+        const uint64_t db = umma_desc(smem_u32(sB + t * B_BYTES), 128, 256);
         const uint32_t acc = t > 0 ? 1u : 0u;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
@@ -148,6 +178,8 @@ __global__ void __launch_bounds__(THREADS, 1) k_conv_tc(const __nv_bfloat16* __r
     phase ^= 1u;
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     if (ok) {
+      const int line = tile / tiles_per_line;
+      const int z0 = (tile % tiles_per_line) * TILE_M;
       uint32_t r[16];
       const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16);
       asm volatile(
@@ -158,7 +190,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_conv_tc(const __nv_bfloat16* __r
             "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
           : "r"(taddr));
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-      const size_t v = ((size_t)x * N + y) * N + z0 + warp * 32 + lane;
+      const size_t v = (size_t)line * N + z0 + warp * 32 + lane;
       float o[C];
 #pragma unroll
       for (int c = 0; c < C; c++) {
@@ -169,7 +201,8 @@ __global__ void __launch_bounds__(THREADS, 1) k_conv_tc(const __nv_bfloat16* __r
       if (out_f) {
         float4* d = reinterpret_cast<float4*>(out_f + v * C);
 #pragma unroll
-        for (int q = 0; q < 4; q++) d[q] = make_float4(o[4 * q], o[4 * q + 1], o[4 * q + 2], o[4 * q + 3]);
+        for (int q = 0; q < 4; q++)
+          d[q] = make_float4(o[4 * q], o[4 * q + 1], o[4 * q + 2], o[4 * q + 3]);
       }
       if (out_b) {
         __nv_bfloat16 hb[C];
@@ -183,6 +216,8 @@ __global__ void __launch_bounds__(THREADS, 1) k_conv_tc(const __nv_bfloat16* __r
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
   }
+  // copies still in flight (a prefetch after a timeout) finish before exit
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   if (warp == 0)
@@ -205,7 +240,7 @@ cudaError_t launch(const __nv_bfloat16* in, int N, const __nv_bfloat16* w, const
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const int grid = ntiles < sms ? ntiles : sms;
+  const int grid = ntiles < CTAS_PER_SM * sms ? ntiles : CTAS_PER_SM * sms;
   prof_mark(st, CG_ST_OTHER);
   k_conv_tc<FLIP><<<grid, THREADS, SMEM, st>>>(in, N, w, bias, act, of, ob);
   return cudaGetLastError();

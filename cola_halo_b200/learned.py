@@ -143,7 +143,8 @@ def evaluate(nc, boxsize, sched, net, train_seeds, eval_seeds, table, *, omega_m
              epochs=1, lr=2e-3, log=None):
     """Train on PM pairs, then judge plain-coarse and learned-coarse runs
     against the plain factor-3 run on held-out seeds: P(k) error up to half
-    the particle Nyquist wavenumber, and device wall time per run."""
+    the particle Nyquist wavenumber, and the device time of each run's time
+    loop (with the host wall time beside it)."""
     import time
 
     from .sim import Simulation
@@ -157,26 +158,39 @@ def evaluate(nc, boxsize, sched, net, train_seeds, eval_seeds, table, *, omega_m
     res = {"train_s": train_s, "train_steps": len(hist), "loss_first": float(np.mean(hist[:10])),
            "loss_last": float(np.mean(hist[-10:])), "seeds": []}
 
-    def timed(fn):
-        fine.sync()
-        coarse.sync()
+    lib = _lib.load()
+    nst = _lib.NSTAGES
+
+    def timed_run(sim, force):
+        """The time loop up to the z = 0 output (its 11 force evaluations,
+        kicks and drifts), timed on the device: the library's event profile
+        spans the first launch to the last.  The snapshot itself (a download
+        of the same size for every method) is taken after the timed region."""
+        sim.sync()
+        _lib.check(lib.cg_prof_begin(8192), "cg_prof_begin")
         t = time.perf_counter()
-        out = fn()
-        fine.sync()
-        coarse.sync()
-        return out, time.perf_counter() - t
+        run_time_loop(sched, output_scale_factors((0.0,)), move=sim.move, force=force,
+                      kick=sim.kick, drift=sim.drift, snapshot=lambda a, i: None)
+        ms = (ctypes.c_double * nst)()
+        cnt = (ctypes.c_int * nst)()
+        lib.cg_prof_end(ms, cnt, nst)
+        wall = time.perf_counter() - t
+        snap = sim.snapshot(output_scale_factors((0.0,))[0])
+        return snap, sum(ms) / 1e3, wall
+
     for seed in eval_seeds:
         p = _lpt_particles(nc, boxsize, seed, omega_m, sched.a_init, table)
         fine.set_particles(p, sched.a_init, sched.a_init)
-        s_f, t_f = timed(lambda: fine.run(sched)[-1][1])
+        s_f, t_f, w_f = timed_run(fine, fine.forces)
         coarse.set_particles(p, sched.a_init, sched.a_init)
-        s_c, t_c = timed(lambda: coarse.run(sched)[-1][1])
+        s_c, t_c, w_c = timed_run(coarse, coarse.forces)
         coarse.set_particles(p, sched.a_init, sched.a_init)
-        s_l, t_l = timed(lambda: net.run(coarse, sched)[-1][1])
+        s_l, t_l, w_l = timed_run(coarse, lambda: net.forces(coarse))
         k, pf, _ = power_spectrum_on(fine, s_f["x"], 1.0)
         _, pc, _ = power_spectrum_on(fine, s_c["x"], 1.0)
         _, pl, _ = power_spectrum_on(fine, s_l["x"], 1.0)
         r = {"seed": seed, "fine_s": t_f, "coarse_s": t_c, "learned_s": t_l,
+             "fine_wall_s": w_f, "coarse_wall_s": w_c, "learned_wall_s": w_l,
              "err_coarse": pk_error(k, pc, pf, kmax), "err_learned": pk_error(k, pl, pf, kmax)}
         res["seeds"].append(r)
         if log:
