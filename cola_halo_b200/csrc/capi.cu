@@ -892,3 +892,6 @@ extern "C" int lpt_set_displacement(const double InitTime, const double omega_m,
 }
 
 int cg_set_error_from_lpt(int code, const char* msg) { return set_err(code, "%s", msg); }
+// The drop-in failure path (msg_abort semantics) for drop-in entry points
+// defined in other translation units.
+void cg_dropin_error(int code, const char* msg) { dropin_fail(code, "%s", msg); }

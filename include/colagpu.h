@@ -205,6 +205,23 @@ int cg_batch_last_ms(cg_batch* b, float* ms);
 int cg_fft_r2c(int n, const float* real_in, float* spec_out);
 int cg_fft_c2r(int n, const float* spec_in, float* real_out);
 
+/* Friends-of-friends halos (fof.c:427-1181 on one process).  pmin: np
+ * reference ParticleMinimum structs (32 B: x, v, id) in host or device
+ * memory, positions within one box length of [0, L).  Particles closer than
+ * ll are linked (periodic box of side boxsize); groups of at least
+ * nfof_min members are halos: member count, centre (a member plus the mean
+ * minimum-image offset, wrapped into [0, L)) and mean velocity.  Halos come
+ * in the order of each group's smallest particle index.  Up to max_halos
+ * are written to `halos` (may be NULL); *nhalo receives the total count.
+ * Synchronous; allocates and frees its own device scratch. */
+typedef struct {
+  int nfof;
+  float x[3];
+  float v[3];
+} cg_halo;
+int cg_fof(const void* pmin, long long np, float boxsize, float ll, int nfof_min,
+           cg_halo* halos, long long max_halos, long long* nhalo);
+
 /* FFT schedule autotuner (no reference counterpart).  From 256 up each
  * mesh size has several compiled variants of the strided x pass (ky columns
  * per CTA, maximum radix) and, up to 768, of the fused y Green pass (lines

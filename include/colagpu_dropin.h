@@ -107,6 +107,23 @@ double PowerSpec(const double k);
 /* power.h:6 (power.c:199-202) */
 double GrowthFactor(double astart, double aend);
 
+/* fof.h:6 (fof.c:973-988): bytes the reference wants in mem1 for the halo
+ * finder.  Returned for callers that size their arena with it; the GPU
+ * finder keeps its own device buffers. */
+size_t fof_calc_memory(const int np_alloc, const int nc);
+/* fof.h:7 (fof.c:990-1033).  mem / mem_size are accepted and not used. */
+void fof_init(const int np_alloc, const int nc, void* mem, size_t mem_size);
+/* fof.h:8 (fof.c:1035-1084): friends-of-friends halos of the snapshot's
+ * particles with linking length ll, on the GPU.  Wraps the snapshot's
+ * positions into the box in place, as the reference does; unlike the
+ * reference it leaves the particle order unchanged (the reference sorts
+ * them into its k-d tree). */
+void fof_find_halos(Snapshot* snapshot, const float ll);
+/* fof.h:10 (fof.c:1086-1181): the halos of the last fof_find_halos with
+ * at least 32 members, one line each, "nfof x y z vx vy vz" in the
+ * reference's format. */
+void fof_write_halos(char filename[]);
+
 /* Residency and error controls of the drop-in layer (no reference
  * counterpart). */
 int cg_particles_upload(Particles* particles);

@@ -3,7 +3,8 @@
 The library is the reference's own C code (unchanged) linked against the
 project's shims; see oracle/Makefile.  The functions bound here are the
 reference's public hot-path entry points (pm.h:6-11, cola.h:7-18,
-lpt.h:6-8, power.h:4-6, move.h:7, comm.h:8, msg.h:4-9, timer.h:4-10).
+lpt.h:6-8, power.h:4-6, move.h:7, comm.h:8, msg.h:4-9, timer.h:4-10) and the
+friends-of-friends halo finder (fof.h:6-10).
 """
 import ctypes
 import os
@@ -51,6 +52,10 @@ def load():
         "cola_drift": (None, [P, f, f]),
         "cola_set_snapshot": (None, [d, P, P]),
         "move_particles2": (None, [P, f, P, sz]),
+        "fof_calc_memory": (sz, [i, i]),
+        "fof_init": (None, [i, i, P, sz]),
+        "fof_find_halos": (None, [P, f]),
+        "fof_write_halos": (None, [ctypes.c_char_p]),
         "growthD": (f, [f]),
         "growthD2": (f, [f]),
         "Sq": (d, [d, d, d]),
@@ -93,3 +98,27 @@ def set_cola_omega(omega_m):
     p.a_x = 0.5
     p.a_v = 0.5
     lib.cola_kick(ctypes.byref(p), omega_m, 0.5)
+
+
+def fof_catalog(pmin, boxsize, nc, ll, workdir):
+    """Halos of ParticleMinimum array `pmin` by the reference's own
+    fof_find_halos + fof_write_halos (fof.c:1035-1181, one rank), read back
+    from the text file it writes: an array of (nfof, x[3], v[3]) rows in
+    the file's order.  `pmin` is not modified."""
+    import numpy as np
+    from cola_halo_b200.types import HostSnapshot
+    lib = load()
+    n = len(pmin)
+    lib.comm_init(nc, nc, boxsize)
+    np_alloc = int(1.25 * n) + 16
+    size = lib.fof_calc_memory(np_alloc, nc)
+    mem = np.zeros(size + 64, dtype=np.uint8)
+    lib.fof_init(np_alloc, nc, mem.ctypes.data, size)
+    snap = HostSnapshot(nc, np_alloc, boxsize, 0.3)
+    snap.p[:n] = pmin
+    snap.struct.np_local = n
+    lib.fof_find_halos(snap.ptr, ll)
+    path = os.path.join(workdir, "fof_ref.txt")
+    lib.fof_write_halos(path.encode())
+    rows = np.loadtxt(path, ndmin=2) if os.path.getsize(path) else np.zeros((0, 7))
+    return rows

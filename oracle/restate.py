@@ -665,3 +665,56 @@ class OracleRun:
         pos, vel = cola_set_snapshot(self.x, self.v, self.f, self.dx1, self.dx2,
                                      self.a_x, self.a_v, aout, self.ct)
         self.snapshots.append((aout, pos, vel))
+
+
+# --------------------------------------------------------------------------
+# Friends-of-friends halos (fof.c:427-1181 on one rank).
+def fof_halos(x, v, boxsize, ll, nfof_min=32):
+    """Periodic friends-of-friends: particles closer than `ll` (strict,
+    squared distance in float32 as kdFoF forms it, fof.c:569-572) are
+    linked; groups of at least nfof_min (fof.c:224) are halos.  Positions
+    are wrapped into the box first (move_particles2_min, fof.c:1042).
+    Returns rows (nfof, x[3], v[3]) with the halo centre = one member plus
+    the mean minimum-image offset of all members, wrapped into [0, L)
+    (fof.c:287-322, 1141-1150), and the mean velocity; sorted by
+    (nfof, x, y, z)."""
+    from scipy.sparse import coo_matrix
+    from scipy.sparse.csgraph import connected_components
+    from scipy.spatial import cKDTree
+    L = f32(boxsize)
+    x = wrap(np.asarray(x, dtype=f32), L)
+    n = len(x)
+    if n == 0:
+        return np.zeros((0, 7))
+    # candidates within ll (inclusive, in float64), then the float32 test
+    xs = np.where(x >= L, np.nextafter(L, f32(0)), x).astype(np.float64)
+    tree = cKDTree(xs, boxsize=float(L) + 1e-9)
+    pairs = tree.query_pairs(r=float(ll) * (1 + 1e-6), output_type="ndarray")
+    keep = np.zeros(len(pairs), dtype=bool)
+    if len(pairs):
+        a, b = pairs[:, 0], pairs[:, 1]
+        d = x[a] - x[b]
+        half = f32(0.5) * L
+        d = np.where(d > half, (x[a] - L) - x[b], np.where(d < -half, (x[b] - L) - x[a], d))
+        d = d.astype(f32)
+        d2 = ((d[:, 0] * d[:, 0]).astype(f32) + (d[:, 1] * d[:, 1]).astype(f32)).astype(f32)
+        d2 = (d2 + (d[:, 2] * d[:, 2]).astype(f32)).astype(f32)
+        keep = d2 < f32(ll) * f32(ll)
+        pairs = pairs[keep]
+    g = coo_matrix((np.ones(len(pairs)), (pairs[:, 0], pairs[:, 1])), shape=(n, n))
+    ncomp, lab = connected_components(g, directed=False)
+    sizes = np.bincount(lab, minlength=ncomp)
+    rows = []
+    v = np.asarray(v, dtype=np.float64)
+    for c in np.nonzero(sizes >= nfof_min)[0]:
+        idx = np.nonzero(lab == c)[0]
+        x0 = x[idx[0]].astype(np.float64)
+        dx = x[idx].astype(np.float64) - x0
+        dx = np.where(dx > 0.5 * float(L), dx - float(L), np.where(dx < -0.5 * float(L), dx + float(L), dx))
+        c0 = x0 + dx.mean(axis=0)
+        c0 = np.where(c0 < 0, c0 + float(L), c0)
+        c0 = np.where(c0 >= float(L), c0 - float(L), c0)
+        rows.append([len(idx), *c0, *v[idx].mean(axis=0)])
+    rows = np.array(rows).reshape(-1, 7)
+    order = np.lexsort((rows[:, 3], rows[:, 2], rows[:, 1], rows[:, 0]))
+    return rows[order]

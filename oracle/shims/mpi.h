@@ -6,7 +6,8 @@
  * world of size 1: point-to-point calls to "self" and every collective reduce
  * to a copy of the send buffer into the receive buffer.  Only the API surface
  * the reference's hot path uses is provided (pm.c:150-159,461-472,494,520-545;
- * move.c:87-168; comm.c:39-177; lpt.c:566; power.c:43-58; msg.c:36-45).
+ * move.c:87-168; comm.c:39-177; lpt.c:566; power.c:43-58; msg.c:36-45;
+ * fof.c:669,855-889,1094-1121 for the gathers of the halo finder).
  */
 #ifndef ORACLE_SHIM_MPI_H
 #define ORACLE_SHIM_MPI_H
@@ -56,6 +57,13 @@ int MPI_Bcast(void* buffer, int count, MPI_Datatype datatype, int root,
 int MPI_Allgather(const void* sendbuf, int sendcount, MPI_Datatype sendtype,
                   void* recvbuf, int recvcount, MPI_Datatype recvtype,
                   MPI_Comm comm);
+int MPI_Gather(const void* sendbuf, int sendcount, MPI_Datatype sendtype,
+               void* recvbuf, int recvcount, MPI_Datatype recvtype, int root,
+               MPI_Comm comm);
+/* rank 0 of one: the send buffer lands at recvbuf + displs[0] elements */
+int MPI_Gatherv(const void* sendbuf, int sendcount, MPI_Datatype sendtype,
+                void* recvbuf, const int* recvcounts, const int* displs,
+                MPI_Datatype recvtype, int root, MPI_Comm comm);
 
 /* Test hook: the exit code of the last MPI_Abort is reported through this
  * callback when one is installed (so a ctypes caller can turn an abort into a

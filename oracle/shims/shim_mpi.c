@@ -95,3 +95,22 @@ int MPI_Allgather(const void* sendbuf, int sendcount, MPI_Datatype sendtype,
   if (n && sendbuf != recvbuf) memmove(recvbuf, sendbuf, n);
   return MPI_SUCCESS;
 }
+
+int MPI_Gather(const void* sendbuf, int sendcount, MPI_Datatype sendtype,
+               void* recvbuf, int recvcount, MPI_Datatype recvtype, int root,
+               MPI_Comm comm)
+{
+  (void)root;
+  return MPI_Allgather(sendbuf, sendcount, sendtype, recvbuf, recvcount, recvtype, comm);
+}
+
+int MPI_Gatherv(const void* sendbuf, int sendcount, MPI_Datatype sendtype,
+                void* recvbuf, const int* recvcounts, const int* displs,
+                MPI_Datatype recvtype, int root, MPI_Comm comm)
+{
+  (void)recvcounts; (void)root; (void)comm;
+  size_t n = (size_t)sendcount * type_size(sendtype);
+  char* dst = (char*)recvbuf + (size_t)(displs ? displs[0] : 0) * type_size(recvtype);
+  if (n && (const void*)dst != sendbuf) memmove(dst, sendbuf, n);
+  return MPI_SUCCESS;
+}
