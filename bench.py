@@ -513,6 +513,8 @@ def main():
     ap.add_argument("--train-seeds", type=int, default=16)
     ap.add_argument("--eval-seeds", type=int, default=8)
     ap.add_argument("--epochs", type=int, default=3)
+    ap.add_argument("--fof", action="store_true",
+                    help="friends-of-friends halo finding on the z = 0 snapshot (b = 0.2)")
     ap.add_argument("--batch", action="store_true",
                     help="batched realizations: 32 x 128^3 particles / 384^3 meshes, uneven "
                          "boxes and step counts, one CUDA graph per run")
@@ -523,12 +525,89 @@ def main():
         return run_learned(args)
     if args.batch:
         return run_batch(args)
+    if args.fof:
+        return run_fof(args)
     cfg = CONFIGS[args.config]
     args.config_desc = "%d^3 particles, %d^3 mesh, L=%g Mpc/h, BBKS, 2LPT z=49, 10 steps" % (
         cfg["nc"], cfg["nc"] * cfg["factor"], cfg["L"])
     if args.impl == "reference":
         return run_reference(args, cfg)
     return run_b200(args, cfg)
+
+
+def _z0_snapshot(lib, cfg, table):
+    """The z = 0 snapshot (host ParticleMinimum array) of one realization."""
+    from cola_halo_b200 import Simulation
+    from cola_halo_b200.learned import _lpt_particles
+    from cola_halo_b200.schedule import Schedule
+    nc, L, om = cfg["nc"], cfg["L"], cfg["om"]
+    sched = Schedule.linear(cfg["a_init"], 1.0, cfg["nsteps"])
+    p = _lpt_particles(nc, L, cfg["seed"], om, sched.a_init, table)
+    sim = Simulation(nc, nc * cfg["factor"], L, om)
+    sim.set_particles(p, sched.a_init, sched.a_init)
+    snap = sim.run(sched)[-1][1]
+    sim.close()
+    return snap
+
+
+def run_fof(args):
+    """Friends-of-friends (b = 0.2, >= 32 members) on the z = 0 snapshot of
+    the 256^3 and 128^3 workloads: particles per second of one synchronous
+    cg_fof call on a device-resident snapshot (its scratch allocation and
+    the catalogue download included; median of the timed calls), and the
+    reference's own fof.c on the 128^3 snapshot on one host core."""
+    rank, world, local = dist_setup(args)
+    if rank != 0:
+        return 0
+    from cola_halo_b200 import _lib
+    from cola_halo_b200.bbks import write_bbks_table
+    from cola_halo_b200.halos import fof
+    lib = _lib.load()
+    _lib.check(lib.cg_set_device(local), "cg_set_device")
+    cuda = Cudart()
+    table = write_bbks_table(os.path.join(tempfile.mkdtemp(), "bbks.dat"))
+    out = {"metric": "FoF particles/s", "unit": "particles/s", "higher_is_better": True,
+           "n_gpus": 1, "dtype": "f32", "data": "synthetic (seeded 2LPT initial conditions, "
+           "BBKS P(k), 10 COLA steps to z = 0)", "runs": {}}
+    for name in ("c2", "c3"):
+        cfg = CONFIGS[name]
+        nc, L = cfg["nc"], cfg["L"]
+        ll = float(np.float32(0.2 * L / nc))
+        snap = _z0_snapshot(lib, cfg, table)
+        d = cuda.device_copy_of(snap)
+        for _ in range(max(args.warmup, 1)):
+            halos = fof(d.value, L, ll, np_count=len(snap))
+        times = []
+        for _ in range(args.steps):
+            cuda.sync_device()
+            t0 = time.perf_counter()
+            halos = fof(d.value, L, ll, np_count=len(snap))
+            times.append(time.perf_counter() - t0)
+        wall_s = float(np.median(times))
+        run = {"particles": len(snap), "boxsize": L, "ll": ll, "halos": int(len(halos)),
+               "largest": int(halos["nfof"].max()) if len(halos) else 0,
+               "wall_s": wall_s, "particles_per_s": len(snap) / wall_s}
+        if name == "c3" and not args.no_cpu_baseline:
+            try:
+                from oracle import ref
+                if os.path.exists(ref.LIB_PATH):
+                    t0 = time.perf_counter()
+                    rows = ref.fof_catalog(snap, L, nc, np.float32(ll), tempfile.mkdtemp())
+                    cpu_s = time.perf_counter() - t0
+                    run["cpu_reference_s"] = cpu_s
+                    run["cpu_reference_halos"] = int(len(rows))
+                    out["cpu_baseline"] = {"value": len(snap) / cpu_s, "unit": "particles/s",
+                                           "cores": 1, "kind": "reference",
+                                           "sample": "fof.c (k-d tree, one thread) on the "
+                                                     "128^3 z = 0 snapshot"}
+            except Exception as e:  # reported, not fatal
+                run["cpu_reference_error"] = str(e)
+        out["runs"][name] = run
+    out["value"] = out["runs"]["c2"]["particles_per_s"]
+    out["config"] = {"workload": "FoF b = 0.2 on the 256^3 / L = 600 z = 0 snapshot "
+                                 "(value) and the 128^3 / L = 300 one"}
+    print(json.dumps(out))
+    return 0
 
 
 def run_batch(args):
@@ -603,7 +682,7 @@ def run_learned(args):
     P(k) error up to 0.5 k_Nyq and wall time per realization."""
     from cola_halo_b200 import _lib
     from cola_halo_b200.bbks import write_bbks_table
-    from cola_halo_b200.learned import ConvNet, evaluate
+    from cola_halo_b200.learned import MF_EDGES, ConvNet, evaluate
     from cola_halo_b200.schedule import Schedule
     lib = _lib.load()
     _lib.check(lib.cg_set_device(0), "cg_set_device")
@@ -638,6 +717,13 @@ def run_learned(args):
            "pk_err_learned": err_l,
            "pk_err_coarse": float(np.mean([r["err_coarse"] for r in seeds])),
            "pk_err_learned_max": float(np.max([r["err_learned"] for r in seeds])),
+           "mass_function": {"log10_nfof_edges": [round(float(e), 4) for e in MF_EDGES],
+                             "fine": res.get("mf_fine"), "coarse": res.get("mf_coarse"),
+                             "learned": res.get("mf_learned"),
+                             "ratio_err_coarse": res.get("mf_err_coarse"),
+                             "ratio_err_learned": res.get("mf_err_learned"),
+                             "halo_finder": "GPU FoF (cg_fof), b = 0.2, >= 32 members, "
+                                            "summed over the evaluation seeds"},
            "train_s": res["train_s"], "train_steps": res["train_steps"],
            "loss_first": res["loss_first"], "loss_last": res["loss_last"]}
     print(json.dumps(out))

@@ -133,6 +133,28 @@ def power_spectrum_on(sim_pk, snap_x, a):
     return sim_pk.power_spectrum(deconvolve_cic=True, subtract_shot=True)
 
 
+# log10(members) bin edges of the halo mass function: 32 members up, 0.25 dex
+MF_EDGES = np.log10(32.0) + 0.25 * np.arange(13)
+
+
+def halo_counts(snap, boxsize, nc, b=0.2):
+    """FoF (b = 0.2 of the mean particle spacing, >= 32 members, fof.c) halo
+    counts of a snapshot in the MF_EDGES log-mass bins (mass in particles)."""
+    from .halos import fof
+    ll = float(np.float32(b * boxsize / nc))
+    h = fof(snap, boxsize, ll)
+    return np.histogram(np.log10(h["nfof"].astype(np.float64)), bins=MF_EDGES)[0]
+
+
+def mf_ratio_error(counts, counts_ref, min_ref=20):
+    """max over bins with at least `min_ref` reference halos of
+    |N / N_ref - 1|."""
+    ok = counts_ref >= min_ref
+    if not ok.any():
+        return float("nan")
+    return float(np.max(np.abs(counts[ok] / counts_ref[ok] - 1.0)))
+
+
 def pk_error(k, p, p_ref, kmax):
     """max over bins with 0 < k <= kmax of |P/P_ref - 1|."""
     ok = (k > 0) & (k <= kmax) & (p_ref > 0)
@@ -189,12 +211,23 @@ def evaluate(nc, boxsize, sched, net, train_seeds, eval_seeds, table, *, omega_m
         k, pf, _ = power_spectrum_on(fine, s_f["x"], 1.0)
         _, pc, _ = power_spectrum_on(fine, s_c["x"], 1.0)
         _, pl, _ = power_spectrum_on(fine, s_l["x"], 1.0)
+        mf_f, mf_c, mf_l = (halo_counts(s, boxsize, nc) for s in (s_f, s_c, s_l))
+        res["mf_fine"] = res.get("mf_fine", 0) + mf_f
+        res["mf_coarse"] = res.get("mf_coarse", 0) + mf_c
+        res["mf_learned"] = res.get("mf_learned", 0) + mf_l
         r = {"seed": seed, "fine_s": t_f, "coarse_s": t_c, "learned_s": t_l,
              "fine_wall_s": w_f, "coarse_wall_s": w_c, "learned_wall_s": w_l,
-             "err_coarse": pk_error(k, pc, pf, kmax), "err_learned": pk_error(k, pl, pf, kmax)}
+             "err_coarse": pk_error(k, pc, pf, kmax), "err_learned": pk_error(k, pl, pf, kmax),
+             "halos_fine": int(mf_f.sum()), "halos_coarse": int(mf_c.sum()),
+             "halos_learned": int(mf_l.sum())}
         res["seeds"].append(r)
         if log:
             log(str(r))
     fine.close()
     coarse.close()
+    if "mf_fine" in res:
+        res["mf_err_coarse"] = mf_ratio_error(res["mf_coarse"], res["mf_fine"])
+        res["mf_err_learned"] = mf_ratio_error(res["mf_learned"], res["mf_fine"])
+        for key in ("mf_fine", "mf_coarse", "mf_learned"):
+            res[key] = [int(c) for c in res[key]]
     return res
