@@ -42,6 +42,7 @@ SIGNATURES = {
     "cg_sim_forces": (i32, [P, dptr]),
     "cg_sim_kick": (i32, [P, f32]),
     "cg_sim_drift": (i32, [P, f32]),
+    "cg_sim_kick_drift": (i32, [P, f32, f32]),
     "cg_sim_kick_coeffs": (i32, [P, f32, f32, f32]),
     "cg_sim_drift_coeffs": (i32, [P, f32, f32, f32]),
     "cg_sim_snapshot": (i32, [P, f64, f32, P]),
@@ -139,7 +140,7 @@ def load(build_if_missing=True):
     return lib
 
 
-NSTAGES = 14   # CG_ST_COUNT in csrc/internal.h
+NSTAGES = 15   # CG_ST_COUNT in csrc/internal.h
 
 
 def check(rc, what=""):

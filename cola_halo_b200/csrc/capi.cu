@@ -280,6 +280,23 @@ extern "C" int cg_sim_drift(cg_sim* s, float apos1) {
   return CG_OK;
 }
 
+// cg_sim_kick(avel1) then cg_sim_drift(apos1) in one pass over the particles.
+extern "C" int cg_sim_kick_drift(cg_sim* s, float avel1, float apos1) {
+  if (!s) return set_err(CG_EINVAL, "cg_sim_kick_drift: NULL");
+  float dda, q1, q2, dyyy, da1, da2;
+  s->ct->kick(s->a_v, s->a_x, avel1, &dda, &q1, &q2);
+  s->ct->drift(s->a_x, avel1, apos1, &dyyy, &da1, &da2);
+  const float* f[3] = {s->ps.f[0], s->ps.f[1], s->ps.f[2]};
+  const float* d1[3] = {s->ps.dx1[0], s->ps.dx1[1], s->ps.dx1[2]};
+  const float* d2[3] = {s->ps.dx2[0], s->ps.dx2[1], s->ps.dx2[2]};
+  CG_CHECK(dev_kick_drift(s->ps.x, s->ps.v, f, d1, d2, s->ps.n, s->ct->om32, dda, q1, q2, dyyy,
+                          da1, da2, s->st),
+           "kick_drift");
+  s->a_v = avel1;
+  s->a_x = apos1;
+  return CG_OK;
+}
+
 // cola.c:341-384: coefficients of the final half kick and drift to aout.
 static int queue_snapshot(cg_sim* s, double aout, float omega_m, void* d_out) {
   ColaTime ct(omega_m);

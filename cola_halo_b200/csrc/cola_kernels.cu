@@ -32,11 +32,15 @@ __global__ void __launch_bounds__(T) k_wrap(P3 x, long long n, float L) {
   long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long stride = (long long)gridDim.x * blockDim.x;
   for (; i < n; i += stride) {
+    // the three loads first: the component arrays may alias as far as the
+    // compiler knows, so a store would hold back the next load
+    float v[3];
+#pragma unroll
+    for (int a = 0; a < 3; a++) v[a] = x.p[a][i];
 #pragma unroll
     for (int a = 0; a < 3; a++) {
-      float v = x.p[a][i];
-      if (v < 0.0f) x.p[a][i] = __fadd_rn(v, L);
-      else if (v >= L) x.p[a][i] = __fsub_rn(v, L);
+      if (v[a] < 0.0f) x.p[a][i] = __fadd_rn(v[a], L);
+      else if (v[a] >= L) x.p[a][i] = __fsub_rn(v[a], L);
     }
   }
 }
@@ -55,10 +59,18 @@ __global__ void __launch_bounds__(T) k_kick(P3 v, C3 f, C3 dx1, C3 dx2, long lon
   long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long stride = (long long)gridDim.x * blockDim.x;
   for (; i < n; i += stride) {
+    float fv[3], d1[3], d2[3], vv[3];
 #pragma unroll
     for (int a = 0; a < 3; a++) {
-      const float ax = kick_acc(f.p[a][i], dx1.p[a][i], dx2.p[a][i], c, q1, q2);
-      v.p[a][i] = __fadd_rn(v.p[a][i], __fmul_rn(ax, dda));
+      fv[a] = f.p[a][i];
+      d1[a] = dx1.p[a][i];
+      d2[a] = dx2.p[a][i];
+      vv[a] = v.p[a][i];
+    }
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      const float ax = kick_acc(fv[a], d1[a], d2[a], c, q1, q2);
+      v.p[a][i] = __fadd_rn(vv[a], __fmul_rn(ax, dda));
     }
   }
 }
@@ -69,11 +81,55 @@ __global__ void __launch_bounds__(T) k_drift(P3 x, C3 v, C3 dx1, C3 dx2, long lo
   long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long stride = (long long)gridDim.x * blockDim.x;
   for (; i < n; i += stride) {
+    float xv[3], vv[3], d1[3], d2[3];
 #pragma unroll
     for (int a = 0; a < 3; a++) {
-      const float lpt = __fadd_rn(__fmul_rn(dx1.p[a][i], da1), __fmul_rn(dx2.p[a][i], da2));
-      const float step = __fadd_rn(__fmul_rn(v.p[a][i], dyyy), lpt);
-      x.p[a][i] = __fadd_rn(x.p[a][i], step);
+      xv[a] = x.p[a][i];
+      vv[a] = v.p[a][i];
+      d1[a] = dx1.p[a][i];
+      d2[a] = dx2.p[a][i];
+    }
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      const float lpt = __fadd_rn(__fmul_rn(d1[a], da1), __fmul_rn(d2[a], da2));
+      const float step = __fadd_rn(__fmul_rn(vv[a], dyyy), lpt);
+      x.p[a][i] = __fadd_rn(xv[a], step);
+    }
+  }
+}
+
+// cola_kick then cola_drift of the same particle in one pass (the kick's
+// new velocity feeds the drift, as in the two calls): reads x, v, f, dx1,
+// dx2 once and writes x and v once.  The arithmetic is k_kick's followed by
+// k_drift's, so the results are bit-identical to the two kernels.
+__global__ void __launch_bounds__(T) k_kick_drift(P3 x, P3 v, C3 f, C3 dx1, C3 dx2, long long n,
+                                                  double c, float dda, float q1, float q2,
+                                                  float dyyy, float da1, float da2) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (; i < n; i += stride) {
+    // all 15 loads first (the arrays may alias as far as the compiler
+    // knows, so stores would otherwise hold back the next component's loads)
+    float xv[3], vv[3], fv[3], d1[3], d2[3];
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      xv[a] = x.p[a][i];
+      vv[a] = v.p[a][i];
+      fv[a] = f.p[a][i];
+      d1[a] = dx1.p[a][i];
+      d2[a] = dx2.p[a][i];
+    }
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      const float ax = kick_acc(fv[a], d1[a], d2[a], c, q1, q2);
+      vv[a] = __fadd_rn(vv[a], __fmul_rn(ax, dda));
+      const float lpt = __fadd_rn(__fmul_rn(d1[a], da1), __fmul_rn(d2[a], da2));
+      xv[a] = __fadd_rn(xv[a], __fadd_rn(__fmul_rn(vv[a], dyyy), lpt));
+    }
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      v.p[a][i] = vv[a];
+      x.p[a][i] = xv[a];
     }
   }
 }
@@ -172,6 +228,18 @@ cudaError_t dev_drift(float* const x[3], const float* const v[3], const float* c
                        float da2, cudaStream_t st) {
   prof_mark(st, CG_ST_DRIFT);
   if (n > 0) k_drift<<<grid_for(n), T, 0, st>>>(mk(x), mkc(v), mkc(dx1), mkc(dx2), n, dyyy, da1, da2);
+  return cudaGetLastError();
+}
+
+cudaError_t dev_kick_drift(float* const x[3], float* const v[3], const float* const f[3],
+                           const float* const dx1[3], const float* const dx2[3], long long n,
+                           float omega_m, float dda, float q1, float q2, float dyyy, float da1,
+                           float da2, cudaStream_t st) {
+  const double c = -1.5 * (double)omega_m;
+  prof_mark(st, CG_ST_KICK_DRIFT);
+  if (n > 0)
+    k_kick_drift<<<grid_for(n), T, 0, st>>>(mk(x), mk(v), mkc(f), mkc(dx1), mkc(dx2), n, c, dda,
+                                            q1, q2, dyyy, da1, da2);
   return cudaGetLastError();
 }
 

@@ -10,7 +10,7 @@
 enum {
   CG_ST_FILL = 0, CG_ST_DEPOSIT, CG_ST_FZ, CG_ST_FX_FWD, CG_ST_GREEN, CG_ST_FX_INV,
   CG_ST_ZI, CG_ST_INTERP, CG_ST_WRAP, CG_ST_KICK, CG_ST_DRIFT, CG_ST_SNAPSHOT, CG_ST_LPT,
-  CG_ST_OTHER, CG_ST_COUNT
+  CG_ST_OTHER, CG_ST_KICK_DRIFT, CG_ST_COUNT
 };
 // Call before every kernel launch: counts it and, while a profile is open,
 // records a CUDA event on the launch stream.
@@ -128,6 +128,11 @@ cudaError_t dev_kick(float* const v[3], const float* const f[3],
 cudaError_t dev_drift(float* const x[3], const float* const v[3],
                        const float* const dx1[3], const float* const dx2[3],
                        long long n, float dyyy, float da1, float da2, cudaStream_t st);
+// dev_kick then dev_drift (with the kicked velocity) in one kernel.
+cudaError_t dev_kick_drift(float* const x[3], float* const v[3], const float* const f[3],
+                           const float* const dx1[3], const float* const dx2[3], long long n,
+                           float omega_m, float dda, float q1, float q2, float dyyy, float da1,
+                           float da2, cudaStream_t st);
 cudaError_t dev_snapshot(const float* const x[3], const float* const v[3],
                           const float* const f[3], const float* const dx1[3],
                           const float* const dx2[3], long long n,

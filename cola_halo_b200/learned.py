@@ -74,7 +74,8 @@ class ConvNet:
         snaps = []
         run_time_loop(sched, output_scale_factors(zout), move=coarse.move,
                       force=lambda: self.forces(coarse), kick=coarse.kick, drift=coarse.drift,
-                      snapshot=lambda a, i: snaps.append((a, coarse.snapshot(a))))
+                      snapshot=lambda a, i: snaps.append((a, coarse.snapshot(a))),
+                      kick_drift=coarse.kick_drift)
         return snaps
 
 
@@ -192,7 +193,8 @@ def evaluate(nc, boxsize, sched, net, train_seeds, eval_seeds, table, *, omega_m
         _lib.check(lib.cg_prof_begin(8192), "cg_prof_begin")
         t = time.perf_counter()
         run_time_loop(sched, output_scale_factors((0.0,)), move=sim.move, force=force,
-                      kick=sim.kick, drift=sim.drift, snapshot=lambda a, i: None)
+                      kick=sim.kick, drift=sim.drift, snapshot=lambda a, i: None,
+                      kick_drift=sim.kick_drift)
         ms = (ctypes.c_double * nst)()
         cnt = (ctypes.c_int * nst)()
         lib.cg_prof_end(ms, cnt, nst)

@@ -51,11 +51,13 @@ def output_scale_factors(zout):
     return [float(np.float32(1.0 / (1.0 + z))) for z in zout]
 
 
-def run_time_loop(sched, aout, *, move, force, kick, drift, snapshot):
+def run_time_loop(sched, aout, *, move, force, kick, drift, snapshot, kick_drift=None):
     """Drive one realization's time loop with the reference's control flow.
 
     ``move()``, ``force()``, ``kick(avel1)``, ``drift(apos1)`` and
     ``snapshot(aout, iout)`` are the per-step actions (``main.c:167-205``).
+    ``kick_drift(avel1, apos1)``, when given, replaces a kick and the drift
+    that follows it whenever no output falls between them.
     Returns the list of (event, a) pairs in the order they happened.
     """
     events = []
@@ -74,6 +76,11 @@ def run_time_loop(sched, aout, *, move, force, kick, drift, snapshot):
             iout += 1
         if iout >= nout:
             break
+        if kick_drift is not None and not (iout < nout and apos0 < aout[iout] <= avel1):
+            kick_drift(avel1, apos1)
+            events.append(("kick", avel1))
+            events.append(("drift", apos1))
+            continue
         kick(avel1)
         events.append(("kick", avel1))
         while iout < nout and apos0 < aout[iout] <= avel1:

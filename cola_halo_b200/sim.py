@@ -111,6 +111,10 @@ class Simulation:
     def drift(self, apos1):
         _lib.check(self.lib.cg_sim_drift(self.h, apos1), "cg_sim_drift")
 
+    def kick_drift(self, avel1, apos1):
+        """kick(avel1) then drift(apos1) in one pass (bit-identical)."""
+        _lib.check(self.lib.cg_sim_kick_drift(self.h, avel1, apos1), "cg_sim_kick_drift")
+
     def kick_coeffs(self, dda, q1, q2):
         _lib.check(self.lib.cg_sim_kick_coeffs(self.h, dda, q1, q2), "cg_sim_kick_coeffs")
 
@@ -134,7 +138,8 @@ class Simulation:
         run_time_loop(sched, aout, move=self.move,
                       force=lambda: self.forces(check_density),
                       kick=self.kick, drift=self.drift,
-                      snapshot=lambda a, i: snaps.append((a, self.snapshot(a))))
+                      snapshot=lambda a, i: snaps.append((a, self.snapshot(a))),
+                      kick_drift=self.kick_drift)
         return snaps
 
 

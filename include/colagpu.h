@@ -88,6 +88,10 @@ int cg_sim_kick(cg_sim* s, float avel1);
 int cg_sim_drift(cg_sim* s, float apos1);
 /* The same updates with caller-supplied single-precision coefficients
  * (dda, q1, q2) / (dyyy, da1, da2); they do not change a_x / a_v. */
+/* cg_sim_kick(avel1) followed by cg_sim_drift(apos1) in one pass over the
+ * particles (no reference counterpart; the same results bit for bit, with
+ * one read of the particle state instead of two). */
+int cg_sim_kick_drift(cg_sim* s, float avel1, float apos1);
 int cg_sim_kick_coeffs(cg_sim* s, float dda, float q1, float q2);
 int cg_sim_drift_coeffs(cg_sim* s, float dyyy, float da1, float da2);
 /* cola_set_snapshot (cola.c:341-416) into a host ParticleMinimum array. */

@@ -45,6 +45,27 @@ def test_wrap_kick_drift_bit_exact(gpu_lib):
     np.testing.assert_array_equal(sim.get_particles()["x"], xn)
 
 
+def test_fused_kick_drift_bit_identical(gpu_lib):
+    """cg_sim_kick_drift equals cg_sim_kick followed by cg_sim_drift."""
+    from cola_halo_b200 import Simulation
+    nc, L = 16, 100.0
+    p = _state(nc ** 3, L, 2)
+    sim = Simulation(nc, 48, L, OM)
+    sim.set_particles(p, 0.3, 0.35)
+    sim.move()
+    sim.forces()              # float atomics: computed once, used by both paths
+    sim.kick(0.4)
+    sim.drift(0.45)
+    pa, ta = sim.get_particles(), sim.times()
+    sim.set_particles(p, 0.3, 0.35)      # same state, the forces stay
+    sim.move()
+    sim.kick_drift(0.4, 0.45)
+    pb, tb = sim.get_particles(), sim.times()
+    np.testing.assert_array_equal(pa["x"], pb["x"])
+    np.testing.assert_array_equal(pa["v"], pb["v"])
+    assert ta == tb
+
+
 def test_kick_drift_coefficients_match_oracle(gpu_lib):
     """The library's double-precision host coefficients (cola.c:77-134)."""
     from cola_halo_b200 import drift_coeffs, kick_coeffs
