@@ -226,6 +226,15 @@ typedef struct {
 int cg_fof(const void* pmin, long long np, float boxsize, float ll, int nfof_min,
            cg_halo* halos, long long max_halos, long long* nhalo);
 
+/* Coarse density grid (coarse_grid.c:17-121): CIC assignment of np
+ * ParticleMinimum (host or device memory) onto an nc^3 grid [x][y][z] of a
+ * periodic box, then delta = nc^3 / np_total * rho - 1, all in float with
+ * the reference's weight arithmetic.  delta_out (nc^3 floats, host or
+ * device) receives the contrast; *mass_sum (may be NULL) the sum of rho in
+ * double.  Synchronous; allocates and frees its own device grid. */
+int cg_coarse_grid(const void* pmin, long long np, long long np_total, float boxsize, int nc,
+                   float* delta_out, double* mass_sum);
+
 /* FFT schedule autotuner (no reference counterpart).  From 256 up each
  * mesh size has several compiled variants of the strided x pass (ky columns
  * per CTA, maximum radix) and, up to 768, of the fused y Green pass (lines

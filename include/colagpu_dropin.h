@@ -124,6 +124,13 @@ void fof_find_halos(Snapshot* snapshot, const float ll);
  * reference's format. */
 void fof_write_halos(char filename[]);
 
+/* coarse_grid.h:6 (coarse_grid.c:17-121): CIC density contrast of the
+ * snapshot's particles on an nc^3 grid, written as [float boxsize][int nc]
+ * [nc^3 float delta, x slowest][int nc].  The grid is assigned on the GPU;
+ * mem1 / size1 are accepted and not used. */
+void coarse_grid2(const char filename[], Snapshot const* const snapshot, const int nc,
+                  void* const mem1, const size_t size1);
+
 /* Residency and error controls of the drop-in layer (no reference
  * counterpart). */
 int cg_particles_upload(Particles* particles);

@@ -56,6 +56,7 @@ def load():
         "fof_init": (None, [i, i, P, sz]),
         "fof_find_halos": (None, [P, f]),
         "fof_write_halos": (None, [ctypes.c_char_p]),
+        "coarse_grid2": (None, [ctypes.c_char_p, P, i, P, sz]),
         "growthD": (f, [f]),
         "growthD2": (f, [f]),
         "Sq": (d, [d, d, d]),
@@ -122,3 +123,34 @@ def fof_catalog(pmin, boxsize, nc, ll, workdir):
     lib.fof_write_halos(path.encode())
     rows = np.loadtxt(path, ndmin=2) if os.path.getsize(path) else np.zeros((0, 7))
     return rows
+
+
+def read_grid_file(path):
+    """(boxsize, delta[nc, nc, nc]) of a coarse-grid file (coarse_grid.c:46-91:
+    float boxsize, int nc, nc^3 float delta with x slowest, int nc)."""
+    import numpy as np
+    raw = open(path, "rb").read()
+    L = np.frombuffer(raw, np.float32, 1, 0)[0]
+    nc = int(np.frombuffer(raw, np.int32, 1, 4)[0])
+    ng = nc * nc * nc
+    assert len(raw) == 12 + 4 * ng, "coarse grid file size"
+    assert int(np.frombuffer(raw, np.int32, 1, 8 + 4 * ng)[0]) == nc, "coarse grid trailer"
+    return L, np.frombuffer(raw, np.float32, ng, 8).reshape(nc, nc, nc).copy()
+
+
+def coarse_grid_file(pmin, boxsize, nc, path, np_total=None):
+    """The reference's coarse_grid2 (coarse_grid.c:17-93, one rank) on
+    ParticleMinimum array `pmin`, written to `path`; returns read_grid_file."""
+    import numpy as np
+    from cola_halo_b200.types import HostSnapshot
+    lib = load()
+    n = len(pmin)
+    lib.comm_init(max(nc, 1), max(nc, 1), boxsize)
+    snap = HostSnapshot(nc, max(n, 1), boxsize, 0.3)
+    snap.p[:n] = pmin
+    snap.struct.np_local = n
+    snap.struct.np_total = n if np_total is None else np_total
+    size = 4 * nc * nc * (nc + 16)
+    mem = np.zeros(size // 4 + 16, dtype=np.float32)
+    lib.coarse_grid2(path.encode(), snap.ptr, nc, mem.ctypes.data, size)
+    return read_grid_file(path)

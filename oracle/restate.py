@@ -718,3 +718,45 @@ def fof_halos(x, v, boxsize, ll, nfof_min=32):
     rows = np.array(rows).reshape(-1, 7)
     order = np.lexsort((rows[:, 3], rows[:, 2], rows[:, 1], rows[:, 0]))
     return rows[order]
+
+
+# --------------------------------------------------------------------------
+# Coarse density grid (coarse_grid.c:17-121 on one rank).
+def coarse_grid(x, boxsize, nc, np_total=None):
+    """CIC density contrast on an nc^3 grid [x][y][z].  Float32 throughout in
+    the reference's operation order: s = x * (nc / L), ix = floor(s), left
+    weight w = 1 - (s - ix), periodic neighbours (coarse_grid.c:96-108), the
+    eight products formed left to right and added particle by particle,
+    corner by corner (coarse_grid.c:110-120); then delta = nbar_inv * rho - 1
+    with nbar_inv = (double) nc^3 / np_total rounded to float
+    (coarse_grid.c:51, 70-73).  Returns (delta, sum of rho in float64)."""
+    x = np.asarray(x, dtype=f32).reshape(-1, 3)
+    n = len(x)
+    ng = nc * nc * nc
+    dx_inv = f32(nc) / f32(boxsize)
+    s = x * dx_inv
+    ix = np.floor(s).astype(np.int64)
+    w = f32(1.0) - (s - ix.astype(f32))
+    u = f32(1.0) - w
+    i0 = np.mod(ix, nc)
+    i1 = np.mod(ix + 1, nc)
+    # corner order of coarse_grid.c:113-120: (x, y, z) from {0: left, 1: right}
+    corners = ((0, 0, 0), (0, 1, 0), (0, 0, 1), (0, 1, 1),
+               (1, 0, 0), (1, 1, 0), (1, 0, 1), (1, 1, 1))
+    idx = np.empty((n, 8), dtype=np.int64)
+    val = np.empty((n, 8), dtype=f32)
+    for c, (a, b, d) in enumerate(corners):
+        ia = i1[:, 0] if a else i0[:, 0]
+        ib = i1[:, 1] if b else i0[:, 1]
+        id_ = i1[:, 2] if d else i0[:, 2]
+        wa = u[:, 0] if a else w[:, 0]
+        wb = u[:, 1] if b else w[:, 1]
+        wd = u[:, 2] if d else w[:, 2]
+        idx[:, c] = (ia * nc + ib) * nc + id_
+        val[:, c] = (wa * wb) * wd
+    grid = np.zeros(ng, dtype=f32)
+    np.add.at(grid, idx.ravel(), val.ravel())       # sequential, in order
+    total = float(np.sum(grid, dtype=f64))
+    nbar_inv = f32(float(ng) / float(n if np_total is None else np_total))
+    delta = nbar_inv * grid - f32(1.0)
+    return delta.reshape(nc, nc, nc), total

@@ -10,6 +10,10 @@ Writes
   ref_nc16.npz      nc=16, 48^3 mesh, L=100 Mpc/h, seed 100, Omega_m=0.273,
                     reference schedule (10 steps): 2LPT particles, the
                     forces of the first step, and the z=0 snapshot
+  ref_coarse_grid.npz  the reference's coarse_grid2 file contents (nc = 16)
+                    of that z=0 snapshot
+
+    python tests/golden/make_golden.py coarse    # only ref_coarse_grid.npz
 """
 import os
 import sys
@@ -62,7 +66,28 @@ def main():
                         x0=ics["x"], dx1=ics["dx1"], dx2=ics["dx2"], id=ics["id"],
                         f0=forces[0], snap_x=s["x"], snap_v=s["v"], snap_id=s["id"],
                         meta=np.array([nc, factor, L, seed, OM, sched.a_init]))
+    coarse_grid()
+
+
+def coarse_grid():
+    import tempfile
+    g = np.load(os.path.join(HERE, "ref_nc16.npz"))
+    L = float(g["meta"][2])
+    snap = np.zeros(len(g["snap_x"]), dtype=R_pmin_dtype())
+    snap["x"], snap["v"], snap["id"] = g["snap_x"], g["snap_v"], g["snap_id"]
+    with tempfile.TemporaryDirectory() as d:
+        Lf, delta = R.coarse_grid_file(snap, L, 16, os.path.join(d, "grid.bin"))
+    np.savez_compressed(os.path.join(HERE, "ref_coarse_grid.npz"), delta=delta,
+                        meta=np.array([16, Lf, len(snap)]))
+
+
+def R_pmin_dtype():
+    from cola_halo_b200.types import PARTICLE_MIN_DTYPE
+    return PARTICLE_MIN_DTYPE
 
 
 if __name__ == "__main__":
-    main()
+    if sys.argv[1:] == ["coarse"]:
+        coarse_grid()
+    else:
+        main()
