@@ -46,7 +46,9 @@ def test_coarse_grid_matches_restatement_uniform(gpu_lib, nc):
     delta, total = coarse_grid(pmin_of(x), L, nc)
     want, want_total = R.coarse_grid(x, L, nc)
     assert_grid_close(delta, want)
-    assert abs(total - want_total) < 1e-6 * len(x)
+    # the mass sums of float cells; at nc = 1 one cell holds all 1.6e6
+    # weights, whose float sum depends on the order at the 1e-6 level
+    assert abs(total - want_total) <= 1e-5 * len(x)
 
 
 def test_coarse_grid_faces_and_np_total(gpu_lib):
