@@ -592,10 +592,16 @@ def run_fof(args):
         run = {"particles": len(snap), "boxsize": L, "ll": ll, "halos": int(len(halos)),
                "largest": int(halos["nfof"].max()) if len(halos) else 0,
                "wall_s": wall_s, "particles_per_s": len(snap) / wall_s}
+        run["coarse_grid"] = _time_coarse_grid(cuda, d, snap, L, args)
         if name == "c3" and not args.no_cpu_baseline:
             try:
                 from oracle import ref
                 if os.path.exists(ref.LIB_PATH):
+                    for cg in run["coarse_grid"]:
+                        t0 = time.perf_counter()
+                        ref.coarse_grid_file(snap, L, cg["nc"], os.path.join(tempfile.mkdtemp(),
+                                                                             "grid.bin"))
+                        cg["cpu_reference_s"] = time.perf_counter() - t0
                     t0 = time.perf_counter()
                     rows = ref.fof_catalog(snap, L, nc, np.float32(ll), tempfile.mkdtemp())
                     cpu_s = time.perf_counter() - t0
@@ -613,6 +619,28 @@ def run_fof(args):
                                  "(value) and the 128^3 / L = 300 one"}
     print(json.dumps(out))
     return 0
+
+
+def _time_coarse_grid(cuda, d, snap, L, args, grids=(16, 64, 256)):
+    """One synchronous cg_coarse_grid call on the device-resident snapshot
+    per grid size (nc = 16 is the reference's default coarse_grid_nc): its
+    grid allocation, the CIC pass, delta and the download of the grid
+    included; median over the timed calls."""
+    from cola_halo_b200.coarse import coarse_grid
+    out = []
+    for nc in grids:
+        for _ in range(max(args.warmup, 1)):
+            coarse_grid(d.value, L, nc, np_count=len(snap))
+        times = []
+        for _ in range(args.steps):
+            cuda.sync_device()
+            t0 = time.perf_counter()
+            _, total = coarse_grid(d.value, L, nc, np_count=len(snap))
+            times.append(time.perf_counter() - t0)
+        wall_s = float(np.median(times))
+        out.append({"nc": nc, "wall_s": wall_s, "particles_per_s": len(snap) / wall_s,
+                    "mass_sum": total})
+    return out
 
 
 def run_batch(args):

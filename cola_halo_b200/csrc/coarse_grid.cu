@@ -31,35 +31,76 @@ int grid_for(long long n) {
   return (int)b;
 }
 
+// The eight cells and CIC weights of one particle, in the reference's
+// corner order and arithmetic (coarse_grid.c:101-120).
+__device__ __forceinline__ void cic_corners(const ParticleMinimum& q, float dx_inv, int nc,
+                                            int idx[8], float val[8]) {
+  int i0[3], i1[3];
+  float w[3];
+#pragma unroll
+  for (int j = 0; j < 3; j++) {
+    const float s = __fmul_rn(q.x[j], dx_inv);
+    const int ix = (int)floorf(s);
+    w[j] = __fsub_rn(1.0f, __fsub_rn(s, (float)ix));
+    // (ix + nc) % nc and (ix + 1 + nc) % nc for ix >= -nc, as the
+    // reference; any other ix (a particle far outside the box, NaN)
+    // still lands in the grid
+    int m = ix % nc;
+    if (m < 0) m += nc;
+    i0[j] = m;
+    i1[j] = m + 1 == nc ? 0 : m + 1;
+  }
+  const float u0 = __fsub_rn(1.0f, w[0]), u1 = __fsub_rn(1.0f, w[1]), u2 = __fsub_rn(1.0f, w[2]);
+  const int a0 = i0[0] * nc, a1 = i1[0] * nc;
+  idx[0] = (a0 + i0[1]) * nc + i0[2];  val[0] = __fmul_rn(__fmul_rn(w[0], w[1]), w[2]);
+  idx[1] = (a0 + i1[1]) * nc + i0[2];  val[1] = __fmul_rn(__fmul_rn(w[0], u1), w[2]);
+  idx[2] = (a0 + i0[1]) * nc + i1[2];  val[2] = __fmul_rn(__fmul_rn(w[0], w[1]), u2);
+  idx[3] = (a0 + i1[1]) * nc + i1[2];  val[3] = __fmul_rn(__fmul_rn(w[0], u1), u2);
+  idx[4] = (a1 + i0[1]) * nc + i0[2];  val[4] = __fmul_rn(__fmul_rn(u0, w[1]), w[2]);
+  idx[5] = (a1 + i1[1]) * nc + i0[2];  val[5] = __fmul_rn(__fmul_rn(u0, u1), w[2]);
+  idx[6] = (a1 + i0[1]) * nc + i1[2];  val[6] = __fmul_rn(__fmul_rn(u0, w[1]), u2);
+  idx[7] = (a1 + i1[1]) * nc + i1[2];  val[7] = __fmul_rn(__fmul_rn(u0, u1), u2);
+}
+
+// Grids up to kSmemCells cells: each CTA accumulates its particles into a
+// private copy of the grid in shared memory, then adds the copy to the
+// global grid, so the global atomics are one per cell per CTA instead of
+// eight per particle on a few thousand addresses.
+constexpr int kSmemThreads = 512;
+constexpr int kSmemCells = 16384;
+
+__global__ void __launch_bounds__(kSmemThreads) k_coarse_cic_smem(
+    const ParticleMinimum* __restrict__ p, long long n, float dx_inv, int nc,
+    float* __restrict__ grid) {
+  extern __shared__ float sg[];
+  const int ng = nc * nc * nc;
+  for (int i = threadIdx.x; i < ng; i += kSmemThreads) sg[i] = 0.0f;
+  __syncthreads();
+  for (long long i = (long long)blockIdx.x * kSmemThreads + threadIdx.x; i < n;
+       i += (long long)gridDim.x * kSmemThreads) {
+    int idx[8];
+    float val[8];
+    cic_corners(p[i], dx_inv, nc, idx, val);
+#pragma unroll
+    for (int c = 0; c < 8; c++) atomicAdd(&sg[idx[c]], val[c]);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < ng; i += kSmemThreads) {
+    const float v = sg[i];
+    if (v != 0.0f) atomicAdd(grid + i, v);
+  }
+}
+
+// Larger grids: eight global atomics per particle, spread over many cells.
 __global__ void k_coarse_cic(const ParticleMinimum* __restrict__ p, long long n, float dx_inv,
                              int nc, float* __restrict__ grid) {
   for (long long i = (long long)blockIdx.x * T + threadIdx.x; i < n;
        i += (long long)gridDim.x * T) {
-    int i0[3], i1[3];
-    float w[3];
+    int idx[8];
+    float val[8];
+    cic_corners(p[i], dx_inv, nc, idx, val);
 #pragma unroll
-    for (int j = 0; j < 3; j++) {
-      const float s = __fmul_rn(p[i].x[j], dx_inv);
-      const int ix = (int)floorf(s);
-      w[j] = __fsub_rn(1.0f, __fsub_rn(s, (float)ix));
-      // (ix + nc) % nc and (ix + 1 + nc) % nc for ix >= -nc, as the
-      // reference; any other ix (a particle far outside the box, NaN)
-      // still lands in the grid
-      int m = ix % nc;
-      if (m < 0) m += nc;
-      i0[j] = m;
-      i1[j] = m + 1 == nc ? 0 : m + 1;
-    }
-    const float u0 = __fsub_rn(1.0f, w[0]), u1 = __fsub_rn(1.0f, w[1]), u2 = __fsub_rn(1.0f, w[2]);
-    auto at = [&](int a, int b, int c) { return grid + ((size_t)a * nc + b) * nc + c; };
-    atomicAdd(at(i0[0], i0[1], i0[2]), __fmul_rn(__fmul_rn(w[0], w[1]), w[2]));
-    atomicAdd(at(i0[0], i1[1], i0[2]), __fmul_rn(__fmul_rn(w[0], u1), w[2]));
-    atomicAdd(at(i0[0], i0[1], i1[2]), __fmul_rn(__fmul_rn(w[0], w[1]), u2));
-    atomicAdd(at(i0[0], i1[1], i1[2]), __fmul_rn(__fmul_rn(w[0], u1), u2));
-    atomicAdd(at(i1[0], i0[1], i0[2]), __fmul_rn(__fmul_rn(u0, w[1]), w[2]));
-    atomicAdd(at(i1[0], i1[1], i0[2]), __fmul_rn(__fmul_rn(u0, u1), w[2]));
-    atomicAdd(at(i1[0], i0[1], i1[2]), __fmul_rn(__fmul_rn(u0, w[1]), u2));
-    atomicAdd(at(i1[0], i1[1], i1[2]), __fmul_rn(__fmul_rn(u0, u1), u2));
+    for (int c = 0; c < 8; c++) atomicAdd(grid + idx[c], val[c]);
   }
 }
 
@@ -82,7 +123,7 @@ __global__ void k_coarse_delta(float* __restrict__ grid, long long n, float nbar
 
 extern "C" int cg_coarse_grid(const void* pmin, long long np, long long np_total, float boxsize,
                               int nc, float* delta, double* mass_sum) {
-  if ((np > 0 && !pmin) || np < 0 || np_total <= 0 || !(boxsize > 0.0f) || nc < 1 || nc > 2048 ||
+  if ((np > 0 && !pmin) || np < 0 || np_total <= 0 || !(boxsize > 0.0f) || nc < 1 || nc > 1024 ||
       !delta)
     return cg_set_error_from_lpt(CG_EINVAL, "cg_coarse_grid: bad arguments");
   const long long ng = (long long)nc * nc * nc;
@@ -109,7 +150,21 @@ extern "C" int cg_coarse_grid(const void* pmin, long long np, long long np_total
   if (e == cudaSuccess) {
     const float dx_inv = (float)nc / boxsize;                       // coarse_grid.c:100
     const float nbar_inv = (float)((double)ng / (double)np_total);  // coarse_grid.c:60
-    if (np > 0) {
+    if (np > 0 && ng <= kSmemCells) {
+      const int smem = (int)(sizeof(float) * ng);
+      int per_sm = 0, sms = 0, dev = 0;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+      cudaFuncSetAttribute(k_coarse_cic_smem, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)(sizeof(float) * kSmemCells));
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_coarse_cic_smem, kSmemThreads,
+                                                    smem);
+      long long blocks = (np + kSmemThreads - 1) / kSmemThreads;
+      const long long cap = (long long)(per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1);
+      if (blocks > cap) blocks = cap;
+      prof_mark(st, CG_ST_OTHER);
+      k_coarse_cic_smem<<<(int)blocks, kSmemThreads, smem, st>>>(d_p, np, dx_inv, nc, d_grid);
+    } else if (np > 0) {
       prof_mark(st, CG_ST_OTHER);
       k_coarse_cic<<<grid_for(np), T, 0, st>>>(d_p, np, dx_inv, nc, d_grid);
     }

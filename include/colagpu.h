@@ -231,7 +231,9 @@ int cg_fof(const void* pmin, long long np, float boxsize, float ll, int nfof_min
  * periodic box, then delta = nc^3 / np_total * rho - 1, all in float with
  * the reference's weight arithmetic.  delta_out (nc^3 floats, host or
  * device) receives the contrast; *mass_sum (may be NULL) the sum of rho in
- * double.  Synchronous; allocates and frees its own device grid. */
+ * double.  1 <= nc <= 1024.  Grids of up to 16384 cells are accumulated
+ * per CTA in shared memory first.  Synchronous; allocates and frees its own
+ * device grid. */
 int cg_coarse_grid(const void* pmin, long long np, long long np_total, float boxsize, int nc,
                    float* delta_out, double* mass_sum);
 

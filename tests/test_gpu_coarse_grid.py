@@ -38,7 +38,7 @@ def test_coarse_grid_matches_golden_fixture(gpu_lib):
     assert abs(total - n) < 1e-3 * n
 
 
-@pytest.mark.parametrize("nc", [1, 7, 16, 64, 128])
+@pytest.mark.parametrize("nc", [7, 16, 25, 26, 64, 128])
 def test_coarse_grid_matches_restatement_uniform(gpu_lib, nc):
     from cola_halo_b200.coarse import coarse_grid
     L = 250.0
@@ -46,9 +46,29 @@ def test_coarse_grid_matches_restatement_uniform(gpu_lib, nc):
     delta, total = coarse_grid(pmin_of(x), L, nc)
     want, want_total = R.coarse_grid(x, L, nc)
     assert_grid_close(delta, want)
-    # the mass sums of float cells; at nc = 1 one cell holds all 1.6e6
-    # weights, whose float sum depends on the order at the 1e-6 level
     assert abs(total - want_total) <= 1e-5 * len(x)
+
+
+def test_coarse_grid_single_cell(gpu_lib):
+    """nc = 1: one cell holds all 8 n weights.  The reference's running
+    float sum of 1.6e6 terms drifts by ~8e-4 (199846 instead of 200000);
+    the GPU sums per CTA first, so it is checked against the float64 sum of
+    the same float weights instead."""
+    from cola_halo_b200.coarse import coarse_grid
+    L = 250.0
+    x = np.random.default_rng(1).uniform(0, L, (200000, 3)).astype(np.float32)
+    delta, total = coarse_grid(pmin_of(x), L, 1)
+    s = x * (np.float32(1) / np.float32(L))
+    w = np.float32(1) - (s - np.floor(s))
+    u = np.float32(1) - w
+    exact = 0.0
+    for a in (w, u):
+        for b in (w, u):
+            for c in (w, u):
+                exact += float(np.sum((a[:, 0] * b[:, 1]) * c[:, 2], dtype=np.float64))
+    assert abs(total - exact) <= 1e-5 * exact
+    want = np.float32(1.0 / len(x)) * np.float32(exact) - np.float32(1)
+    assert abs(float(delta[0, 0, 0]) - float(want)) <= 1e-5
 
 
 def test_coarse_grid_faces_and_np_total(gpu_lib):
