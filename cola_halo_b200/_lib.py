@@ -73,6 +73,9 @@ SIGNATURES = {
     "cg_batch_last_ms": (i32, [P, fptr]),
     "cg_fof": (i32, [P, i64, f32, f32, i32, P, i64, ctypes.POINTER(i64)]),
     "cg_coarse_grid": (i32, [P, i64, i64, f32, i32, P, ctypes.POINTER(f64)]),
+    "cg_write_gadget": (i32, [ctypes.c_char_p, P, i64, i64, i32, f32, f32, f32, f32, i32]),
+    "cg_sim_write_gadget": (i32, [P, f64, f32, f32, ctypes.c_char_p, i32]),
+    "cg_snapshot_invalidate": (None, []),
     "cg_autotune": (i32, [i32, i32, P, P]),
     "cg_schedule_variants": (i32, [i32, ctypes.POINTER(i32), ctypes.POINTER(i32)]),
     "cg_get_schedule": (i32, [i32, ctypes.POINTER(i32), ctypes.POINTER(i32)]),
@@ -107,6 +110,7 @@ SIGNATURES = {
     "fof_find_halos": (None, [P, f32]),
     "fof_write_halos": (None, [ctypes.c_char_p]),
     "coarse_grid2": (None, [ctypes.c_char_p, P, i32, P, sz]),
+    "write_snapshot": (None, [ctypes.c_char_p, P, i32]),
     "cg_particles_upload": (i32, [P]),
     "cg_particles_download": (i32, [P]),
     "cg_dropin_set_sync": (None, [i32]),

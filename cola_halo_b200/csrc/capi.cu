@@ -17,6 +17,7 @@
 #include "internal.h"
 #include "lpt.h"
 #include "convnet.h"
+#include "gadget.h"
 
 #include <vector>
 
@@ -85,6 +86,7 @@ struct cg_sim {
   float a_x = 0, a_v = 0;
   cudaStream_t st = nullptr;
   void* d_aos = nullptr;      // staging: Particle (56 B) / ParticleMinimum (32 B) arrays
+  bool aos_snapshot = false;  // d_aos holds the last snapshot (ParticleMinimum[n])
   float* soa_block = nullptr; // one allocation for all SoA float arrays
 };
 
@@ -162,6 +164,7 @@ extern "C" int cg_sim_set_particles(cg_sim* s, const void* particles, long long 
   s->ps.n = np;
   s->a_x = a_x;
   s->a_v = a_v;
+  s->aos_snapshot = false;
   if (np == 0) return CG_OK;
   const cudaMemcpyKind kind =
       is_device_ptr(particles) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
@@ -173,6 +176,7 @@ extern "C" int cg_sim_set_particles(cg_sim* s, const void* particles, long long 
 extern "C" int cg_sim_get_particles(cg_sim* s, void* particles) {
   if (!s || !particles) return set_err(CG_EINVAL, "cg_sim_get_particles: NULL");
   if (s->ps.n == 0) return CG_OK;
+  s->aos_snapshot = false;
   CG_CHECK(particles_soa_to_aos(s->d_aos, &s->ps, s->st), "soa_to_aos");
   CG_CHECK(cudaMemcpyAsync(particles, s->d_aos, 56 * (size_t)s->ps.n, cudaMemcpyDefault, s->st),
            "download particles");
@@ -322,10 +326,21 @@ extern "C" int cg_sim_snapshot(cg_sim* s, double aout, float omega_m, void* pmin
   if (!s || !pmin_out) return set_err(CG_EINVAL, "cg_sim_snapshot: NULL");
   int rc = queue_snapshot(s, aout, omega_m, s->d_aos);
   if (rc) return rc;
+  s->aos_snapshot = true;
   CG_CHECK(cudaMemcpyAsync(pmin_out, s->d_aos, 32 * (size_t)s->ps.n, cudaMemcpyDefault, s->st),
            "download snapshot");
   CG_CHECK(cudaStreamSynchronize(s->st), "sync");
   return CG_OK;
+}
+
+extern "C" int cg_sim_write_gadget(cg_sim* s, double aout, float omega_m, float h,
+                                   const char* filename, int use_long_id) {
+  if (!s || !filename) return set_err(CG_EINVAL, "cg_sim_write_gadget: NULL");
+  int rc = queue_snapshot(s, aout, omega_m, s->d_aos);
+  if (rc) return rc;
+  s->aos_snapshot = true;
+  return gadget_write(filename, s->d_aos, true, s->ps.n, s->ps.n, 1, (float)aout, s->L, omega_m,
+                      h, use_long_id, s->st);
 }
 
 extern "C" int cg_sim_sync(cg_sim* s) {
@@ -634,6 +649,8 @@ struct DropIn {
   int bound_np = -1;
   bool full_sync = false;
   bool abort_on_error = true;
+  const ParticleMinimum* snap_p = nullptr;   // host array of the last cola_set_snapshot
+  int snap_np = -1;
   int lpt_nc = 0;
   PowerTable power;
   bool power_ready = false;
@@ -722,7 +739,14 @@ extern "C" void cg_dropin_finalize(void) {
   g_drop.bound_p = nullptr;
   g_drop.bound_np = -1;
   g_drop.nc_pm = 0;
+  g_drop.snap_p = nullptr;
+  g_drop.snap_np = -1;
   lpt_dropin_release();
+}
+
+extern "C" void cg_snapshot_invalidate(void) {
+  g_drop.snap_p = nullptr;
+  g_drop.snap_np = -1;
 }
 
 extern "C" int cg_particles_upload(Particles* p) {
@@ -832,6 +856,19 @@ extern "C" void cola_set_snapshot(const double aout, Particles const* const part
   snapshot->np_local = particles->np_local;          // cola.c:412-414
   snapshot->np_average = particles->np_average;
   snapshot->a = (float)aout;
+  g_drop.snap_p = g_drop.full_sync ? nullptr : snapshot->p;
+  g_drop.snap_np = snapshot->np_local;
+}
+
+// The device copy of `snapshot` left by the last cola_set_snapshot (the
+// drop-in sim's ParticleMinimum staging array), while it still matches:
+// same host array and count, not overwritten since, no full-sync mode.
+ParticleMinimum* dropin_device_snapshot(const Snapshot* snapshot, cudaStream_t* st) {
+  if (!snapshot || !g_drop.sim || g_drop.full_sync || !g_drop.sim->aos_snapshot ||
+      g_drop.snap_p != snapshot->p || g_drop.snap_np != snapshot->np_local)
+    return nullptr;
+  if (st) *st = g_drop.sim->st;
+  return (ParticleMinimum*)g_drop.sim->d_aos;
 }
 
 // ---------------------------------------------------------- power.c

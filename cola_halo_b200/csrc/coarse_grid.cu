@@ -14,6 +14,7 @@
 
 #include "../../include/colagpu.h"
 #include "../../include/colagpu_dropin.h"
+#include "gadget.h"
 #include "internal.h"
 
 extern int cg_set_error_from_lpt(int code, const char* msg);
@@ -204,8 +205,12 @@ extern "C" void coarse_grid2(const char filename[], Snapshot const* const snapsh
     return;
   }
   double sum = 0.0;
-  if (cg_coarse_grid(snapshot->p, snapshot->np_local, snapshot->np_total, snapshot->boxsize, nc,
-                     delta, &sum) != CG_OK) {
+  // the device copy cola_set_snapshot left, when it still matches
+  cudaStream_t st = 0;
+  const ParticleMinimum* d = dropin_device_snapshot(snapshot, &st);
+  if (d) cudaStreamSynchronize(st);
+  if (cg_coarse_grid(d ? (const void*)d : (const void*)snapshot->p, snapshot->np_local,
+                     snapshot->np_total, snapshot->boxsize, nc, delta, &sum) != CG_OK) {
     free(delta);
     cg_dropin_error(10010, "coarse_grid2: coarse grid failed");
     return;

@@ -28,6 +28,7 @@
 
 #include "../../include/colagpu.h"
 #include "../../include/colagpu_dropin.h"
+#include "gadget.h"
 #include "internal.h"
 
 extern int cg_set_error_from_lpt(int code, const char* msg);
@@ -440,6 +441,88 @@ void cg_dropin_error(int code, const char* msg);
 namespace {
 cg_halo* g_halos = nullptr;
 long long g_nhalo = 0;
+
+// move_particles2_min's wrap of a snapshot (move.c:33-41, float add or
+// subtract of L once per axis), in place on the device.  Particles it moves
+// are listed -- index and new position, up to `cap` -- so that the host copy
+// can be patched without downloading the whole snapshot.
+__global__ void k_wrap_list(ParticleMinimum* __restrict__ p, long long n, float L,
+                            unsigned long long* __restrict__ count, long long cap,
+                            long long* __restrict__ idx, float* __restrict__ xs) {
+  for (long long i = (long long)blockIdx.x * CG_THREADS + threadIdx.x; i < n;
+       i += (long long)gridDim.x * CG_THREADS) {
+    float x[3];
+    bool moved = false;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      x[k] = p[i].x[k];
+      if (x[k] < 0.0f) {
+        x[k] = __fadd_rn(x[k], L);
+        moved = true;
+      } else if (x[k] >= L) {
+        x[k] = __fsub_rn(x[k], L);
+        moved = true;
+      }
+    }
+    if (!moved) continue;
+#pragma unroll
+    for (int k = 0; k < 3; k++) p[i].x[k] = x[k];
+    const unsigned long long slot = atomicAdd(count, 1ULL);
+    if ((long long)slot < cap) {
+      idx[slot] = i;
+#pragma unroll
+      for (int k = 0; k < 3; k++) xs[3 * slot + k] = x[k];
+    }
+  }
+}
+
+// Wrap the device snapshot d (n particles, after the work on st) and bring
+// the host copy h to the same positions.
+cudaError_t wrap_device_and_host(ParticleMinimum* d, ParticleMinimum* h, long long n, float L,
+                                 cudaStream_t st) {
+  if (n == 0) return cudaSuccess;
+  const long long cap = n < (1LL << 20) ? n : (1LL << 20);
+  unsigned long long* d_count = nullptr;
+  long long* d_idx = nullptr;
+  float* d_x = nullptr;
+  cudaError_t e = cudaMalloc(&d_count, sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaMalloc(&d_idx, sizeof(long long) * cap);
+  if (e == cudaSuccess) e = cudaMalloc(&d_x, sizeof(float) * 3 * cap);
+  if (e == cudaSuccess) e = cudaMemsetAsync(d_count, 0, sizeof(unsigned long long), st);
+  if (e == cudaSuccess) {
+    long long blocks = (n + CG_THREADS - 1) / CG_THREADS;
+    if (blocks > 148LL * 16) blocks = 148LL * 16;
+    prof_mark(st, CG_ST_WRAP);
+    k_wrap_list<<<(int)blocks, CG_THREADS, 0, st>>>(d, n, L, d_count, cap, d_idx, d_x);
+    e = cudaGetLastError();
+  }
+  unsigned long long moved = 0;
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(&moved, d_count, sizeof(moved), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e == cudaSuccess && moved > 0) {
+    if ((long long)moved <= cap) {
+      long long* idx = (long long*)malloc(sizeof(long long) * moved);
+      float* xs = (float*)malloc(sizeof(float) * 3 * moved);
+      if (!idx || !xs) e = cudaErrorMemoryAllocation;
+      if (e == cudaSuccess)
+        e = cudaMemcpy(idx, d_idx, sizeof(long long) * moved, cudaMemcpyDeviceToHost);
+      if (e == cudaSuccess)
+        e = cudaMemcpy(xs, d_x, sizeof(float) * 3 * moved, cudaMemcpyDeviceToHost);
+      if (e == cudaSuccess)
+        for (unsigned long long j = 0; j < moved; j++)
+          memcpy(h[idx[j]].x, xs + 3 * j, sizeof(float) * 3);
+      free(idx);
+      free(xs);
+    } else {
+      e = cudaMemcpy(h, d, sizeof(ParticleMinimum) * n, cudaMemcpyDeviceToHost);
+    }
+  }
+  cudaFree(d_count);
+  cudaFree(d_idx);
+  cudaFree(d_x);
+  return e;
+}
 }  // namespace
 
 extern "C" size_t fof_calc_memory(const int np_alloc, const int nc) {
@@ -456,19 +539,13 @@ extern "C" void fof_init(const int np_alloc, const int nc, void* mem, size_t mem
 }
 
 extern "C" void fof_find_halos(Snapshot* snapshot, const float ll) {
-  if (!snapshot || !(snapshot->boxsize > 0.0f)) {
+  if (!snapshot || !(snapshot->boxsize > 0.0f) || snapshot->np_local < 0 ||
+      (snapshot->np_local > 0 && !snapshot->p)) {
     cg_dropin_error(7000, "fof_find_halos: bad snapshot");
     return;
   }
-  // move_particles2_min (fof.c:1042): one-shot wrap into the box, in place
   const float L = snapshot->boxsize;
   const int n = snapshot->np_local;
-  for (int i = 0; i < n; i++)
-    for (int k = 0; k < 3; k++) {
-      float& x = snapshot->p[i].x[k];
-      if (x < 0.0f) x += L;
-      else if (x >= L) x -= L;
-    }
   const long long cap = n / 32 + 1;   // halos hold at least 32 particles each
   cg_halo* h = (cg_halo*)realloc(g_halos, sizeof(cg_halo) * cap);
   if (!h) {
@@ -476,9 +553,26 @@ extern "C" void fof_find_halos(Snapshot* snapshot, const float ll) {
     return;
   }
   g_halos = h;
+  g_nhalo = 0;
+  // the snapshot on the device: the copy cola_set_snapshot left, or an upload
+  cudaStream_t st = 0;
+  ParticleMinimum* d = dropin_device_snapshot(snapshot, &st);
+  ParticleMinimum* own = nullptr;
+  cudaError_t e = cudaSuccess;
+  if (!d && n > 0) {
+    e = cudaMalloc(&own, sizeof(ParticleMinimum) * n);
+    if (e == cudaSuccess)
+      e = cudaMemcpy(own, snapshot->p, sizeof(ParticleMinimum) * n, cudaMemcpyHostToDevice);
+    d = own;
+    st = 0;
+  }
+  // move_particles2_min (fof.c:1042): one-shot wrap into the box, in place,
+  // on both copies
+  if (e == cudaSuccess) e = wrap_device_and_host(d, snapshot->p, n, L, st);
   long long nh = 0;
-  if (cg_fof(snapshot->p, n, L, ll, 32, g_halos, cap, &nh) != CG_OK) {
-    g_nhalo = 0;
+  const int rc = e == cudaSuccess ? cg_fof(d, n, L, ll, 32, g_halos, cap, &nh) : CG_ECUDA;
+  cudaFree(own);
+  if (rc != CG_OK) {
     cg_dropin_error(7050, "fof_find_halos failed");
     return;
   }

@@ -128,6 +128,13 @@ class Simulation:
         _lib.check(self.lib.cg_sim_snapshot(self.h, aout, om, out.ctypes.data), "cg_sim_snapshot")
         return out
 
+    def write_gadget(self, filename, aout, h=0.7, use_long_id=False, omega_m=None):
+        """The snapshot at aout written as a GADGET-1 file straight from the
+        device (cg_sim_write_gadget)."""
+        om = self.omega_m if omega_m is None else omega_m
+        _lib.check(self.lib.cg_sim_write_gadget(self.h, aout, om, h, str(filename).encode(),
+                                                int(bool(use_long_id))), "cg_sim_write_gadget")
+
     def sync(self):
         _lib.check(self.lib.cg_sim_sync(self.h), "cg_sim_sync")
 

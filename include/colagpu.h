@@ -39,7 +39,7 @@ extern "C" {
 #define CG_EDENSITY (-4)    /* CIC density sum check failed (pm.c:548-553) */
 #define CG_EPARTICLE (-5)   /* a particle position was non-finite or below 0 */
 #define CG_EUNSUPPORTED (-6)/* mesh size not built into this library */
-#define CG_EFILE (-7)       /* input file unreadable */
+#define CG_EFILE (-7)       /* file unreadable or unwritable */
 
 typedef struct cg_sim cg_sim;
 
@@ -236,6 +236,21 @@ int cg_fof(const void* pmin, long long np, float boxsize, float ll, int nfof_min
  * device grid. */
 int cg_coarse_grid(const void* pmin, long long np, long long np_total, float boxsize, int nc,
                    float* delta_out, double* mass_sum);
+
+/* GADGET-1 snapshot file (write.c:14-107, one file): header, positions,
+ * velocities times 1/sqrt(a), ids (4-byte unsigned, or 8-byte with
+ * use_long_id), each record framed by its int byte length.  pmin holds np
+ * ParticleMinimum in host or device memory; the header's particle mass uses
+ * np_total.  Device input is formatted on the GPU chunk by chunk and
+ * downloaded through pinned buffers while the previous chunk is written.
+ * Synchronous.  CG_EFILE when the file cannot be written. */
+int cg_write_gadget(const char* filename, const void* pmin, long long np, long long np_total,
+                    int num_files, float a, float boxsize, float omega_m, float h,
+                    int use_long_id);
+/* The snapshot at aout (as cg_sim_snapshot) written straight from the
+ * device as a GADGET-1 file, with no host copy of the particles. */
+int cg_sim_write_gadget(cg_sim* s, double aout, float omega_m, float h, const char* filename,
+                        int use_long_id);
 
 /* FFT schedule autotuner (no reference counterpart).  From 256 up each
  * mesh size has several compiled variants of the strided x pass (ky columns

@@ -3,12 +3,15 @@
  *
  * Each function has the name, signature and argument meaning of the
  * reference function it replaces (cited below), so the reference's driver
- * (main.c) links against libcolagpu instead of pm.o, cola.o, lpt.o, power.o
- * and move.o.  The data types are the reference's (particle.h:6-48).
+ * (main.c) links against libcolagpu instead of pm.o, cola.o, lpt.o, power.o,
+ * move.o, fof.o, coarse_grid.o and write.o.  The data types are the
+ * reference's (particle.h:6-48).
  *
  * Errors: like the reference (msg_abort -> MPI_Abort, msg.c:36-45) a failure
  * prints a message and exits the process with the reference's error code
- * (4001 mesh allocation, 6040 density check, 3000 power table, 3010 sigma8),
+ * (4001 mesh allocation, 6040 density check, 3000 power table, 3010 sigma8,
+ * 7000/7050 halo finding, 8110 halo file, 10010/10021 coarse grid, 9000
+ * GADGET file),
  * unless cg_dropin_set_abort(0) was called, in which case the call returns
  * and cg_last_error() describes the failure.
  *
@@ -131,8 +134,20 @@ void fof_write_halos(char filename[]);
 void coarse_grid2(const char filename[], Snapshot const* const snapshot, const int nc,
                   void* const mem1, const size_t size1);
 
+/* write.h:7 (write.c:14-107): GADGET-1 file "<filebase>.0" of the
+ * snapshot (one process), the reference's bytes.  Error 9000 when the file
+ * cannot be written. */
+void write_snapshot(const char filebase[], Snapshot const* const snapshot, int use_long_id);
+
 /* Residency and error controls of the drop-in layer (no reference
  * counterpart). */
+/* Snapshot residency: cola_set_snapshot leaves its result on the device as
+ * well as in snapshot->p, and fof_find_halos, coarse_grid2 and
+ * write_snapshot read that device copy while the Snapshot's array and
+ * np_local are unchanged (fof_find_halos wraps both copies).  A caller that
+ * edits snapshot->p in between calls cg_snapshot_invalidate() first; the
+ * next call then reads the host array. */
+void cg_snapshot_invalidate(void);
 int cg_particles_upload(Particles* particles);
 int cg_particles_download(Particles* particles);
 void cg_dropin_set_sync(int full);

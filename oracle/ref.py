@@ -57,6 +57,7 @@ def load():
         "fof_find_halos": (None, [P, f]),
         "fof_write_halos": (None, [ctypes.c_char_p]),
         "coarse_grid2": (None, [ctypes.c_char_p, P, i, P, sz]),
+        "write_snapshot": (None, [ctypes.c_char_p, P, i]),
         "growthD": (f, [f]),
         "growthD2": (f, [f]),
         "Sq": (d, [d, d, d]),
@@ -154,3 +155,19 @@ def coarse_grid_file(pmin, boxsize, nc, path, np_total=None):
     mem = np.zeros(size // 4 + 16, dtype=np.float32)
     lib.coarse_grid2(path.encode(), snap.ptr, nc, mem.ctypes.data, size)
     return read_grid_file(path)
+
+
+def gadget_file(pmin, boxsize, omega_m, h, a, filebase, use_long_id=0):
+    """The bytes of the reference's write_snapshot (write.c:14-107, one rank)
+    for ParticleMinimum array `pmin`: it writes "<filebase>.0"."""
+    from cola_halo_b200.types import HostSnapshot
+    lib = load()
+    n = len(pmin)
+    lib.comm_init(16, 16, boxsize)
+    snap = HostSnapshot(16, max(n, 1), boxsize, omega_m, h=h)
+    snap.p[:n] = pmin
+    snap.struct.np_local = n
+    snap.struct.a = a
+    lib.write_snapshot(filebase.encode(), snap.ptr, int(use_long_id))
+    with open(filebase + ".0", "rb") as f:
+        return f.read()

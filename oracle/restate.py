@@ -760,3 +760,40 @@ def coarse_grid(x, boxsize, nc, np_total=None):
     nbar_inv = f32(float(ng) / float(n if np_total is None else np_total))
     delta = nbar_inv * grid - f32(1.0)
     return delta.reshape(nc, nc, nc), total
+
+
+# --------------------------------------------------------------------------
+# GADGET-1 snapshot file (write.c:14-107 on one rank).
+def gadget_bytes(x, v, ids, a, boxsize, omega_m, h, use_long_id=False, np_total=None,
+                 num_files=1):
+    """The file as bytes: four records, each framed by its int32 byte length
+    -- the 256-byte header (gadget_file.h:4-24), positions, velocities times
+    vfac = (float)(1/sqrt(a)) in float32, ids as uint32 (or uint64 with
+    use_long_id).  Header values are formed in float64 from the float32
+    snapshot fields as write.c:42-64 forms them."""
+    import struct
+    x = np.asarray(x, dtype=f32).reshape(-1, 3)
+    v = np.asarray(v, dtype=f32).reshape(-1, 3)
+    ids = np.asarray(ids, dtype=np.int64)
+    n = len(x)
+    nt = n if np_total is None else int(np_total)
+    L, om, af, hf = (float(f32(boxsize)), float(f32(omega_m)), float(f32(a)), float(f32(h)))
+    with np.errstate(divide="ignore", invalid="ignore"):   # C: n = 0 gives inf
+        mass = float(f64(om * 27.7455 * math.pow(L, 3.0)) / f64(nt))
+    hdr = struct.pack("<6i6d2d2i6I2i4d2i6Ii", 0, n, 0, 0, 0, 0,
+                      0.0, mass, 0.0, 0.0, 0.0, 0.0,
+                      af, 1.0 / af - 1, 0, 0,
+                      0, nt & 0xFFFFFFFF, 0, 0, 0, 0,
+                      0, num_files, L, om, 1.0 - om, hf, 0, 0,
+                      0, (nt >> 32) & 0xFFFFFFFF, 0, 0, 0, 0, 0)
+    hdr += b"\0" * (256 - len(hdr))
+    assert len(hdr) == 256
+    vfac = f32(1.0 / math.sqrt(af))
+    vel = (vfac * v).astype(f32)
+    idarr = ids.astype(np.uint64) if use_long_id else (ids & 0xFFFFFFFF).astype(np.uint32)
+
+    def rec(payload):
+        m = struct.pack("<i", len(payload) & 0xFFFFFFFF if len(payload) < 2 ** 31
+                        else len(payload) - 2 ** 32)
+        return m + payload + m
+    return (rec(hdr) + rec(x.tobytes()) + rec(vel.tobytes()) + rec(idarr.tobytes()))

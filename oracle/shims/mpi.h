@@ -7,7 +7,8 @@
  * to a copy of the send buffer into the receive buffer.  Only the API surface
  * the reference's hot path uses is provided (pm.c:150-159,461-472,494,520-545;
  * move.c:87-168; comm.c:39-177; lpt.c:566; power.c:43-58; msg.c:36-45;
- * fof.c:669,855-889,1094-1121 for the gathers of the halo finder).
+ * fof.c:669,855-889,1094-1121 for the gathers of the halo finder;
+ * write.c:39-40,280-323 for the GADGET writer and the subsample file).
  */
 #ifndef ORACLE_SHIM_MPI_H
 #define ORACLE_SHIM_MPI_H
@@ -64,6 +65,23 @@ int MPI_Gather(const void* sendbuf, int sendcount, MPI_Datatype sendtype,
 int MPI_Gatherv(const void* sendbuf, int sendcount, MPI_Datatype sendtype,
                 void* recvbuf, const int* recvcounts, const int* displs,
                 MPI_Datatype recvtype, int root, MPI_Comm comm);
+
+int MPI_Scatter(const void* sendbuf, int sendcount, MPI_Datatype sendtype,
+                void* recvbuf, int recvcount, MPI_Datatype recvtype, int root,
+                MPI_Comm comm);
+
+/* MPI-IO on one rank: a file handle is a stdio stream. */
+typedef void* MPI_File;
+typedef int MPI_Info;
+typedef long long MPI_Offset;
+#define MPI_INFO_NULL 0
+#define MPI_MODE_CREATE 1
+#define MPI_MODE_WRONLY 4
+int MPI_File_open(MPI_Comm comm, const char* filename, int amode, MPI_Info info,
+                  MPI_File* fh);
+int MPI_File_write_at(MPI_File fh, MPI_Offset offset, const void* buf, int count,
+                      MPI_Datatype datatype, MPI_Status* status);
+int MPI_File_close(MPI_File* fh);
 
 /* Test hook: the exit code of the last MPI_Abort is reported through this
  * callback when one is installed (so a ctypes caller can turn an abort into a

@@ -114,3 +114,39 @@ int MPI_Gatherv(const void* sendbuf, int sendcount, MPI_Datatype sendtype,
   if (n && (const void*)dst != sendbuf) memmove(dst, sendbuf, n);
   return MPI_SUCCESS;
 }
+
+int MPI_Scatter(const void* sendbuf, int sendcount, MPI_Datatype sendtype,
+                void* recvbuf, int recvcount, MPI_Datatype recvtype, int root,
+                MPI_Comm comm)
+{
+  (void)recvcount; (void)recvtype; (void)root; (void)comm;
+  size_t n = (size_t)sendcount * type_size(sendtype);
+  if (n && sendbuf != recvbuf) memmove(recvbuf, sendbuf, n);
+  return MPI_SUCCESS;
+}
+
+int MPI_File_open(MPI_Comm comm, const char* filename, int amode, MPI_Info info,
+                  MPI_File* fh)
+{
+  (void)comm; (void)info;
+  FILE* fp = fopen(filename, (amode & MPI_MODE_CREATE) ? "w" : "r+");
+  *fh = fp;
+  return fp ? MPI_SUCCESS : 1;
+}
+
+int MPI_File_write_at(MPI_File fh, MPI_Offset offset, const void* buf, int count,
+                      MPI_Datatype datatype, MPI_Status* status)
+{
+  (void)status;
+  FILE* fp = (FILE*)fh;
+  size_t n = (size_t)count * type_size(datatype);
+  if (fseeko(fp, (off_t)offset, SEEK_SET) != 0) return 1;
+  return fwrite(buf, 1, n, fp) == n ? MPI_SUCCESS : 1;
+}
+
+int MPI_File_close(MPI_File* fh)
+{
+  int rc = fclose((FILE*)*fh);
+  *fh = 0;
+  return rc == 0 ? MPI_SUCCESS : 1;
+}
