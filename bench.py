@@ -23,6 +23,7 @@ import os
 import statistics
 import subprocess
 import sys
+import shutil
 import tempfile
 import threading
 import time
@@ -593,6 +594,7 @@ def run_fof(args):
                "largest": int(halos["nfof"].max()) if len(halos) else 0,
                "wall_s": wall_s, "particles_per_s": len(snap) / wall_s}
         run["coarse_grid"] = _time_coarse_grid(cuda, d, snap, L, args)
+        run["gadget"] = _time_gadget(cuda, d, snap, L, args)
         if name == "c3" and not args.no_cpu_baseline:
             try:
                 from oracle import ref
@@ -602,6 +604,11 @@ def run_fof(args):
                         ref.coarse_grid_file(snap, L, cg["nc"], os.path.join(tempfile.mkdtemp(),
                                                                              "grid.bin"))
                         cg["cpu_reference_s"] = time.perf_counter() - t0
+                    gdir = tempfile.mkdtemp()
+                    t0 = time.perf_counter()
+                    ref.gadget_file(snap, L, 0.273, 0.705, 1.0, os.path.join(gdir, "snp"), 0)
+                    run["gadget"]["cpu_reference_s"] = time.perf_counter() - t0
+                    shutil.rmtree(gdir, ignore_errors=True)
                     t0 = time.perf_counter()
                     rows = ref.fof_catalog(snap, L, nc, np.float32(ll), tempfile.mkdtemp())
                     cpu_s = time.perf_counter() - t0
@@ -641,6 +648,30 @@ def _time_coarse_grid(cuda, d, snap, L, args, grids=(16, 64, 256)):
         out.append({"nc": nc, "wall_s": wall_s, "particles_per_s": len(snap) / wall_s,
                     "mass_sum": total})
     return out
+
+
+def _time_gadget(cuda, d, snap, L, args):
+    """One synchronous cg_write_gadget call (4-byte ids) of the
+    device-resident snapshot to a file in a fresh temporary directory:
+    formatting, download and the writes into the page cache, median over the
+    timed calls (the file is deleted between calls)."""
+    from cola_halo_b200.gadget import write_gadget
+    tmp = tempfile.mkdtemp()
+    path = os.path.join(tmp, "snp.0")
+    times = []
+    for k in range(max(args.warmup, 1) + args.steps):
+        if os.path.exists(path):
+            os.remove(path)
+        cuda.sync_device()
+        t0 = time.perf_counter()
+        write_gadget(path, d.value, 1.0, L, 0.273, 0.705, np_count=len(snap))
+        if k >= max(args.warmup, 1):
+            times.append(time.perf_counter() - t0)
+    size = os.path.getsize(path)
+    shutil.rmtree(tmp, ignore_errors=True)
+    wall_s = float(np.median(times))
+    return {"bytes": size, "wall_s": wall_s, "GB_per_s": size / wall_s / 1e9,
+            "dir": os.path.dirname(tmp)}
 
 
 def run_batch(args):
