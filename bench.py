@@ -519,6 +519,8 @@ def main():
     ap.add_argument("--train-seeds", type=int, default=16)
     ap.add_argument("--eval-seeds", type=int, default=8)
     ap.add_argument("--epochs", type=int, default=3)
+    ap.add_argument("--cufft", action="store_true",
+                    help="the mesh r2c / c2r transforms beside cuFFT's at 384^3 and 768^3")
     ap.add_argument("--fof", action="store_true",
                     help="friends-of-friends halo finding on the z = 0 snapshot (b = 0.2)")
     ap.add_argument("--batch", action="store_true",
@@ -533,6 +535,8 @@ def main():
         return run_batch(args)
     if args.fof:
         return run_fof(args)
+    if args.cufft:
+        return run_cufft(args)
     cfg = CONFIGS[args.config]
     args.config_desc = "%d^3 particles, %d^3 mesh, L=%g Mpc/h, BBKS, 2LPT z=49, 10 steps" % (
         cfg["nc"], cfg["nc"] * cfg["factor"], cfg["L"])
@@ -672,6 +676,51 @@ def _time_gadget(cuda, d, snap, L, args):
     wall_s = float(np.median(times))
     return {"bytes": size, "wall_s": wall_s, "GB_per_s": size / wall_s / 1e9,
             "dir": os.path.dirname(tmp)}
+
+
+def run_cufft(args):
+    """Device time of one 3-D r2c and one c2r of an N^3 float mesh held in
+    HBM: this library's transforms (cg_fft_time: z, x, y passes, layout
+    [kz][kx][ky]) beside cuFFT's (torch.fft.rfftn / irfftn, layout
+    [x][y][kz]), each the mean of the timed launches after a warm-up."""
+    rank, world, local = dist_setup(args)
+    if rank != 0:
+        return 0
+    import torch
+    from cola_halo_b200 import _lib
+    lib = _lib.load()
+    _lib.check(lib.cg_set_device(local), "cg_set_device")
+    reps = max(args.steps, 1)
+    out = {"metric": "3-D real FFT device time", "unit": "ms", "higher_is_better": False,
+           "n_gpus": 1, "dtype": "f32", "runs": {},
+           "library": "cuFFT (torch %s) through torch.fft.rfftn / irfftn" % torch.__version__}
+    for n in (384, 768):
+        r2c, c2r = ctypes.c_float(), ctypes.c_float()
+        _lib.check(lib.cg_fft_time(n, reps, ctypes.byref(r2c), ctypes.byref(c2r)), "cg_fft_time")
+        x = torch.zeros((n, n, n), device="cuda:%d" % local, dtype=torch.float32)
+        spec = torch.fft.rfftn(x)
+        y = torch.empty_like(x)
+
+        def timed(f):
+            f()
+            torch.cuda.synchronize()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record()
+            for _ in range(reps):
+                f()
+            b.record()
+            b.synchronize()
+            return a.elapsed_time(b) / reps
+        cr = timed(lambda: torch.fft.rfftn(x, out=spec))
+        cc = timed(lambda: torch.fft.irfftn(spec, s=(n, n, n), out=y))
+        out["runs"][str(n)] = {"r2c_ms": r2c.value, "c2r_ms": c2r.value, "cufft_r2c_ms": cr,
+                               "cufft_c2r_ms": cc, "r2c_speedup": cr / r2c.value,
+                               "c2r_speedup": cc / c2r.value}
+        del x, spec, y
+        torch.cuda.empty_cache()
+    print(json.dumps(out))
+    return 0
 
 
 def run_batch(args):

@@ -52,6 +52,7 @@ SIGNATURES = {
     "cg_pk_bins_noalloc": (i32, [P, i32, f32, i32, i32, P, P, P, i64, P]),
     "cg_sim_stream": (P, [P]),
     "cg_sim_copy_particles": (i32, [P, P]),
+    "cg_sim_set_sort_interval": (i32, [P, i32]),
     "cg_net_create": (i32, [ctypes.POINTER(P), i32, ctypes.c_ulonglong]),
     "cg_net_destroy": (None, [P]),
     "cg_net_num_params": (i32, []),
@@ -82,6 +83,7 @@ SIGNATURES = {
     "cg_set_schedule": (i32, [i32, i32, i32]),
     "cg_fft_r2c": (i32, [i32, P, P]),
     "cg_fft_c2r": (i32, [i32, P, P]),
+    "cg_fft_time": (i32, [i32, i32, fptr, fptr]),
     "cg_launch_count": (i64, []),
     "cg_stage_name": (ctypes.c_char_p, [i32]),
     "cg_prof_begin": (i32, [i32]),
@@ -146,7 +148,7 @@ def load(build_if_missing=True):
     return lib
 
 
-NSTAGES = 15   # CG_ST_COUNT in csrc/internal.h
+NSTAGES = 16   # CG_ST_COUNT in csrc/internal.h
 
 
 def check(rc, what=""):

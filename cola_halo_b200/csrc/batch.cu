@@ -129,7 +129,7 @@ cudaError_t record_realization(cg_batch* b, Real& r, StreamBufs& sb) {
       const float Dv2 = (float)b->ct->D2v((double)aout);
       written = true;
       return dev_snapshot(cx, cv, cf, c1, c2, r.ps.n, b->ct->om32, dda, q1, q2, Dv, Dv2, dyyy,
-                          da1, da2, vfac, r.ps.id, r.snap, st);
+                          da1, da2, vfac, r.ps.id, nullptr, r.snap, st);
     };
     if (avel0 <= aout && aout <= apos0) {
       if ((e = snapshot()) != cudaSuccess) return e;

@@ -88,14 +88,22 @@ struct cg_sim {
   void* d_aos = nullptr;      // staging: Particle (56 B) / ParticleMinimum (32 B) arrays
   bool aos_snapshot = false;  // d_aos holds the last snapshot (ParticleMinimum[n])
   float* soa_block = nullptr; // one allocation for all SoA float arrays
+  long long* id_alloc = nullptr;
+  int* orig_alloc = nullptr;
+  ParticleOrder order;        // cell-order sort (reorder.cu)
+  int sort_every = 2;         // sort at every sort_every-th move (0: never)
+  long long moves = 0;
+  bool sorted = false;        // the arrays are in an order of their own
 };
 
 static void sim_free(cg_sim* s) {
   if (!s) return;
   if (s->st) cudaStreamSynchronize(s->st);
   pm_plan_free(&s->pm);
+  particle_order_free(&s->order);
   cudaFree(s->soa_block);
-  cudaFree(s->ps.id);
+  cudaFree(s->id_alloc);
+  cudaFree(s->orig_alloc);
   cudaFree(s->d_aos);
   if (s->st) cudaStreamDestroy(s->st);
   delete s;
@@ -123,8 +131,12 @@ extern "C" int cg_sim_create(cg_sim** out, int nc, int ngrid, float boxsize, dou
     s->ps.cap = np_capacity;
     e = cudaMalloc(&s->soa_block, sizeof(float) * 15 * (size_t)np_capacity);
   }
-  if (e == cudaSuccess) e = cudaMalloc(&s->ps.id, sizeof(long long) * (size_t)np_capacity);
+  if (e == cudaSuccess) e = cudaMalloc(&s->id_alloc, sizeof(long long) * (size_t)np_capacity);
+  if (e == cudaSuccess) e = cudaMalloc(&s->orig_alloc, sizeof(int) * (size_t)np_capacity);
   if (e == cudaSuccess) e = cudaMalloc(&s->d_aos, 56 * (size_t)np_capacity);
+  s->ps.id = s->id_alloc;
+  s->ps.orig = s->orig_alloc;
+  if (const char* ev = getenv("COLAGPU_SORT_EVERY")) s->sort_every = atoi(ev) > 0 ? atoi(ev) : 0;
   if (e != cudaSuccess) {
     int rc = cuda_err(e, "cg_sim_create");
     sim_free(s);
@@ -161,10 +173,15 @@ extern "C" int cg_sim_set_particles(cg_sim* s, const void* particles, long long 
   if (np < 0 || np > s->ps.cap)
     return set_err(CG_EINVAL, "cg_sim_set_particles: np=%lld exceeds capacity %lld", np,
                    s->ps.cap);
+  // forces already computed keep their meaning for particles given again in
+  // the same order (the caller's order, which the upload restores)
+  if (s->sorted) CG_CHECK(particles_unsort_forces(&s->ps, &s->order, s->st), "unsort forces");
+  s->sorted = false;
   s->ps.n = np;
   s->a_x = a_x;
   s->a_v = a_v;
   s->aos_snapshot = false;
+  s->moves = 0;
   if (np == 0) return CG_OK;
   const cudaMemcpyKind kind =
       is_device_ptr(particles) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
@@ -188,19 +205,33 @@ extern "C" int cg_sim_get_forces(cg_sim* s, float* f) {
   if (!s || !f) return set_err(CG_EINVAL, "cg_sim_get_forces: NULL");
   const size_t n = (size_t)s->ps.n;
   if (n == 0) return CG_OK;
-  // interleave on the host side: copy three component arrays into (n,3)
+  // interleave on the host side: copy three component arrays into (n,3),
+  // each particle at its caller's index
   float* tmp = (float*)malloc(sizeof(float) * 3 * n);
-  if (!tmp) return set_err(CG_ENOMEM, "host malloc");
-  for (int a = 0; a < 3; a++) {
-    cudaError_t e = cudaMemcpyAsync(tmp + a * n, s->ps.f[a], sizeof(float) * n,
-                                    cudaMemcpyDeviceToHost, s->st);
-    if (e != cudaSuccess) { free(tmp); return cuda_err(e, "download forces"); }
+  int* orig = (int*)malloc(sizeof(int) * n);
+  if (!tmp || !orig) {
+    free(tmp);
+    free(orig);
+    return set_err(CG_ENOMEM, "host malloc");
   }
-  cudaError_t e = cudaStreamSynchronize(s->st);
-  if (e != cudaSuccess) { free(tmp); return cuda_err(e, "sync"); }
-  for (size_t i = 0; i < n; i++)
-    for (int a = 0; a < 3; a++) f[3 * i + a] = tmp[a * n + i];
+  cudaError_t e = cudaSuccess;
+  for (int a = 0; a < 3 && e == cudaSuccess; a++)
+    e = cudaMemcpyAsync(tmp + a * n, s->ps.f[a], sizeof(float) * n, cudaMemcpyDeviceToHost,
+                        s->st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(orig, s->ps.orig, sizeof(int) * n, cudaMemcpyDeviceToHost, s->st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
+  if (e != cudaSuccess) {
+    free(tmp);
+    free(orig);
+    return cuda_err(e, "download forces");
+  }
+  for (size_t i = 0; i < n; i++) {
+    const size_t j = (size_t)orig[i] < n ? (size_t)orig[i] : i;
+    for (int a = 0; a < 3; a++) f[3 * j + a] = tmp[a * n + i];
+  }
   free(tmp);
+  free(orig);
   return CG_OK;
 }
 
@@ -217,6 +248,18 @@ extern "C" void* cg_sim_stream(cg_sim* s) { return s ? (void*)s->st : nullptr; }
 extern "C" int cg_sim_move(cg_sim* s) {
   if (!s) return set_err(CG_EINVAL, "cg_sim_move: NULL");
   CG_CHECK(dev_wrap(s->ps.x, s->ps.n, s->L, s->st), "wrap");
+  if (s->sort_every > 0 && ++s->moves % s->sort_every == 0) {
+    // the caller's view is unchanged: outputs go back through orig
+    s->aos_snapshot = false;
+    CG_CHECK(particles_sort_cells(&s->ps, &s->order, s->L, s->st), "cell-order sort");
+    s->sorted = true;
+  }
+  return CG_OK;
+}
+
+extern "C" int cg_sim_set_sort_interval(cg_sim* s, int every) {
+  if (!s || every < 0) return set_err(CG_EINVAL, "cg_sim_set_sort_interval: bad arguments");
+  s->sort_every = every;
   return CG_OK;
 }
 
@@ -317,7 +360,7 @@ static int queue_snapshot(cg_sim* s, double aout, float omega_m, void* d_out) {
   const float* d1[3] = {s->ps.dx1[0], s->ps.dx1[1], s->ps.dx1[2]};
   const float* d2[3] = {s->ps.dx2[0], s->ps.dx2[1], s->ps.dx2[2]};
   CG_CHECK(dev_snapshot(x, v, f, d1, d2, s->ps.n, ct.om32, dda, q1, q2, Dv, Dv2, dyyy, da1,
-                         da2, vfac, s->ps.id, d_out, s->st),
+                         da2, vfac, s->ps.id, s->ps.orig, d_out, s->st),
            "snapshot");
   return CG_OK;
 }
@@ -401,7 +444,11 @@ extern "C" int cg_sim_copy_particles(cg_sim* dst, const cg_sim* src) {
     CG_CHECK(cudaMemcpyAsync(dst->ps.dx2[a], src->ps.dx2[a], 4 * n, cudaMemcpyDeviceToDevice, dst->st), "copy");
   }
   CG_CHECK(cudaMemcpyAsync(dst->ps.id, src->ps.id, 8 * n, cudaMemcpyDeviceToDevice, dst->st), "copy");
+  CG_CHECK(cudaMemcpyAsync(dst->ps.orig, src->ps.orig, 4 * n, cudaMemcpyDeviceToDevice, dst->st),
+           "copy");
   dst->ps.n = src->ps.n;
+  dst->sorted = src->sorted;
+  dst->aos_snapshot = false;
   dst->a_x = src->a_x;
   dst->a_v = src->a_v;
   return CG_OK;
@@ -608,6 +655,45 @@ static int host_fft(int n, const float* in, float* out, bool forward) {
   free(hs);
   mesh_fft_free(&f);
   return cuda_err(e, "cg_fft");
+}
+
+// Device time of the plain 3-D transforms on device-resident data (no
+// host copies, no layout conversion): the mean of `reps` launches each.
+extern "C" int cg_fft_time(int n, int reps, float* ms_r2c, float* ms_c2r) {
+  if (!pm_supported_mesh(n) || reps < 1) return set_err(CG_EINVAL, "cg_fft_time: bad arguments");
+  MeshFFT f;
+  CG_CHECK(mesh_fft_alloc(&f, n), "mesh_fft_alloc");
+  const size_t nh = (size_t)(n / 2 + 1);
+  float* dr = nullptr;
+  float2* ds = nullptr;
+  cudaEvent_t a = nullptr, b = nullptr;
+  cudaError_t e = cudaMalloc(&dr, sizeof(float) * (size_t)n * n * n);
+  if (e == cudaSuccess) e = cudaMalloc(&ds, sizeof(float2) * nh * n * n);
+  if (e == cudaSuccess) e = cudaMemset(dr, 0, sizeof(float) * (size_t)n * n * n);
+  if (e == cudaSuccess) e = cudaEventCreate(&a);
+  if (e == cudaSuccess) e = cudaEventCreate(&b);
+  float t_r2c = 0.0f, t_c2r = 0.0f;
+  for (int pass = 0; pass < 2 && e == cudaSuccess; pass++) {
+    const bool fwd = pass == 0;
+    e = fwd ? mesh_r2c(&f, dr, ds, 0) : mesh_c2r(&f, ds, dr, 0);      // warm-up
+    if (e == cudaSuccess) e = cudaEventRecord(a, 0);
+    for (int r = 0; r < reps && e == cudaSuccess; r++)
+      e = fwd ? mesh_r2c(&f, dr, ds, 0) : mesh_c2r(&f, ds, dr, 0);
+    if (e == cudaSuccess) e = cudaEventRecord(b, 0);
+    if (e == cudaSuccess) e = cudaEventSynchronize(b);
+    float ms = 0.0f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, a, b);
+    (fwd ? t_r2c : t_c2r) = ms / reps;
+  }
+  if (a) cudaEventDestroy(a);
+  if (b) cudaEventDestroy(b);
+  cudaFree(dr);
+  cudaFree(ds);
+  mesh_fft_free(&f);
+  if (e != cudaSuccess) return cuda_err(e, "cg_fft_time");
+  if (ms_r2c) *ms_r2c = t_r2c;
+  if (ms_c2r) *ms_c2r = t_c2r;
+  return CG_OK;
 }
 
 extern "C" int cg_fft_r2c(int n, const float* real_in, float* spec_out) {

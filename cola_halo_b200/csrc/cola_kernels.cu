@@ -147,6 +147,7 @@ __global__ void __launch_bounds__(T) k_snapshot(C3 x, C3 v, C3 f, C3 dx1, C3 dx2
                                                 float Dv, float Dv2, float dyyy, float da1,
                                                 float da2, float vfac,
                                                 const long long* __restrict__ id,
+                                                const int* __restrict__ orig,
                                                 PMin* __restrict__ out) {
   long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long stride = (long long)gridDim.x * blockDim.x;
@@ -165,13 +166,14 @@ __global__ void __launch_bounds__(T) k_snapshot(C3 x, C3 v, C3 f, C3 dx1, C3 dx2
       o.x[a] = __fadd_rn(p, __fadd_rn(__fmul_rn(d1, da1), __fmul_rn(d2, da2)));
     }
     o.id = id[i];
-    out[i] = o;
+    out[orig ? orig[i] : i] = o;
   }
 }
 
 __global__ void __launch_bounds__(T) k_aos_to_soa(const PFull* __restrict__ in, long long n,
                                                   P3 x, P3 dx1, P3 dx2, P3 v,
-                                                  long long* __restrict__ id) {
+                                                  long long* __restrict__ id,
+                                                  int* __restrict__ orig) {
   long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long stride = (long long)gridDim.x * blockDim.x;
   for (; i < n; i += stride) {
@@ -184,12 +186,14 @@ __global__ void __launch_bounds__(T) k_aos_to_soa(const PFull* __restrict__ in, 
       v.p[a][i] = p.v[a];
     }
     id[i] = p.id;
+    if (orig) orig[i] = (int)i;
   }
 }
 
 __global__ void __launch_bounds__(T) k_soa_to_aos(PFull* __restrict__ out, long long n, C3 x,
                                                   C3 dx1, C3 dx2, C3 v,
-                                                  const long long* __restrict__ id) {
+                                                  const long long* __restrict__ id,
+                                                  const int* __restrict__ orig) {
   long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long stride = (long long)gridDim.x * blockDim.x;
   for (; i < n; i += stride) {
@@ -202,7 +206,7 @@ __global__ void __launch_bounds__(T) k_soa_to_aos(PFull* __restrict__ out, long 
       p.v[a] = v.p[a][i];
     }
     p.id = id[i];
-    out[i] = p;
+    out[orig ? orig[i] : i] = p;
   }
 }
 
@@ -247,14 +251,14 @@ cudaError_t dev_snapshot(const float* const x[3], const float* const v[3],
                           const float* const f[3], const float* const dx1[3],
                           const float* const dx2[3], long long n, float omega_m, float dda,
                           float q1, float q2, float Dv, float Dv2, float dyyy, float da1,
-                          float da2, float vfac, const long long* id, void* out_aos,
-                          cudaStream_t st) {
+                          float da2, float vfac, const long long* id, const int* orig,
+                          void* out_aos, cudaStream_t st) {
   const double c = -1.5 * (double)omega_m;
   prof_mark(st, CG_ST_SNAPSHOT);
   if (n > 0)
     k_snapshot<<<grid_for(n), T, 0, st>>>(mkc(x), mkc(v), mkc(f), mkc(dx1), mkc(dx2), n, c,
                                           dda, q1, q2, Dv, Dv2, dyyy, da1, da2, vfac, id,
-                                          reinterpret_cast<PMin*>(out_aos));
+                                          orig, reinterpret_cast<PMin*>(out_aos));
   return cudaGetLastError();
 }
 
@@ -262,7 +266,8 @@ cudaError_t particles_aos_to_soa(const void* aos, ParticleSoA* s, cudaStream_t s
   prof_mark(st, CG_ST_OTHER);
   if (s->n > 0)
     k_aos_to_soa<<<grid_for(s->n), T, 0, st>>>(reinterpret_cast<const PFull*>(aos), s->n,
-                                               mk(s->x), mk(s->dx1), mk(s->dx2), mk(s->v), s->id);
+                                               mk(s->x), mk(s->dx1), mk(s->dx2), mk(s->v), s->id,
+                                               s->orig);
   return cudaGetLastError();
 }
 
@@ -271,6 +276,6 @@ cudaError_t particles_soa_to_aos(void* aos, const ParticleSoA* s, cudaStream_t s
   if (s->n > 0)
     k_soa_to_aos<<<grid_for(s->n), T, 0, st>>>(reinterpret_cast<PFull*>(aos), s->n,
                                                mkc(s->x), mkc(s->dx1), mkc(s->dx2), mkc(s->v),
-                                               s->id);
+                                               s->id, s->orig);
   return cudaGetLastError();
 }

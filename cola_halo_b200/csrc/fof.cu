@@ -30,13 +30,13 @@
 #include "../../include/colagpu_dropin.h"
 #include "gadget.h"
 #include "internal.h"
+#include "scan.cuh"
 
 extern int cg_set_error_from_lpt(int code, const char* msg);
 
 namespace {
 
 constexpr int T = CG_THREADS;
-constexpr int SCAN_B = 1024;            // elements per scan block
 constexpr int MAX_NCELL = 512;          // cells per dimension at most
 constexpr int kRetryLimit = 1 << 22;    // union / find iterations per call
 
@@ -81,56 +81,6 @@ __global__ void k_fof_bin(const PMin* __restrict__ p, long long n, float L, floa
     key[i] = k;
     atomicAdd(count + k, 1u);
   }
-}
-
-// Exclusive scan of n unsigned values: per-block scans, a scan of the
-// block sums by one CTA, then the block offsets added back.
-__global__ void __launch_bounds__(SCAN_B) k_scan_blocks(const unsigned* __restrict__ in,
-                                                        unsigned* __restrict__ out, long long n,
-                                                        unsigned* __restrict__ bsum) {
-  __shared__ unsigned s[SCAN_B];
-  const long long i = (long long)blockIdx.x * SCAN_B + threadIdx.x;
-  const unsigned v = i < n ? in[i] : 0u;
-  s[threadIdx.x] = v;
-  __syncthreads();
-  for (int o = 1; o < SCAN_B; o <<= 1) {
-    const unsigned t = threadIdx.x >= (unsigned)o ? s[threadIdx.x - o] : 0u;
-    __syncthreads();
-    s[threadIdx.x] += t;
-    __syncthreads();
-  }
-  if (i < n) out[i] = s[threadIdx.x] - v;
-  if (threadIdx.x == SCAN_B - 1) bsum[blockIdx.x] = s[threadIdx.x];
-}
-
-__global__ void __launch_bounds__(SCAN_B) k_scan_sums(unsigned* __restrict__ bsum, int nb,
-                                                      unsigned* __restrict__ total) {
-  __shared__ unsigned s[SCAN_B];
-  unsigned carry = 0;
-  for (int base = 0; base < nb; base += SCAN_B) {
-    const int i = base + threadIdx.x;
-    const unsigned v = i < nb ? bsum[i] : 0u;
-    s[threadIdx.x] = v;
-    __syncthreads();
-    for (int o = 1; o < SCAN_B; o <<= 1) {
-      const unsigned t = threadIdx.x >= (unsigned)o ? s[threadIdx.x - o] : 0u;
-      __syncthreads();
-      s[threadIdx.x] += t;
-      __syncthreads();
-    }
-    if (i < nb) bsum[i] = carry + s[threadIdx.x] - v;
-    const unsigned chunk = s[SCAN_B - 1];
-    __syncthreads();
-    carry += chunk;
-  }
-  if (threadIdx.x == 0 && total) *total = carry;
-}
-
-__global__ void k_scan_add(unsigned* __restrict__ out, long long n,
-                           const unsigned* __restrict__ bsum) {
-  for (long long i = (long long)blockIdx.x * T + threadIdx.x; i < n;
-       i += (long long)gridDim.x * T)
-    out[i] += bsum[i / SCAN_B];
 }
 
 __global__ void k_fof_scatter(const float* __restrict__ xw, const unsigned* __restrict__ key,
@@ -303,23 +253,6 @@ __global__ void k_fof_finish(const float* __restrict__ xw, const unsigned* __res
   }
 }
 
-// Exclusive scan of n values in place into `out` (bsum: ceil(n/SCAN_B)
-// entries of scratch); *total (device) receives the sum.
-void scan(const unsigned* in, unsigned* out, long long n, unsigned* bsum, unsigned* total,
-          cudaStream_t st) {
-  const long long nb = (n + SCAN_B - 1) / SCAN_B;
-  if (nb == 0) {
-    cudaMemsetAsync(total, 0, sizeof(unsigned), st);
-    return;
-  }
-  prof_mark(st, CG_ST_OTHER);
-  k_scan_blocks<<<(unsigned)nb, SCAN_B, 0, st>>>(in, out, n, bsum);
-  prof_mark(st, CG_ST_OTHER);
-  k_scan_sums<<<1, SCAN_B, 0, st>>>(bsum, (int)nb, total);
-  prof_mark(st, CG_ST_OTHER);
-  k_scan_add<<<grid_for(n), T, 0, st>>>(out, n, bsum);
-}
-
 template <class TPtr>
 void release(TPtr*& p) {
   if (p) cudaFree(p);
@@ -345,7 +278,7 @@ extern "C" int cg_fof(const void* pmin, long long np, float boxsize, float ll, i
   if (nc < 1) nc = 1;
   const long long ncells = nc * nc * nc;
   const float inv = (float)nc / boxsize;
-  const long long nblk = ((ncells > np ? ncells : np) + SCAN_B - 1) / SCAN_B;
+  const long long nblk = cgscan::scratch_entries(ncells > np ? ncells : np);
 
   cudaPointerAttributes attr;
   bool on_device = cudaPointerGetAttributes(&attr, pmin) == cudaSuccess &&
@@ -386,7 +319,7 @@ extern "C" int cg_fof(const void* pmin, long long np, float boxsize, float ll, i
     const int g = grid_for(np);
     prof_mark(st, CG_ST_OTHER);
     k_fof_bin<<<g, T, 0, st>>>(d_p, np, boxsize, inv, (int)nc, xw, key, count);
-    scan(count, start, ncells, bsum, word, st);
+    cgscan::exclusive(count, start, ncells, bsum, word, CG_ST_OTHER, st);
     prof_mark(st, CG_ST_OTHER);
     k_fof_scatter<<<g, T, 0, st>>>(xw, key, np, start, cursor, pos);
     prof_mark(st, CG_ST_OTHER);
@@ -400,7 +333,7 @@ extern "C" int cg_fof(const void* pmin, long long np, float boxsize, float ll, i
     k_fof_roots<<<g, T, 0, st>>>(parent, np, word + 1);
     prof_mark(st, CG_ST_OTHER);
     k_fof_flag<<<g, T, 0, st>>>(parent, size, np, (unsigned)nfof_min, flag);
-    scan(flag, hid, np, bsum, word, st);
+    cgscan::exclusive(flag, hid, np, bsum, word, CG_ST_OTHER, st);
     e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaMemcpy(&nh, word, sizeof(unsigned), cudaMemcpyDeviceToHost);
     if (e == cudaSuccess && nh > 0) {

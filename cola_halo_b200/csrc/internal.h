@@ -10,7 +10,7 @@
 enum {
   CG_ST_FILL = 0, CG_ST_DEPOSIT, CG_ST_FZ, CG_ST_FX_FWD, CG_ST_GREEN, CG_ST_FX_INV,
   CG_ST_ZI, CG_ST_INTERP, CG_ST_WRAP, CG_ST_KICK, CG_ST_DRIFT, CG_ST_SNAPSHOT, CG_ST_LPT,
-  CG_ST_OTHER, CG_ST_KICK_DRIFT, CG_ST_COUNT
+  CG_ST_OTHER, CG_ST_KICK_DRIFT, CG_ST_SORT, CG_ST_COUNT
 };
 // Call before every kernel launch: counts it and, while a profile is open,
 // records a CUDA event on the launch stream.
@@ -107,7 +107,10 @@ cudaError_t pm_interp(PmPlan* p, const float* const x[3], long long n,
                       float* const f[3], cudaStream_t st);
 
 // Particle state on the device, structure of arrays (one array per
-// component), in the caller's particle order.
+// component).  The arrays may be kept in an order of their own (cell
+// order, reorder.cu); orig[i] is then the caller's index of particle i, and
+// everything handed back to the caller is put in the caller's order by it.
+// orig == NULL means the caller's order.
 struct ParticleSoA {
   long long n;              // particles held
   long long cap;            // capacity
@@ -117,6 +120,7 @@ struct ParticleSoA {
   float* dx2[3];
   float* f[3];
   long long* id;
+  int* orig;
 };
 
 // cola_kernels.cu
@@ -138,8 +142,45 @@ cudaError_t dev_snapshot(const float* const x[3], const float* const v[3],
                           const float* const dx2[3], long long n,
                           float omega_m, float dda, float q1, float q2,
                           float Dv, float Dv2, float dyyy, float da1, float da2,
-                          float vfac, const long long* id, void* out_aos,
+                          float vfac, const long long* id, const int* orig, void* out_aos,
                           cudaStream_t st);
-// AoS (reference Particle, 56 B) <-> SoA conversion on the device.
+// AoS (reference Particle, 56 B) <-> SoA conversion on the device.  The
+// upload resets orig to the caller's order; the download writes particle i
+// at orig[i].
 cudaError_t particles_aos_to_soa(const void* aos, ParticleSoA* s, cudaStream_t st);
 cudaError_t particles_soa_to_aos(void* aos, const ParticleSoA* s, cudaStream_t st);
+
+// reorder.cu: cell order of the particles.  Particles are sorted by the
+// cell of a grid of about eight particles per cell (x slowest, z fastest), so
+// that consecutive threads of the deposit and the interpolation touch
+// neighbouring mesh cells.  A counting sort: bin counts (each particle's
+// rank in its bin from the same atomic), a prefix sum, and one scatter of x, v, dx1, dx2, f, id and orig into a second set of
+// arrays, which then becomes the working set.
+struct ParticleOrder {
+  long long cap = 0;        // particles the arrays hold
+  long long nbins = 0;      // bins the counts hold
+  float* alloc = nullptr;   // owned: 15 floats per particle
+  long long* alloc_id = nullptr;
+  int* alloc_orig = nullptr;
+  // the scratch set (a sort writes here, then exchanges it with the
+  // particles' working set, so these point into either allocation)
+  float* x[3] = {nullptr, nullptr, nullptr};
+  float* v[3] = {nullptr, nullptr, nullptr};
+  float* dx1[3] = {nullptr, nullptr, nullptr};
+  float* dx2[3] = {nullptr, nullptr, nullptr};
+  float* f[3] = {nullptr, nullptr, nullptr};
+  long long* id = nullptr;
+  int* orig = nullptr;
+  unsigned* key = nullptr;  // per particle: its bin, then (cap on) its rank in the bin
+  unsigned* cnt = nullptr;  // per bin: count, then start
+  unsigned* bsum = nullptr; // scan scratch
+};
+void particle_order_free(ParticleOrder* o);
+// Sort s into cell order, allocating o's arrays on first use (o's
+// capacity is s->cap).  s's array pointers are exchanged with o's scratch
+// set, so the owner of s must free its arrays through the allocations it
+// made, not through s's current pointers.
+cudaError_t particles_sort_cells(ParticleSoA* s, ParticleOrder* o, float L, cudaStream_t st);
+// Put s's forces back in the caller's order (before the particles
+// themselves are replaced in that order); o holds the scratch arrays.
+cudaError_t particles_unsort_forces(ParticleSoA* s, ParticleOrder* o, cudaStream_t st);

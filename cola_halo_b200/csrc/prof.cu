@@ -29,7 +29,8 @@ Profile g_prof;
 
 const char* kNames[CG_ST_COUNT] = {"fill", "deposit", "fz_r2c", "fx_fwd", "green_y",
                                     "fx_inv", "zi_c2r", "interp", "wrap", "kick",
-                                    "drift", "snapshot", "lpt", "other", "kick_drift"};
+                                    "drift", "snapshot", "lpt", "other", "kick_drift",
+                                    "sort"};
 }  // namespace
 
 void prof_mark(cudaStream_t st, int stage) {

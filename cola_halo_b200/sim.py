@@ -135,6 +135,12 @@ class Simulation:
         _lib.check(self.lib.cg_sim_write_gadget(self.h, aout, om, h, str(filename).encode(),
                                                 int(bool(use_long_id))), "cg_sim_write_gadget")
 
+    def set_sort_interval(self, every):
+        """Sort the particles into cell order at every `every`-th move (0:
+        never); outputs keep the order the particles were given in."""
+        _lib.check(self.lib.cg_sim_set_sort_interval(self.h, int(every)),
+                   "cg_sim_set_sort_interval")
+
     def sync(self):
         _lib.check(self.lib.cg_sim_sync(self.h), "cg_sim_sync")
 

@@ -79,6 +79,15 @@ long long cg_sim_np(cg_sim* s);
 
 /* move_particles2 on one GPU (move.c:34-41): periodic wrap of x, y, z. */
 int cg_sim_move(cg_sim* s);
+/* Cell order (no reference counterpart): every `every`-th cg_sim_move
+ * (default 2; 0 = never; the environment variable COLAGPU_SORT_EVERY sets
+ * the default) sorts the particles on the device by a grid of about eight
+ * particles per cell, so that the deposit and the interpolation keep the
+ * memory locality of the initial lattice as structure forms.  Results are
+ * unchanged up to the order of the deposit's float additions: every output
+ * (cg_sim_get_particles, cg_sim_get_forces, snapshots) is in the order the
+ * particles were given in. */
+int cg_sim_set_sort_interval(cg_sim* s, int every);
 /* pm_calculate_forces (pm.c:565-596).  If density_sum is non-NULL the
  * stream is synchronised and the mesh sum (check_total_density) returned. */
 int cg_sim_forces(cg_sim* s, double* density_sum);
@@ -208,6 +217,10 @@ int cg_batch_last_ms(cg_batch* b, float* ms);
  * FFTW's c2r does.  Synchronous; allocates its own scratch. */
 int cg_fft_r2c(int n, const float* real_in, float* spec_out);
 int cg_fft_c2r(int n, const float* spec_in, float* real_out);
+/* Device time in ms of one r2c and one c2r of an n^3 mesh held in device
+ * memory (the mean of `reps` launches after a warm-up); for comparing the
+ * transforms with other FFT implementations. */
+int cg_fft_time(int n, int reps, float* ms_r2c, float* ms_c2r);
 
 /* Friends-of-friends halos (fof.c:427-1181 on one process).  pmin: np
  * reference ParticleMinimum structs (32 B: x, v, id) in host or device
