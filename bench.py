@@ -113,6 +113,7 @@ class Clocks:
         self.dev = dev
         self.proc = None
         self.lines = []
+        self.n0 = 0
 
     def start(self):
         try:
@@ -122,6 +123,12 @@ class Clocks:
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            # nvidia-smi takes a moment to start: let its first sample arrive
+            # before the timed region opens, and keep only later samples
+            t0 = time.time()
+            while not self.lines and time.time() - t0 < 5.0:
+                time.sleep(0.01)
+            self.n0 = len(self.lines)
         except Exception:
             self.proc = None
 
@@ -132,6 +139,11 @@ class Clocks:
     def stop(self):
         if not self.proc:
             return None
+        # a region shorter than the sampling period: take the sample that
+        # follows its end
+        t0 = time.time()
+        while len(self.lines) <= self.n0 and time.time() - t0 < 0.5:
+            time.sleep(0.005)
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
@@ -140,7 +152,7 @@ class Clocks:
         self.t.join(timeout=2)
         sm, mx, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        for ln in self.lines[self.n0:] or self.lines:
             parts = [p.strip() for p in ln.split(",")]
             if len(parts) < 9:
                 continue
