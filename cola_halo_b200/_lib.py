@@ -76,6 +76,7 @@ SIGNATURES = {
     "cg_coarse_grid": (i32, [P, i64, i64, f32, i32, P, ctypes.POINTER(f64)]),
     "cg_write_gadget": (i32, [ctypes.c_char_p, P, i64, i64, i32, f32, f32, f32, f32, i32]),
     "cg_sim_write_gadget": (i32, [P, f64, f32, f32, ctypes.c_char_p, i32]),
+    "cg_sim_initial_snapshot": (i32, [P, f32, P]),
     "cg_snapshot_invalidate": (None, []),
     "cg_autotune": (i32, [i32, i32, P, P]),
     "cg_schedule_variants": (i32, [i32, ctypes.POINTER(i32), ctypes.POINTER(i32)]),
@@ -100,6 +101,7 @@ SIGNATURES = {
     "cola_kick": (None, [P, f32, f32]),
     "cola_drift": (None, [P, f32, f32]),
     "cola_set_snapshot": (None, [f64, P, P]),
+    "set_noncola_initial": (None, [P, P]),
     "move_particles2": (None, [P, f32, P, sz]),
     "lpt_init": (None, [i32, P, sz]),
     "lpt_set_displacement": (i32, [f64, f64, i32, f64, P]),

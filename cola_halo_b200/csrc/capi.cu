@@ -376,6 +376,23 @@ extern "C" int cg_sim_snapshot(cg_sim* s, double aout, float omega_m, void* pmin
   return CG_OK;
 }
 
+// set_noncola_initial (cola.c:297-338) on the device: the snapshot of the
+// 2LPT initial condition at a_x, downloaded into pmin_out.
+extern "C" int cg_sim_initial_snapshot(cg_sim* s, float omega_m, void* pmin_out) {
+  if (!s || !pmin_out) return set_err(CG_EINVAL, "cg_sim_initial_snapshot: NULL");
+  const float aout = s->a_x;
+  ColaTime ct(omega_m);
+  const float vfac = 100.0f / aout;                              // cola.c:310
+  const float Dv = (float)ct.DprimeQ((double)aout, 1.0);         // cola.c:312
+  const float Dv2 = (float)ct.D2v((double)aout);                 // cola.c:313
+  CG_CHECK(dev_initial_snapshot(&s->ps, vfac, Dv, Dv2, s->d_aos, s->st), "initial snapshot");
+  s->aos_snapshot = true;
+  CG_CHECK(cudaMemcpyAsync(pmin_out, s->d_aos, 32 * (size_t)s->ps.n, cudaMemcpyDefault, s->st),
+           "download snapshot");
+  CG_CHECK(cudaStreamSynchronize(s->st), "sync");
+  return CG_OK;
+}
+
 extern "C" int cg_sim_write_gadget(cg_sim* s, double aout, float omega_m, float h,
                                    const char* filename, int use_long_id) {
   if (!s || !filename) return set_err(CG_EINVAL, "cg_sim_write_gadget: NULL");
@@ -942,6 +959,25 @@ extern "C" void cola_set_snapshot(const double aout, Particles const* const part
   snapshot->np_local = particles->np_local;          // cola.c:412-414
   snapshot->np_average = particles->np_average;
   snapshot->a = (float)aout;
+  g_drop.snap_p = g_drop.full_sync ? nullptr : snapshot->p;
+  g_drop.snap_np = snapshot->np_local;
+}
+
+extern "C" void set_noncola_initial(Particles const* const particles, Snapshot* const snapshot) {
+  if (!bind(particles, false)) return;
+  if (snapshot->np_allocated < particles->np_local) {
+    dropin_fail(4002, "set_noncola_initial: snapshot holds %d < %d particles",
+                snapshot->np_allocated, particles->np_local);
+    return;
+  }
+  if (cg_sim_initial_snapshot(g_drop.sim, snapshot->omega_m, snapshot->p)) {
+    dropin_fail(4001, "set_noncola_initial: %s", cg_last_error());
+    return;
+  }
+  snapshot->np_local = particles->np_local;          // cola.c:333-336
+  snapshot->np_total = particles->np_total;
+  snapshot->np_average = particles->np_average;
+  snapshot->a = particles->a_x;
   g_drop.snap_p = g_drop.full_sync ? nullptr : snapshot->p;
   g_drop.snap_np = snapshot->np_local;
 }

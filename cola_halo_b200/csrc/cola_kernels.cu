@@ -170,6 +170,28 @@ __global__ void __launch_bounds__(T) k_snapshot(C3 x, C3 v, C3 f, C3 dx1, C3 dx2
   }
 }
 
+// set_noncola_initial (cola.c:297-338): positions as they are, 2LPT
+// velocities vfac (dx1 Dv + dx2 Dv2) in float, in the caller's order
+__global__ void __launch_bounds__(T) k_initial_snapshot(C3 x, C3 dx1, C3 dx2, long long n,
+                                                        float vfac, float Dv, float Dv2,
+                                                        const long long* __restrict__ id,
+                                                        const int* __restrict__ orig,
+                                                        PMin* __restrict__ out) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (; i < n; i += stride) {
+    PMin o;
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      const float d1 = dx1.p[a][i], d2 = dx2.p[a][i];
+      o.v[a] = __fmul_rn(vfac, __fadd_rn(__fmul_rn(d1, Dv), __fmul_rn(d2, Dv2)));
+      o.x[a] = x.p[a][i];
+    }
+    o.id = id[i];
+    out[orig ? orig[i] : i] = o;
+  }
+}
+
 __global__ void __launch_bounds__(T) k_aos_to_soa(const PFull* __restrict__ in, long long n,
                                                   P3 x, P3 dx1, P3 dx2, P3 v,
                                                   long long* __restrict__ id,
@@ -259,6 +281,16 @@ cudaError_t dev_snapshot(const float* const x[3], const float* const v[3],
     k_snapshot<<<grid_for(n), T, 0, st>>>(mkc(x), mkc(v), mkc(f), mkc(dx1), mkc(dx2), n, c,
                                           dda, q1, q2, Dv, Dv2, dyyy, da1, da2, vfac, id,
                                           orig, reinterpret_cast<PMin*>(out_aos));
+  return cudaGetLastError();
+}
+
+cudaError_t dev_initial_snapshot(const ParticleSoA* s, float vfac, float Dv, float Dv2,
+                                 void* out_aos, cudaStream_t st) {
+  prof_mark(st, CG_ST_SNAPSHOT);
+  if (s->n > 0)
+    k_initial_snapshot<<<grid_for(s->n), T, 0, st>>>(mkc(s->x), mkc(s->dx1), mkc(s->dx2), s->n,
+                                                     vfac, Dv, Dv2, s->id, s->orig,
+                                                     reinterpret_cast<PMin*>(out_aos));
   return cudaGetLastError();
 }
 

@@ -144,6 +144,10 @@ cudaError_t dev_snapshot(const float* const x[3], const float* const v[3],
                           float Dv, float Dv2, float dyyy, float da1, float da2,
                           float vfac, const long long* id, const int* orig, void* out_aos,
                           cudaStream_t st);
+// set_noncola_initial (cola.c:297-338): ParticleMinimum of the positions and
+// the 2LPT velocities vfac (dx1 Dv + dx2 Dv2), in the caller's order.
+cudaError_t dev_initial_snapshot(const ParticleSoA* s, float vfac, float Dv, float Dv2,
+                                 void* out_aos, cudaStream_t st);
 // AoS (reference Particle, 56 B) <-> SoA conversion on the device.  The
 // upload resets orig to the caller's order; the download writes particle i
 // at orig[i].

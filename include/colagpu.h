@@ -262,6 +262,10 @@ int cg_write_gadget(const char* filename, const void* pmin, long long np, long l
                     int use_long_id);
 /* The snapshot at aout (as cg_sim_snapshot) written straight from the
  * device as a GADGET-1 file, with no host copy of the particles. */
+/* set_noncola_initial (cola.c:297-338): the snapshot of the 2LPT initial
+ * condition at the current a_x (positions, velocities 100/a (dx1 D1' +
+ * dx2 D2')) into pmin_out (np ParticleMinimum, host or device). */
+int cg_sim_initial_snapshot(cg_sim* s, float omega_m, void* pmin_out);
 int cg_sim_write_gadget(cg_sim* s, double aout, float omega_m, float h, const char* filename,
                         int use_long_id);
 

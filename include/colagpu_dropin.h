@@ -91,6 +91,10 @@ void cola_drift(Particles* const particles, const float Omega_m, const float apo
 /* cola.h:18 (cola.c:341-416) */
 void cola_set_snapshot(const double aout, Particles const* const particles,
                        Snapshot* const snapshot);
+/* cola.h:16 (cola.c:297-338): snapshot of the 2LPT initial condition at
+ * particles->a_x (positions, 2LPT velocities in km/s), for the initial
+ * condition file of main.c:131-137. */
+void set_noncola_initial(Particles const* const particles, Snapshot* const snapshot);
 /* move.h:7 (move.c:15-98); one process: the periodic wrap (move.c:34-41). */
 void move_particles2(Particles* const particles, const float BoxSize, void* const buf,
                      const size_t size);

@@ -8,7 +8,8 @@
  * the reference's hot path uses is provided (pm.c:150-159,461-472,494,520-545;
  * move.c:87-168; comm.c:39-177; lpt.c:566; power.c:43-58; msg.c:36-45;
  * fof.c:669,855-889,1094-1121 for the gathers of the halo finder;
- * write.c:39-40,280-323 for the GADGET writer and the subsample file).
+ * write.c:39-40,280-323 for the GADGET writer and the subsample file;
+ * read_param.c and main.c for the reference's own driver).
  */
 #ifndef ORACLE_SHIM_MPI_H
 #define ORACLE_SHIM_MPI_H
@@ -30,6 +31,7 @@ typedef struct { int MPI_SOURCE, MPI_TAG, MPI_ERROR; } MPI_Status;
 #define MPI_LONG_LONG 5
 #define MPI_LONG      6
 #define MPI_UNSIGNED  7
+#define MPI_CHAR      8
 
 #define MPI_SUM 1
 #define MPI_MAX 2

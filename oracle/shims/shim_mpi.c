@@ -18,6 +18,7 @@ static size_t type_size(MPI_Datatype t)
   case MPI_LONG_LONG: return sizeof(long long);
   case MPI_LONG: return sizeof(long);
   case MPI_UNSIGNED: return sizeof(unsigned);
+  case MPI_CHAR: return sizeof(char);
   default:
     fprintf(stderr, "mpi shim: unknown datatype %d\n", t);
     abort();
