@@ -307,6 +307,19 @@ extern "C" int cg_sim_drift_coeffs(cg_sim* s, float dyyy, float da1, float da2) 
   return CG_OK;
 }
 
+// kick with (dda, q1, q2), then drift with (dyyy, da1, da2) and the kicked
+// velocity, in one pass
+static int sim_kick_drift(cg_sim* s, float dda, float q1, float q2, float dyyy, float da1,
+                          float da2) {
+  const float* f[3] = {s->ps.f[0], s->ps.f[1], s->ps.f[2]};
+  const float* d1[3] = {s->ps.dx1[0], s->ps.dx1[1], s->ps.dx1[2]};
+  const float* d2[3] = {s->ps.dx2[0], s->ps.dx2[1], s->ps.dx2[2]};
+  CG_CHECK(dev_kick_drift(s->ps.x, s->ps.v, f, d1, d2, s->ps.n, s->ct->om32, dda, q1, q2, dyyy,
+                          da1, da2, s->st),
+           "kick_drift");
+  return CG_OK;
+}
+
 extern "C" int cg_sim_kick(cg_sim* s, float avel1) {
   if (!s) return set_err(CG_EINVAL, "cg_sim_kick: NULL");
   float dda, q1, q2;
@@ -333,12 +346,8 @@ extern "C" int cg_sim_kick_drift(cg_sim* s, float avel1, float apos1) {
   float dda, q1, q2, dyyy, da1, da2;
   s->ct->kick(s->a_v, s->a_x, avel1, &dda, &q1, &q2);
   s->ct->drift(s->a_x, avel1, apos1, &dyyy, &da1, &da2);
-  const float* f[3] = {s->ps.f[0], s->ps.f[1], s->ps.f[2]};
-  const float* d1[3] = {s->ps.dx1[0], s->ps.dx1[1], s->ps.dx1[2]};
-  const float* d2[3] = {s->ps.dx2[0], s->ps.dx2[1], s->ps.dx2[2]};
-  CG_CHECK(dev_kick_drift(s->ps.x, s->ps.v, f, d1, d2, s->ps.n, s->ct->om32, dda, q1, q2, dyyy,
-                          da1, da2, s->st),
-           "kick_drift");
+  const int rc = sim_kick_drift(s, dda, q1, q2, dyyy, da1, da2);
+  if (rc) return rc;
   s->a_v = avel1;
   s->a_x = apos1;
   return CG_OK;
@@ -754,6 +763,11 @@ struct DropIn {
   bool abort_on_error = true;
   const ParticleMinimum* snap_p = nullptr;   // host array of the last cola_set_snapshot
   int snap_np = -1;
+  // cola_kick is queued and run fused with the cola_drift that follows it
+  // (main.c:191-201 always calls them in that order); any other call runs
+  // it first
+  bool kick_pending = false;
+  float kick_dda = 0, kick_q1 = 0, kick_q2 = 0;
   int lpt_nc = 0;
   PowerTable power;
   bool power_ready = false;
@@ -785,11 +799,23 @@ const ColaTime& times_for(float om) {
 }
 
 // Make the device state of `p` current.  Returns false on failure.
-bool bind(const Particles* p, bool refresh) {
+// Run a queued cola_kick.  Returns false after reporting a failure.
+bool flush_kick() {
+  if (!g_drop.kick_pending) return true;
+  g_drop.kick_pending = false;
+  if (cg_sim_kick_coeffs(g_drop.sim, g_drop.kick_dda, g_drop.kick_q1, g_drop.kick_q2)) {
+    dropin_fail(4001, "cola_kick: %s", cg_last_error());
+    return false;
+  }
+  return true;
+}
+
+bool bind(const Particles* p, bool refresh, bool keep_kick = false) {
   if (!g_drop.nc_pm) {
     dropin_fail(4001, "pm_init has not been called");
     return false;
   }
+  if (!keep_kick && !flush_kick()) return false;
   const int nc = g_drop.nc_pm / g_drop.factor;
   if (!g_drop.sim) {
     long long cap = p->np_allocated > p->np_local ? p->np_allocated : p->np_local;
@@ -836,6 +862,7 @@ extern "C" void cg_dropin_set_sync(int full) { g_drop.full_sync = full != 0; }
 extern "C" void cg_dropin_set_abort(int abort_on_error) { g_drop.abort_on_error = abort_on_error != 0; }
 
 extern "C" void cg_dropin_finalize(void) {
+  g_drop.kick_pending = false;
   cg_sim_destroy(g_drop.sim);
   g_drop.sim = nullptr;
   g_drop.bound = nullptr;
@@ -921,9 +948,16 @@ extern "C" void cola_kick(Particles* const particles, const float Omega_m, const
     g_drop.sim->omega_m = Omega_m;
     g_drop.sim->ct.reset(new ColaTime(Omega_m));
   }
-  if (cg_sim_kick_coeffs(g_drop.sim, dda, q1, q2)) {
-    dropin_fail(4001, "cola_kick: %s", cg_last_error());
-    return;
+  if (g_drop.full_sync) {
+    if (cg_sim_kick_coeffs(g_drop.sim, dda, q1, q2)) {
+      dropin_fail(4001, "cola_kick: %s", cg_last_error());
+      return;
+    }
+  } else {
+    g_drop.kick_pending = true;
+    g_drop.kick_dda = dda;
+    g_drop.kick_q1 = q1;
+    g_drop.kick_q2 = q2;
   }
   particles->a_v = avel1;          // cola.c:115
   g_drop.sim->a_v = avel1;
@@ -931,11 +965,22 @@ extern "C" void cola_kick(Particles* const particles, const float Omega_m, const
 }
 
 extern "C" void cola_drift(Particles* const particles, const float Omega_m, const float apos1) {
-  if (!bind(particles, false)) return;
+  // a kick queued for these particles runs fused with this drift
+  const bool fuse = g_drop.kick_pending && particles == g_drop.bound &&
+                    particles->p == g_drop.bound_p && particles->np_local == g_drop.bound_np;
+  if (!bind(particles, false, fuse)) return;
   const ColaTime& ct = times_for(Omega_m);
   float dyyy, da1, da2;
   ct.drift(particles->a_x, particles->a_v, apos1, &dyyy, &da1, &da2);
-  if (cg_sim_drift_coeffs(g_drop.sim, dyyy, da1, da2)) {
+  int rc;
+  if (fuse && g_drop.kick_pending) {
+    g_drop.kick_pending = false;
+    rc = sim_kick_drift(g_drop.sim, g_drop.kick_dda, g_drop.kick_q1, g_drop.kick_q2, dyyy, da1,
+                        da2);
+  } else {
+    rc = cg_sim_drift_coeffs(g_drop.sim, dyyy, da1, da2);
+  }
+  if (rc) {
     dropin_fail(4001, "cola_drift: %s", cg_last_error());
     return;
   }

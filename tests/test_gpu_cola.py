@@ -96,3 +96,43 @@ def test_snapshot_bit_exact(gpu_lib, bbks_table):
     np.testing.assert_allclose(snap["x"], pos, rtol=0, atol=2e-5)
     np.testing.assert_allclose(snap["v"], vel, rtol=1e-6, atol=1e-3)
     np.testing.assert_array_equal(snap["id"], p["id"])
+
+
+def test_dropin_queued_kick_is_exact(gpu_lib):
+    """The drop-in queues cola_kick and runs it fused with the cola_drift
+    that follows, or before any other call that reads the particles: the
+    particles come out bit for bit as the two separate updates give."""
+    from cola_halo_b200.sim import drift_coeffs, kick_coeffs
+    from cola_halo_b200.types import HostParticles
+    nc, L = 16, 100.0
+    n = nc ** 3
+    om = float(np.float32(OM))
+    p = _state(n, L, 3)
+    lib = gpu_lib
+    lib.cg_dropin_set_abort(0)
+    lib.pm_init(48, 3, L, 1.25, None, 0, None, 0)
+    hp = HostParticles(nc)
+    hp.p[:n] = p
+    hp.struct.np_local = n
+    hp.struct.a_x, hp.struct.a_v = 0.3, 0.35
+    lib.move_particles2(hp.ptr, L, None, 0)
+    lib.pm_calculate_forces(hp.ptr)
+    assert lib.cg_particles_download(hp.ptr) == 0
+    x0, v0 = hp.p["x"][:n].copy(), hp.p["v"][:n].copy()
+    f0 = hp.force[:n].copy()
+    d1, d2 = p["dx1"], p["dx2"]
+    # kick then drift: one fused pass
+    lib.cola_kick(hp.ptr, om, 0.4)
+    lib.cola_drift(hp.ptr, om, 0.45)
+    assert lib.cg_particles_download(hp.ptr) == 0
+    v1 = R.cola_kick(v0, f0, d1, d2, om, *kick_coeffs(om, 0.35, 0.3, 0.4))
+    x1 = R.cola_drift(x0, v1, d1, d2, *drift_coeffs(om, 0.3, 0.4, 0.45))
+    np.testing.assert_array_equal(hp.p["v"][:n], v1)
+    np.testing.assert_array_equal(hp.p["x"][:n], x1)
+    # a queued kick runs before the next call that reads the particles
+    lib.cola_kick(hp.ptr, om, 0.5)
+    assert lib.cg_particles_download(hp.ptr) == 0
+    v2 = R.cola_kick(v1, f0, d1, d2, om, *kick_coeffs(om, 0.4, 0.45, 0.5))
+    np.testing.assert_array_equal(hp.p["v"][:n], v2)
+    np.testing.assert_array_equal(hp.p["x"][:n], x1)
+    lib.cg_dropin_finalize()
