@@ -40,6 +40,9 @@ CONFIGS = {
     "c1": dict(nc=64, factor=3, L=200.0, om=0.273, a_init=0.02, nsteps=10, seed=100),
     # one realization of the batched config (128^3, 384^3 mesh)
     "c3": dict(nc=128, factor=3, L=300.0, om=0.273, a_init=0.02, nsteps=10, seed=100),
+    # the large single-GPU case: 512^3 particles on a 1024^3 mesh (factor 2),
+    # the same mean particle spacing as c2
+    "c5": dict(nc=512, factor=2, L=1200.0, om=0.273, a_init=0.02, nsteps=10, seed=100),
 }
 
 METRIC = "particle-steps/s"
