@@ -91,7 +91,7 @@ struct cg_sim {
   long long* id_alloc = nullptr;
   int* orig_alloc = nullptr;
   ParticleOrder order;        // cell-order sort (reorder.cu)
-  int sort_every = 2;         // sort at every sort_every-th move (0: never)
+  int sort_every = 0;         // sort at every sort_every-th move (0: never)
   long long moves = 0;
   bool sorted = false;        // the arrays are in an order of their own
 };
@@ -136,6 +136,9 @@ extern "C" int cg_sim_create(cg_sim** out, int nc, int ngrid, float boxsize, dou
   if (e == cudaSuccess) e = cudaMalloc(&s->d_aos, 56 * (size_t)np_capacity);
   s->ps.id = s->id_alloc;
   s->ps.orig = s->orig_alloc;
+  // the sort pays only where the particles and meshes are far larger than
+  // L2: 256^3 particles gain 0.45 ms a step, 128^3 lose 0.1 ms
+  s->sort_every = np_capacity >= (1LL << 23) ? 2 : 0;
   if (const char* ev = getenv("COLAGPU_SORT_EVERY")) s->sort_every = atoi(ev) > 0 ? atoi(ev) : 0;
   if (e != cudaSuccess) {
     int rc = cuda_err(e, "cg_sim_create");
@@ -630,7 +633,7 @@ extern "C" int cg_net_forces(cg_net* h, cg_sim* coarse) {
   cudaStream_t st = coarse->st;   // stay on the realization's stream
   const float* x[3] = {coarse->ps.x[0], coarse->ps.x[1], coarse->ps.x[2]};
   CG_CHECK(cnet_features(&h->n, coarse->pm.dens, st), "features");
-  CG_CHECK(cnet_forward(&h->n, st), "forward");
+  CG_CHECK(cnet_forward(&h->n, st, false), "forward");
   CG_CHECK(cnet_apply(&h->n, x, coarse->ps.n, coarse->L, coarse->ps.f, st), "apply");
   return CG_OK;
 }

@@ -24,6 +24,7 @@ struct CNet {
   __nv_bfloat16* wb;           // bf16 weights used by the kernels, 3 x 27*16*16
   __nv_bfloat16* act[3];       // layer inputs: features, hidden 1, hidden 2 [v][16]
   float* out;                  // network output [v][16] (channels 0-2 used)
+  float4* out4;                // its channels 0-3 packed [v]: what the interpolation reads
   float* g0;                   // gradient buffers [v][16]
   float* g1;
   __nv_bfloat16* gb;           // bf16 copy of the gradient fed to the data-gradient conv
@@ -39,7 +40,9 @@ cudaError_t cnet_alloc(CNet* n, int N, unsigned long long seed);
 void cnet_free(CNet* n);
 cudaError_t cnet_sync_bf16(CNet* n, cudaStream_t st);
 cudaError_t cnet_features(CNet* n, const float* delta, cudaStream_t st);
-cudaError_t cnet_forward(CNet* n, cudaStream_t st);
+// full: also write the [v][16] output that the loss and the host API read
+// (the packed out4 is always written)
+cudaError_t cnet_forward(CNet* n, cudaStream_t st, bool full = true);
 cudaError_t cnet_loss_grad(CNet* n, double inv_msum, cudaStream_t st);
 cudaError_t cnet_backward(CNet* n, cudaStream_t st);
 cudaError_t cnet_adam(CNet* n, float lr, cudaStream_t st);
@@ -53,7 +56,7 @@ cudaError_t cnet_apply(const CNet* n, const float* const x[3], long long np, flo
 // is not a multiple of the 128-voxel tile.
 cudaError_t conv_tc_forward(const __nv_bfloat16* in, int N, const __nv_bfloat16* w,
                             const float* bias, int act, float* out_f, __nv_bfloat16* out_b,
-                            cudaStream_t st);
+                            float4* out4, cudaStream_t st);
 cudaError_t conv_tc_backward_data(const __nv_bfloat16* g, int N, const __nv_bfloat16* w,
                                   float* out_f, cudaStream_t st);
 // Device error word of the tensor-core kernels (bounded waits that gave up).

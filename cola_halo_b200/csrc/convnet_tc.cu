@@ -109,7 +109,7 @@ template <bool FLIP, int STAGES, int CPS>
 __global__ void __launch_bounds__(THREADS, CPS)
     k_conv_tc(const __nv_bfloat16* __restrict__ in, int N, const __nv_bfloat16* __restrict__ w,
               const float* __restrict__ bias, int act, float* __restrict__ out_f,
-              __nv_bfloat16* __restrict__ out_b) {
+              __nv_bfloat16* __restrict__ out_b, float4* __restrict__ out4) {
   extern __shared__ __align__(1024) uint8_t sm[];
   uint8_t* const stage0 = sm;
   uint8_t* const stage1 = sm + (STAGES - 1) * STAGE_BYTES;
@@ -228,6 +228,7 @@ __global__ void __launch_bounds__(THREADS, CPS)
         d[0] = *reinterpret_cast<const uint4*>(&hb[0]);
         d[1] = *reinterpret_cast<const uint4*>(&hb[8]);
       }
+      if (out4) out4[v] = make_float4(o[0], o[1], o[2], o[3]);
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
@@ -243,7 +244,7 @@ __global__ void __launch_bounds__(THREADS, CPS)
 
 template <bool FLIP, int STAGES, int CPS>
 cudaError_t launch_v(const __nv_bfloat16* in, int N, const __nv_bfloat16* w, const float* bias,
-                     int act, float* of, __nv_bfloat16* ob, cudaStream_t st) {
+                     int act, float* of, __nv_bfloat16* ob, float4* o4, cudaStream_t st) {
   static bool attr = false;
   if (!attr) {
     cudaError_t e = cudaFuncSetAttribute(k_conv_tc<FLIP, STAGES, CPS>,
@@ -259,7 +260,7 @@ cudaError_t launch_v(const __nv_bfloat16* in, int N, const __nv_bfloat16* w, con
   const int grid = ntiles < CPS * sms ? ntiles : CPS * sms;
   prof_mark(st, CG_ST_OTHER);
   k_conv_tc<FLIP, STAGES, CPS><<<grid, THREADS, smem_bytes(STAGES), st>>>(in, N, w, bias, act,
-                                                                         of, ob);
+                                                                         of, ob, o4);
   return cudaGetLastError();
 }
 
@@ -278,23 +279,23 @@ int conv_variant() {
 
 template <bool FLIP>
 cudaError_t launch(const __nv_bfloat16* in, int N, const __nv_bfloat16* w, const float* bias,
-                   int act, float* of, __nv_bfloat16* ob, cudaStream_t st) {
+                   int act, float* of, __nv_bfloat16* ob, float4* o4, cudaStream_t st) {
   if (N < TILE_M || N % TILE_M) return cudaErrorNotSupported;
-  if (conv_variant() == 1) return launch_v<FLIP, 1, 4>(in, N, w, bias, act, of, ob, st);
-  return launch_v<FLIP, 2, 2>(in, N, w, bias, act, of, ob, st);
+  if (conv_variant() == 1) return launch_v<FLIP, 1, 4>(in, N, w, bias, act, of, ob, o4, st);
+  return launch_v<FLIP, 2, 2>(in, N, w, bias, act, of, ob, o4, st);
 }
 
 }  // namespace
 
 cudaError_t conv_tc_forward(const __nv_bfloat16* in, int N, const __nv_bfloat16* w,
                             const float* bias, int act, float* out_f, __nv_bfloat16* out_b,
-                            cudaStream_t st) {
-  return launch<false>(in, N, w, bias, act, out_f, out_b, st);
+                            float4* out4, cudaStream_t st) {
+  return launch<false>(in, N, w, bias, act, out_f, out_b, out4, st);
 }
 
 cudaError_t conv_tc_backward_data(const __nv_bfloat16* g, int N, const __nv_bfloat16* w,
                                   float* out_f, cudaStream_t st) {
-  return launch<true>(g, N, w, nullptr, 0, out_f, nullptr, st);
+  return launch<true>(g, N, w, nullptr, 0, out_f, nullptr, nullptr, st);
 }
 
 unsigned conv_tc_error_word() {

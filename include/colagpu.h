@@ -80,8 +80,9 @@ long long cg_sim_np(cg_sim* s);
 /* move_particles2 on one GPU (move.c:34-41): periodic wrap of x, y, z. */
 int cg_sim_move(cg_sim* s);
 /* Cell order (no reference counterpart): every `every`-th cg_sim_move
- * (default 2; 0 = never; the environment variable COLAGPU_SORT_EVERY sets
- * the default) sorts the particles on the device by a grid of about eight
+ * (default 2 for simulations of at least 2^23 particles, else 0 = never;
+ * the environment variable COLAGPU_SORT_EVERY sets the default) sorts the
+ * particles on the device by a grid of about eight
  * particles per cell, so that the deposit and the interpolation keep the
  * memory locality of the initial lattice as structure forms.  Results are
  * unchanged up to the order of the deposit's float additions: every output

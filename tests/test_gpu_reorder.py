@@ -75,6 +75,7 @@ def test_copy_particles_keeps_the_order(gpu_lib, bbks_table):
     p = shuffled_lattice(nc, L, bbks_table, seed=8)
     a = Simulation(nc, 2 * nc, L, OM)
     b = Simulation(nc, 2 * nc, L, OM)
+    a.set_sort_interval(1)
     a.set_particles(p, 0.05, 0.05)
     a.move()
     _lib.check(gpu_lib.cg_sim_copy_particles(b.h, a.h), "cg_sim_copy_particles")
