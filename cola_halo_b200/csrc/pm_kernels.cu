@@ -150,6 +150,125 @@ __global__ void __launch_bounds__(T) k_deposit(const float* __restrict__ x0,
   }
 }
 
+// The same deposit for a chunk of CHUNK consecutive particles per CTA,
+// accumulated first in a shared-memory copy of the chunk's bounding box of
+// cells when that box is small.  In cell order (reorder.cu) the particles
+// of a halo sit next to each other, so a warp's eight CIC corners hit the
+// same few cells: global float atomics on one address serialise in L2,
+// shared-memory ones are cheap, and the box is then added to the mesh with
+// one atomic per touched cell.  The weights are deposit_one's products, so
+// only the order of the float additions changes.  Particles whose cloud
+// wraps in y or z, leaves the mesh in x, or has a buffer copy (x > x_right)
+// take the global path, as does every particle of a CTA whose box is large.
+constexpr int DEP_CHUNK = 512;                  // particles per CTA
+constexpr int DEP_VMAX = 3072;                   // cells: 12 KB of shared memory
+
+__device__ __forceinline__ void deposit_one_box(float* __restrict__ box, const Cic& c, int bx,
+                                                int by, int bz, int ny, int nz, float wpar) {
+  const float T2W = __fmul_rn(c.t2, wpar);
+  const float D2W = __fmul_rn(c.d2, wpar);
+  const int i0 = c.i0 - bx, j0 = c.j0 - by, k0 = c.k0 - bz;
+  float* r00 = box + ((i0 * ny) + j0) * nz + k0;          // (i0, j0)
+  float* r01 = r00 + nz;                                   // (i0, j1)
+  float* r10 = r00 + ny * nz;                              // (i1, j0)
+  float* r11 = r10 + nz;                                   // (i1, j1)
+  atomicAdd(r00, __fmul_rn(__fmul_rn(c.t3, c.t1), T2W));
+  atomicAdd(r00 + 1, __fmul_rn(__fmul_rn(c.d3, c.t1), T2W));
+  atomicAdd(r01, __fmul_rn(__fmul_rn(c.t3, c.t1), D2W));
+  atomicAdd(r01 + 1, __fmul_rn(__fmul_rn(c.d3, c.t1), D2W));
+  atomicAdd(r10, __fmul_rn(__fmul_rn(c.t3, c.d1), T2W));
+  atomicAdd(r10 + 1, __fmul_rn(__fmul_rn(c.d3, c.d1), T2W));
+  atomicAdd(r11, __fmul_rn(__fmul_rn(c.t3, c.d1), D2W));
+  atomicAdd(r11 + 1, __fmul_rn(__fmul_rn(c.d3, c.d1), D2W));
+}
+
+__device__ __forceinline__ bool box_eligible(const Cic& c, float px, float x_right, int N) {
+  return c.ok && !(px > x_right) && c.i0 >= 0 && c.i1 < N && c.j1 == c.j0 + 1 &&
+         c.k1 == c.k0 + 1;
+}
+
+template <int CHUNK, int VMAX>
+__global__ void __launch_bounds__(T) k_deposit_box(const float* __restrict__ x0,
+                                                   const float* __restrict__ x1,
+                                                   const float* __restrict__ x2, long long n,
+                                                   float* __restrict__ dens, int N, float scale,
+                                                   float wpar, float x_right, float shiftx,
+                                                   unsigned* __restrict__ err) {
+  __shared__ float box[VMAX];
+  __shared__ int red[6][T / 32];
+  const long long base = (long long)blockIdx.x * CHUNK;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  // bounding box of the eligible clouds' lower corners
+  int lo[3] = {0x7fffffff, 0x7fffffff, 0x7fffffff};
+  int hi[3] = {-1, -1, -1};
+  for (int q = 0; q < CHUNK / T; q++) {
+    const long long i = base + q * T + tid;
+    if (i >= n) break;
+    const float px = x0[i];
+    const Cic c = cic_index(px, x1[i], x2[i], N, scale);
+    if (!box_eligible(c, px, x_right, N)) continue;
+    lo[0] = min(lo[0], c.i0); hi[0] = max(hi[0], c.i0);
+    lo[1] = min(lo[1], c.j0); hi[1] = max(hi[1], c.j0);
+    lo[2] = min(lo[2], c.k0); hi[2] = max(hi[2], c.k0);
+  }
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    for (int o = 16; o > 0; o >>= 1) {
+      lo[a] = min(lo[a], __shfl_xor_sync(0xffffffffu, lo[a], o));
+      hi[a] = max(hi[a], __shfl_xor_sync(0xffffffffu, hi[a], o));
+    }
+    if (lane == 0) {
+      red[a][warp] = lo[a];
+      red[3 + a][warp] = hi[a];
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    lo[a] = red[a][0];
+    hi[a] = red[3 + a][0];
+    for (int w = 1; w < T / 32; w++) {
+      lo[a] = min(lo[a], red[a][w]);
+      hi[a] = max(hi[a], red[3 + a][w]);
+    }
+  }
+  // cells lo .. hi + 1 per axis
+  const long long nx = (long long)hi[0] - lo[0] + 2, ny = (long long)hi[1] - lo[1] + 2,
+                  nz = (long long)hi[2] - lo[2] + 2;
+  const bool use_box = hi[0] >= 0 && nx * ny * nz <= VMAX;
+  const int vol = use_box ? (int)(nx * ny * nz) : 0;
+  for (int v = tid; v < vol; v += T) box[v] = 0.0f;
+  __syncthreads();
+  for (int q = 0; q < CHUNK / T; q++) {
+    const long long i = base + q * T + tid;
+    if (i >= n) break;
+    const float px = x0[i], py = x1[i], pz = x2[i];
+    const Cic c = cic_index(px, py, pz, N, scale);
+    if (!c.ok) {
+      atomicOr(err, isfinite(px) && isfinite(py) && isfinite(pz) ? CG_ERR_BAD_CELL
+                                                                  : CG_ERR_NONFINITE);
+      continue;
+    }
+    if (use_box && box_eligible(c, px, x_right, N)) {
+      deposit_one_box(box, c, lo[0], lo[1], lo[2], (int)ny, (int)nz, wpar);
+      continue;
+    }
+    deposit_one(dens, c, N, wpar);
+    if (px > x_right) {
+      Cic g = cic_index(__fadd_rn(px, shiftx), py, pz, N, scale);
+      if (g.ok) deposit_one(dens, g, N, wpar);
+    }
+  }
+  __syncthreads();
+  for (int v = tid; v < vol; v += T) {
+    const float w = box[v];
+    if (w == 0.0f) continue;
+    const int kk = v % (int)nz, jj = (v / (int)nz) % (int)ny, ii = v / (int)(ny * nz);
+    const int gi = lo[0] + ii, gj = lo[1] + jj, gk = lo[2] + kk;
+    if (gi < N && gj < N && gk < N) atomicAdd(dens + cell(gi, gj, gk, N), w);
+  }
+}
+
 // force_at_particle_locations (pm.c:370-411) for all three axes, plus the
 // buffer copy's force added back as in add_buffer_forces (pm.c:526-531).
 __device__ __forceinline__ float gather4(const float* __restrict__ m, int i, const Cic& c,
@@ -857,8 +976,24 @@ cudaError_t pm_deposit(PmPlan* p, const float* const x[3], long long n, cudaStre
   k_fill<<<grid_for((long long)n4), T, 0, st>>>(reinterpret_cast<float4*>(p->dens), n4, -1.0f);
   if (n > 0) {
     prof_mark(st, CG_ST_DEPOSIT);
-    k_deposit<<<grid_for(n), T, 0, st>>>(x[0], x[1], x[2], n, p->dens, p->N, p->scale,
-                                         p->wpar, p->x_right, p->shiftx, p->err);
+    static const bool plain = getenv("COLAGPU_DEPOSIT") && getenv("COLAGPU_DEPOSIT")[0] == 'p';
+    if (plain)
+      k_deposit<<<grid_for(n), T, 0, st>>>(x[0], x[1], x[2], n, p->dens, p->N, p->scale,
+                                           p->wpar, p->x_right, p->shiftx, p->err);
+    else {
+      static const int chunk = getenv("COLAGPU_DEPOSIT_CHUNK") ? atoi(getenv("COLAGPU_DEPOSIT_CHUNK"))
+                                                               : DEP_CHUNK;
+      if (chunk == 256)
+        k_deposit_box<256, 3072><<<(unsigned)((n + 255) / 256), T, 0, st>>>(
+            x[0], x[1], x[2], n, p->dens, p->N, p->scale, p->wpar, p->x_right, p->shiftx, p->err);
+      else if (chunk == 1024)
+        k_deposit_box<1024, 6144><<<(unsigned)((n + 1023) / 1024), T, 0, st>>>(
+            x[0], x[1], x[2], n, p->dens, p->N, p->scale, p->wpar, p->x_right, p->shiftx, p->err);
+      else
+        k_deposit_box<DEP_CHUNK, DEP_VMAX><<<(unsigned)((n + DEP_CHUNK - 1) / DEP_CHUNK), T, 0,
+                                            st>>>(x[0], x[1], x[2], n, p->dens, p->N, p->scale,
+                                                  p->wpar, p->x_right, p->shiftx, p->err);
+    }
   }
   return cudaGetLastError();
 }
