@@ -449,7 +449,8 @@ __global__ void __launch_bounds__(T) k_fx(const float2* in, float2* out,
 //   I0, J0 signed with the Nyquist index kept at +N/2, F(0,0,0) = 0.
 // GreenLoad applies the factor while the first inverse stage loads the
 // forward-transformed tile: MODE 0 the y component (n_y = J0, the position
-// along the line), MODE 1 the factor without n_a.
+// along the line), MODE 1 the factor without n_a, MODE 2 the y component
+// while it writes the MODE 1 value back in place.
 template <int P, int MODE>
 struct GreenLoad {
   cplx* s;
@@ -461,9 +462,18 @@ struct GreenLoad {
     const int I0 = kx <= N / 2 ? kx : kx - N;
     const int J0 = n <= N / 2 ? n : n - N;
     const int den = kz * kz + I0 * I0 + J0 * J0;
-    if (den == 0) return cplx{0.0f, 0.0f};
+    if (den == 0) {
+      if (MODE == 2) s[b * P + n + (n >> 4)] = cplx{0.0f, 0.0f};
+      return cplx{0.0f, 0.0f};
+    }
     float f2 = __fdiv_rn(f1, (float)den);
-    if (MODE == 0) f2 = __fmul_rn(f2, (float)J0);
+    if (MODE == 2) {
+      // the shared x/z value replaces the loaded one in place (this thread
+      // is the element's only reader in this stage), so the second inverse
+      // transform reads it plainly instead of dividing again
+      s[b * P + n + (n >> 4)] = cplx{-__fmul_rn(f2, p.y), __fmul_rn(f2, p.x)};
+    }
+    if (MODE != 1) f2 = __fmul_rn(f2, (float)J0);
     return cplx{-__fmul_rn(f2, p.y), __fmul_rn(f2, p.x)};
   }
   static constexpr bool kShared = true;
@@ -502,13 +512,13 @@ __global__ void __launch_bounds__(T, MINB) k_green(const float2* __restrict__ sp
   const Gmem gin{const_cast<float2*>(spec) + off, (size_t)N, 1};
   const SmemLine<P> d{D}, w{W};
   fft_tile_y<N, BG, RMG, -1>(gin, d, d, twN);
-  const GreenLoad<P, 0> gy{D, kz, kx0, N, f1};
+  // the y component's load also leaves the shared x/z value in D
+  const GreenLoad<P, 2> gy{D, kz, kx0, N, f1};
   const Gmem oy{g1 + off, (size_t)N, 1};
   fft_tile_y<N, BG, RMG, 1>(gy, w, oy, twN);
   __syncthreads();
-  const GreenLoad<P, 1> gs{D, kz, kx0, N, f1};
   const Gmem os{g2 + off, (size_t)N, 1};
-  fft_tile_y<N, BG, RMG, 1>(gs, d, os, twN);
+  fft_tile_y<N, BG, RMG, 1>(d, d, os, twN);
 }
 
 // ZI: c2r along z of S (lines (x, y0..y0+TY-1) per CTA) into R.  The
