@@ -28,7 +28,7 @@ L, NC, SEED = 64.0, 32, 100
 PARAM = """nc = {nc}
 boxsize = {L}
 random_seed= {seed}
-nrealization= 1
+nrealization= {nreal}
 ntimestep= 10
 a_final= 1.0
 output_redshifts= {{1.0, 0.0}}
@@ -49,11 +49,11 @@ write_longid= {longid}
 """
 
 
-def run_driver(exe, workdir, longid="false"):
+def run_driver(exe, workdir, longid="false", nreal=1):
     os.makedirs(workdir, exist_ok=True)
     param = os.path.join(workdir, "param.txt")
     with open(param, "w") as f:
-        f.write(PARAM.format(nc=NC, L=L, seed=SEED, longid=longid,
+        f.write(PARAM.format(nc=NC, L=L, seed=SEED, longid=longid, nreal=nreal,
                              table=os.path.join(HERE, "golden", "bbks_table.dat")))
     r = subprocess.run([exe, param], cwd=workdir, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, "%s failed (%d):\n%s\n%s" % (exe, r.returncode, r.stdout[-2000:],
@@ -137,3 +137,29 @@ def test_driver_halo_catalogues_match(gpu_lib, outputs):
             j = int(np.argmin(d))
             assert d[j] <= 2e-3 * L
             assert abs(rg[j, 0] - h[0]) <= max(2, 0.02 * h[0])
+
+
+def test_driver_two_realizations_with_long_ids(gpu_lib, outputs, tmp_path):
+    """Two realizations in one process (seeds 100 and 101: the drop-in
+    state is reused, the particles re-uploaded and the snapshot residency
+    renewed) and 8-byte GADGET ids."""
+    cpu = os.path.join(REF_DIR, "cola_halo_cpu")
+    gpu = os.path.join(REF_DIR, "cola_halo_gpu")
+    run_driver(cpu, str(tmp_path / "cpu"), longid="true", nreal=2)
+    run_driver(gpu, str(tmp_path / "gpu"), longid="true", nreal=2)
+    for seed in (SEED, SEED + 1):
+        name = "snp%05db.0" % seed
+        hc, pc, vc, ic = read_gadget(str(tmp_path / "cpu" / name))
+        hg, pg, vg, ig = read_gadget(str(tmp_path / "gpu" / name))
+        assert hc.tobytes() == hg.tobytes()
+        assert ic.dtype == np.uint64 and ig.dtype == np.uint64
+        oc, og = np.argsort(ic, kind="stable"), np.argsort(ig, kind="stable")
+        np.testing.assert_array_equal(ig[og], ic[oc])
+        assert periodic_absdiff(pg[og], pc[oc]).max() <= 1e-5 * L
+        rc = np.loadtxt(str(tmp_path / "cpu" / ("fof%05db.txt" % seed)), ndmin=2)
+        rg = np.loadtxt(str(tmp_path / "gpu" / ("fof%05db.txt" % seed)), ndmin=2)
+        assert abs(len(rg) - len(rc)) <= max(2, len(rc) // 50)
+    # the two seeds differ
+    _, p0, _, i0 = read_gadget(str(tmp_path / "gpu" / ("snp%05db.0" % SEED)))
+    _, p1, _, i1 = read_gadget(str(tmp_path / "gpu" / ("snp%05db.0" % (SEED + 1))))
+    assert not np.array_equal(p0[np.argsort(i0)], p1[np.argsort(i1)])
