@@ -101,3 +101,23 @@ def test_coarse_grid_restatement_matches_golden_fixture():
     got, total = R.coarse_grid(s["snap_x"], L, nc)
     np.testing.assert_array_equal(got, g["delta"])
     assert abs(total - n) < 1e-3 * n
+
+
+def test_grid_file_reader_reads_the_reference_file(ref, tmp_path):
+    """cola_halo_b200.coarse.read_grid_file on a file the reference's own
+    coarse_grid2 wrote, and its rejection of a truncated file."""
+    from oracle import ref as REF
+    from cola_halo_b200.coarse import read_grid_file
+    L = 80.0
+    x = np.random.default_rng(9).uniform(0, L, (5000, 3)).astype(np.float32)
+    path = str(tmp_path / "g.bin")
+    _, want = REF.coarse_grid_file(pmin_of(x), L, 12, path)
+    Lf, got = read_grid_file(path)
+    assert Lf == np.float32(L)
+    np.testing.assert_array_equal(got, want)
+    raw = open(path, "rb").read()
+    bad = str(tmp_path / "bad.bin")
+    open(bad, "wb").write(raw[:-4])
+    import pytest
+    with pytest.raises(ValueError):
+        read_grid_file(bad)
