@@ -39,3 +39,31 @@ def test_roundtrip(gpu_lib):
     x = rng.standard_normal((n, n, n)).astype(np.float32)
     back = fft_c2r(fft_r2c(x)) / n ** 3
     assert np.abs(back - x).max() < 1e-5
+
+
+@pytest.mark.parametrize("n", [384, 768])
+def test_r2c_c2r_match_cufft_at_workload_sizes(gpu_lib, n):
+    """The mesh transforms of the 128^3 and 256^3 workloads against cuFFT
+    (torch.fft, float32, the same unnormalised conventions): both float32
+    FFTs agree to float rounding, ~1e-6 of the spectrum's largest mode."""
+    import torch
+    from cola_halo_b200 import fft_c2r, fft_r2c
+    rng = np.random.default_rng(n)
+    x = rng.standard_normal((n, n, n), dtype=np.float32)
+    got = fft_r2c(x)
+    xd = torch.from_numpy(x).cuda()
+    want = torch.fft.rfftn(xd).cpu().numpy()
+    del xd
+    scale = np.abs(want).max()
+    err = np.abs(got - want)
+    assert err.max() / scale < 1e-5, err.max() / scale
+    assert np.sqrt(np.mean(err.astype(np.float64) ** 2)) / scale < 1e-6
+    back = fft_c2r(got)
+    sd = torch.from_numpy(got).cuda()
+    want_back = torch.fft.irfftn(sd, s=(n, n, n)).cpu().numpy() * float(n) ** 3
+    del sd
+    torch.cuda.empty_cache()
+    scale_b = np.abs(want_back).max()
+    err_b = np.abs(back - want_back)
+    assert err_b.max() / scale_b < 1e-5, err_b.max() / scale_b
+    np.testing.assert_allclose(back / float(n) ** 3, x, rtol=0, atol=1e-4)
