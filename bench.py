@@ -818,8 +818,10 @@ def run_learned(args):
     sched = Schedule.linear(0.02, 1.0, 10)
     table = write_bbks_table(os.path.join(tempfile.mkdtemp(), "bbks.dat"))
     net = ConvNet(nc, seed=7)
+    net2 = ConvNet(nc, seed=8)
     res = evaluate(nc, L, sched, net, list(range(1, args.train_seeds + 1)),
                    list(range(1001, 1001 + args.eval_seeds)), table, epochs=args.epochs,
+                   filter_nk=16, net2=net2,
                    log=lambda s: print(s, file=sys.stderr, flush=True))
     seeds = res["seeds"]
     fine_s = float(np.mean([r["fine_s"] for r in seeds]))
@@ -854,7 +856,27 @@ def run_learned(args):
                                             "summed over the evaluation seeds"},
            "train_s": res["train_s"], "train_steps": res["train_steps"],
            "loss_first": res["loss_first"], "loss_last": res["loss_last"]}
+    # the Fourier-space correction: per-step transfer functions T_s(|n|) of
+    # the coarse force (16 knots, least squares on 4 training seeds), alone
+    # and with a second net trained on the filtered force
+    for name in ("filtered", "filtered_net"):
+        if "err_" + name in seeds[0]:
+            t = float(np.mean([r[name + "_s"] for r in seeds]))
+            out[name] = {"s": t, "speedup_vs_plain_fine": fine_s / t,
+                         "wall_s": float(np.mean([r[name + "_wall_s"] for r in seeds])),
+                         "pk_err": float(np.mean([r["err_" + name] for r in seeds])),
+                         "pk_err_max": float(np.max([r["err_" + name] for r in seeds])),
+                         "mf_ratio_err": res.get("mf_err_" + name),
+                         "mf": res.get("mf_" + name)}
+    if "filters" in res:
+        out["filter"] = {"knots": 16, "fit_seeds": 4, "fit_s": res["filter_fit_s"],
+                         "T_first_last_step": [[round(v, 4) for v in res["filters"][0]],
+                                               [round(v, 4) for v in res["filters"][-1]]]}
+    if "train2_s" in res:
+        out["filtered_net"]["train_s"] = res["train2_s"]
+        out["filtered_net"]["loss_last"] = res["loss2_last"]
     print(json.dumps(out))
+    net2.close()
     return 0
 
 

@@ -260,6 +260,20 @@ extern "C" int cg_sim_move(cg_sim* s) {
   return CG_OK;
 }
 
+extern "C" int cg_sim_set_force_filters(cg_sim* s, const float* knots, int n, int nsets) {
+  if (!s || n < 0 || nsets < 0 || ((long long)n * nsets > 0 && !knots) || n == 1)
+    return set_err(CG_EINVAL, "cg_sim_set_force_filters: bad arguments");
+  CG_CHECK(cudaStreamSynchronize(s->st), "sync");    // no queued Green step reads the old table
+  CG_CHECK(pm_set_filters(&s->pm, knots, n, nsets), "force filters");
+  return CG_OK;
+}
+
+extern "C" int cg_sim_use_force_filter(cg_sim* s, int set) {
+  if (!s || !pm_use_filter(&s->pm, set))
+    return set_err(CG_EINVAL, "cg_sim_use_force_filter: no such filter");
+  return CG_OK;
+}
+
 extern "C" int cg_sim_set_sort_interval(cg_sim* s, int every) {
   if (!s || every < 0) return set_err(CG_EINVAL, "cg_sim_set_sort_interval: bad arguments");
   s->sort_every = every;

@@ -47,6 +47,12 @@ struct PmPlan {
   unsigned* err;            // device: error word
   size_t mesh_bytes;        // bytes of one real mesh
   size_t spec_bytes;        // bytes of one half spectrum
+  float* kfilt;             // device: force transfer functions, kfilt_sets x kfilt_n knots
+  size_t kfilt_cap;         //   floats allocated
+  int kfilt_n;              //   knots per function
+  int kfilt_sets;           //   functions held
+  int kfilt_cur;            //   the one the Green step applies; -1 = none
+  float kfilt_inv_dn;       //   knots per unit of |n|
 };
 
 // Plain 3-D real transforms on the mesh layouts above (unnormalised, FFTW
@@ -85,6 +91,13 @@ void pm_set_schedule(int N, MeshSched s);
 cudaError_t pm_autotune(PmPlan* p, cudaStream_t st, MeshSched* best, float* ms_green,
                         float* ms_fx);
 cudaError_t pm_plan_alloc(PmPlan* p, int N, int factor, float L);
+// Force transfer functions T(|n|) for the Green step: nsets functions of n
+// knots each at |n| = j (sqrt(3) N / 2) / (n - 1), copied from a host array
+// (synchronous); set 0 becomes current.  n = 0 removes them.
+cudaError_t pm_set_filters(PmPlan* p, const float* knots, int n, int nsets);
+// Make set `set` current (-1: none, the reference's force).  False when the
+// plan holds no such set.
+bool pm_use_filter(PmPlan* p, int set);
 void pm_plan_free(PmPlan* p);
 // Full PM force: deposit -> r2c -> Green/gradient -> 3 c2r -> interpolation.
 // Positions and forces are SoA device arrays of n floats per component.

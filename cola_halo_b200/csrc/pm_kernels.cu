@@ -27,6 +27,7 @@
 #include <string.h>
 
 #include <map>
+#include <vector>
 #include <mutex>
 
 #include "fft_core.cuh"
@@ -443,6 +444,24 @@ __global__ void __launch_bounds__(T) k_fx(const float2* in, float2* out,
   }
 }
 
+// Optional isotropic transfer function of the force, T(|n|) (|n| in units
+// of the fundamental), sampled at knots |n| = j / inv_dn, j < n, and
+// interpolated linearly (T = last knot beyond the table): the Fourier-space
+// form of the learned force correction.  t == NULL: no filter, the
+// reference's force unchanged.
+struct KFilter {
+  const float* t;
+  int n;
+  float inv_dn;
+  __device__ __forceinline__ float at(int den) const {
+    const float r = __fmul_rn(sqrtf((float)den), inv_dn);
+    const int i = (int)r;
+    if (i >= n - 1) return t[n - 1];
+    const float a = t[i], b = t[i + 1];
+    return __fadd_rn(a, __fmul_rn(__fsub_rn(r, (float)i), __fsub_rn(b, a)));
+  }
+};
+
 // compute_force_mesh (pm.c:304-346) on lines (kz, kx) that are already
 // transformed along z and x:  F_a = i f2 delta_k,
 //   f2 = f1 / (K^2 + I0^2 + J0^2) * n_a,  f1 = -1/(N^3 2 pi/L),
@@ -456,6 +475,7 @@ struct GreenLoad {
   cplx* s;
   int kz, kx0, N;
   float f1;
+  KFilter kf;
   __device__ __forceinline__ cplx ld(int b, int n) const {
     const cplx p = s[b * P + n + (n >> 4)];
     const int kx = kx0 + b;
@@ -467,6 +487,7 @@ struct GreenLoad {
       return cplx{0.0f, 0.0f};
     }
     float f2 = __fdiv_rn(f1, (float)den);
+    if (kf.t) f2 = __fmul_rn(f2, kf.at(den));
     if (MODE == 2) {
       // the shared x/z value replaces the loaded one in place (this thread
       // is the element's only reader in this stage), so the second inverse
@@ -500,7 +521,7 @@ __global__ void __launch_bounds__(T, MINB) k_green(const float2* __restrict__ sp
                                                          float2* __restrict__ g1,
                                                          float2* __restrict__ g2,
                                                          const float2* __restrict__ twN,
-                                                         float f1) {
+                                                         float f1, KFilter kf) {
   constexpr int P = cgfft::line_pitch<N>();
   extern __shared__ __align__(16) unsigned char smraw[];
   cplx* D = reinterpret_cast<cplx*>(smraw);
@@ -513,7 +534,7 @@ __global__ void __launch_bounds__(T, MINB) k_green(const float2* __restrict__ sp
   const SmemLine<P> d{D}, w{W};
   fft_tile_y<N, BG, RMG, -1>(gin, d, d, twN);
   // the y component's load also leaves the shared x/z value in D
-  const GreenLoad<P, 2> gy{D, kz, kx0, N, f1};
+  const GreenLoad<P, 2> gy{D, kz, kx0, N, f1, kf};
   const Gmem oy{g1 + off, (size_t)N, 1};
   fft_tile_y<N, BG, RMG, 1>(gy, w, oy, twN);
   __syncthreads();
@@ -629,7 +650,7 @@ struct MeshKernels {
   void (*fxi)(const float2*, float2*, const float2*);
   void (*fxi_x)(const float2*, float2*, const float2*);   // inverse, input times n_x
   void (*fxi_z)(const float2*, float2*, const float2*);   // inverse, input times n_z
-  void (*green)(const float2*, float2*, float2*, const float2*, float);
+  void (*green)(const float2*, float2*, float2*, const float2*, float, KFilter);
   void (*zi)(const float2*, float*, const float2*, const float2*);
   size_t sm_fz, sm_fy, sm_fx, sm_green, sm_zi;
   int tk;    // ky columns per CTA of the x pass
@@ -822,7 +843,7 @@ cudaError_t pm_autotune(PmPlan* p, cudaStream_t st, MeshSched* best, float* ms_g
     e = best_time(st, kReps, [&] {
       prof_mark(st, CG_ST_OTHER);
       k.green<<<(N / 2 + 1) * N / k.byg, T, k.sm_green, st>>>(p->spec, p->gsp[1], p->gsp[2],
-                                                               p->twN, p->f1);
+                                                               p->twN, p->f1, KFilter{});
     }, &t);
     if (ms_green) ms_green[v] = t;
     if (e == cudaSuccess && t < tbest) {
@@ -851,6 +872,7 @@ cudaError_t pm_autotune(PmPlan* p, cudaStream_t st, MeshSched* best, float* ms_g
 
 cudaError_t pm_plan_alloc(PmPlan* p, int N, int factor, float L) {
   memset(p, 0, sizeof(*p));
+  p->kfilt_cur = -1;
   MeshKernels k;
   if (!get_kernels(N, &k)) return cudaErrorInvalidValue;
   p->N = N;
@@ -953,7 +975,39 @@ cudaError_t mesh_c2r(const MeshFFT* f, float2* spec, float* real, cudaStream_t s
   return cudaGetLastError();
 }
 
+cudaError_t pm_set_filters(PmPlan* p, const float* knots, int n, int nsets) {
+  p->kfilt_cur = -1;
+  if (n <= 1 || nsets <= 0 || !knots) {
+    p->kfilt_n = p->kfilt_sets = 0;
+    return cudaSuccess;
+  }
+  const size_t need = (size_t)n * nsets;
+  if (need > p->kfilt_cap) {
+    cudaFree(p->kfilt);
+    p->kfilt = nullptr;
+    p->kfilt_cap = 0;
+    cudaError_t e = cudaMalloc(&p->kfilt, sizeof(float) * need);
+    if (e != cudaSuccess) return e;
+    p->kfilt_cap = need;
+  }
+  // a plain (synchronous) copy: done once, before the run that uses it
+  cudaError_t e = cudaMemcpy(p->kfilt, knots, sizeof(float) * need, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return e;
+  p->kfilt_n = n;
+  p->kfilt_sets = nsets;
+  p->kfilt_cur = 0;
+  p->kfilt_inv_dn = (float)((n - 1) / (sqrt(3.0) * p->N / 2.0));
+  return cudaSuccess;
+}
+
+bool pm_use_filter(PmPlan* p, int set) {
+  if (set >= p->kfilt_sets) return false;
+  p->kfilt_cur = set < 0 ? -1 : set;
+  return true;
+}
+
 void pm_plan_free(PmPlan* p) {
+  cudaFree(p->kfilt);
   cudaFree(p->dens);
   cudaFree(p->spec);
   for (int a = 0; a < 3; a++) {
@@ -1026,8 +1080,10 @@ cudaError_t pm_green_c2r(PmPlan* p, cudaStream_t st) {
   const int N = p->N;
   // gsp[1] <- y component, gsp[2] <- the shared x/z spectrum
   prof_mark(st, CG_ST_GREEN);
+  const KFilter kf{p->kfilt_cur >= 0 ? p->kfilt + (size_t)p->kfilt_cur * p->kfilt_n : nullptr,
+                   p->kfilt_n, p->kfilt_inv_dn};
   k.green<<<(N / 2 + 1) * N / k.byg, T, k.sm_green, st>>>(p->spec, p->gsp[1], p->gsp[2],
-                                                           p->twN, p->f1);
+                                                           p->twN, p->f1, kf);
   const dim3 gx(N / k.tk, N / 2 + 1), gz(N / TY, N);
   // x: n_x * gsp[2] -> gsp[0] (gsp[2] is still needed for z)
   prof_mark(st, CG_ST_FX_INV);

@@ -98,12 +98,17 @@ def _lpt_particles(nc, boxsize, seed, omega_m, a_init, table):
 
 
 def train_online(net, coarse, fine, sched, seeds, table, *, lr=2e-3, epochs=1,
-                 steps_per_state=1, omega_m=0.273, log=None):
+                 steps_per_state=1, omega_m=0.273, filters=None, log=None):
     """Train on PM-generated pairs along fine-mesh trajectories: for each
     seed and each time step, copy the fine run's particles to the coarse
     realization and take `steps_per_state` optimiser steps on
-    (coarse features, fine - coarse force).  Returns the loss history."""
+    (coarse features, fine - coarse force).  With `filters` (fitted by
+    fit_force_filter) the coarse force is the filtered one of each step, so
+    the net learns what the transfer function leaves.  Returns the loss
+    history."""
     hist = []
+    if filters is not None:
+        coarse.set_force_filters(filters)
     for ep in range(epochs):
         for seed in seeds:
             p = _lpt_particles(fine.nc, fine.boxsize, seed, omega_m, sched.a_init, table)
@@ -112,6 +117,8 @@ def train_online(net, coarse, fine, sched, seeds, table, *, lr=2e-3, epochs=1,
                 _, _, avel1, apos1 = sched.times(i)
                 fine.move()
                 copy_particles(coarse, fine)
+                if filters is not None:
+                    coarse.use_force_filter(min(i - 1, len(filters) - 1))
                 for _ in range(steps_per_state):
                     hist.append(net.train_step(coarse, fine, lr))
                 # train_step left the fine forces of these positions in `fine`
@@ -120,6 +127,74 @@ def train_online(net, coarse, fine, sched, seeds, table, *, lr=2e-3, epochs=1,
             if log:
                 log("epoch %d seed %d loss %.4g" % (ep, seed, hist[-1]))
     return hist
+
+
+def fit_force_filter(coarse, fine, sched, seeds, table, *, nk=16, sample=1 << 18,
+                     ridge=1e-3, omega_m=0.273, log=None):
+    """Fourier-space learned correction: per force evaluation s of the time
+    loop, the isotropic transfer function T_s(|n|) of the coarse mesh's
+    force that best reproduces the fine mesh's force on the same particles,
+    by linear least squares along fine-mesh trajectories.
+
+    The coarse force is linear in the knots (the Green step multiplies the
+    spectrum by T, every later stage is linear), so with the hat basis e_j
+    (one knot 1, the others 0) F(T) = sum_j T_j F(e_j), and T_s solves
+    (A_s + lam I) T = b_s + lam 1 with A_jk = <F(e_j), F(e_k)>,
+    b_j = <F(e_j), F_fine> summed over a fixed random sample of particles,
+    their three components and the seeds; lam = ridge tr(A_s) / nk pulls
+    poorly constrained knots toward T = 1 (the reference's force).
+    Returns an (nloop - 1, nk) float32 array of knots; the coarse
+    realization's filters are removed again."""
+    nst = sched.nloop - 1
+    A = np.zeros((nst, nk, nk))
+    b = np.zeros((nst, nk))
+    npart = fine.nc ** 3
+    sub = np.sort(np.random.default_rng(0).choice(npart, size=min(sample, npart),
+                                                  replace=False))
+    coarse.set_force_filters(np.eye(nk, dtype=np.float32))
+    G = np.empty((nk, 3 * len(sub)))
+    for seed in seeds:
+        p = _lpt_particles(fine.nc, fine.boxsize, seed, omega_m, sched.a_init, table)
+        fine.set_particles(p, sched.a_init, sched.a_init)
+        for i in range(1, sched.nloop):
+            _, _, avel1, apos1 = sched.times(i)
+            fine.move()
+            copy_particles(coarse, fine)
+            fine.forces()
+            ff = fine.get_forces()[sub].astype(np.float64).ravel()
+            for j in range(nk):
+                coarse.use_force_filter(j)
+                coarse.forces()
+                G[j] = coarse.get_forces()[sub].ravel()
+            A[i - 1] += G @ G.T
+            b[i - 1] += G @ ff
+            fine.kick(avel1)
+            fine.drift(apos1)
+        if log:
+            log("filter fit: seed %d" % seed)
+    coarse.set_force_filters(None)
+    T = np.empty((nst, nk))
+    for s in range(nst):
+        lam = ridge * np.trace(A[s]) / nk
+        T[s] = np.linalg.solve(A[s] + lam * np.eye(nk), b[s] + lam)
+    return T.astype(np.float32)
+
+
+def filtered_force(sim, filters, net=None):
+    """A force callback for run_time_loop that applies filters[s] at the
+    s-th force evaluation (the last one beyond the table), plus the conv
+    net's correction when `net` is given.  Loads the filters once."""
+    sim.set_force_filters(filters)
+    count = [0]
+
+    def force():
+        sim.use_force_filter(min(count[0], len(filters) - 1))
+        count[0] += 1
+        if net is None:
+            sim.forces()
+        else:
+            net.forces(sim)
+    return force
 
 
 def power_spectrum_on(sim_pk, snap_x, a):
@@ -163,11 +238,16 @@ def pk_error(k, p, p_ref, kmax):
 
 
 def evaluate(nc, boxsize, sched, net, train_seeds, eval_seeds, table, *, omega_m=0.273,
-             epochs=1, lr=2e-3, log=None):
+             epochs=1, lr=2e-3, filter_nk=16, filter_seeds=4, net2=None, log=None):
     """Train on PM pairs, then judge plain-coarse and learned-coarse runs
     against the plain factor-3 run on held-out seeds: P(k) error up to half
     the particle Nyquist wavenumber, and the device time of each run's time
-    loop (with the host wall time beside it)."""
+    loop (with the host wall time beside it).
+
+    filter_nk > 0 also fits per-step force transfer functions of filter_nk
+    knots on the first `filter_seeds` training seeds (fit_force_filter) and
+    judges the filtered coarse run; `net2`, when given, is trained on the
+    filtered coarse force and judged as filter + net."""
     import time
 
     from .sim import Simulation
@@ -180,6 +260,20 @@ def evaluate(nc, boxsize, sched, net, train_seeds, eval_seeds, table, *, omega_m
     kmax = 0.5 * np.pi * nc / boxsize
     res = {"train_s": train_s, "train_steps": len(hist), "loss_first": float(np.mean(hist[:10])),
            "loss_last": float(np.mean(hist[-10:])), "seeds": []}
+    filters = None
+    if filter_nk > 0:
+        t0 = time.perf_counter()
+        filters = fit_force_filter(coarse, fine, sched, train_seeds[:filter_seeds], table,
+                                   nk=filter_nk, omega_m=omega_m, log=log)
+        res["filter_fit_s"] = time.perf_counter() - t0
+        res["filters"] = filters.tolist()
+        if net2 is not None:
+            t0 = time.perf_counter()
+            h2 = train_online(net2, coarse, fine, sched, train_seeds, table, lr=lr,
+                              epochs=epochs, omega_m=omega_m, filters=filters, log=log)
+            res["train2_s"] = time.perf_counter() - t0
+            res["loss2_last"] = float(np.mean(h2[-10:]))
+            coarse.set_force_filters(None)
 
     lib = _lib.load()
     nst = _lib.NSTAGES
@@ -222,14 +316,29 @@ def evaluate(nc, boxsize, sched, net, train_seeds, eval_seeds, table, *, omega_m
              "err_coarse": pk_error(k, pc, pf, kmax), "err_learned": pk_error(k, pl, pf, kmax),
              "halos_fine": int(mf_f.sum()), "halos_coarse": int(mf_c.sum()),
              "halos_learned": int(mf_l.sum())}
+        runs = []
+        if filters is not None:
+            runs.append(("filtered", None))
+            if net2 is not None:
+                runs.append(("filtered_net", net2))
+        for name, nt in runs:
+            coarse.set_particles(p, sched.a_init, sched.a_init)
+            s_x, t_x, w_x = timed_run(coarse, filtered_force(coarse, filters, nt))
+            coarse.set_force_filters(None)
+            _, px, _ = power_spectrum_on(fine, s_x["x"], 1.0)
+            mf_x = halo_counts(s_x, boxsize, nc)
+            res["mf_" + name] = res.get("mf_" + name, 0) + mf_x
+            r.update({name + "_s": t_x, name + "_wall_s": w_x,
+                      "err_" + name: pk_error(k, px, pf, kmax), "halos_" + name: int(mf_x.sum())})
         res["seeds"].append(r)
         if log:
             log(str(r))
     fine.close()
     coarse.close()
     if "mf_fine" in res:
-        res["mf_err_coarse"] = mf_ratio_error(res["mf_coarse"], res["mf_fine"])
-        res["mf_err_learned"] = mf_ratio_error(res["mf_learned"], res["mf_fine"])
-        for key in ("mf_fine", "mf_coarse", "mf_learned"):
+        for name in ("coarse", "learned", "filtered", "filtered_net"):
+            if "mf_" + name in res:
+                res["mf_err_" + name] = mf_ratio_error(res["mf_" + name], res["mf_fine"])
+        for key in [k for k in res if k.startswith("mf_") and not k.startswith("mf_err")]:
             res[key] = [int(c) for c in res[key]]
     return res

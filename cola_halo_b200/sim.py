@@ -135,6 +135,21 @@ class Simulation:
         _lib.check(self.lib.cg_sim_write_gadget(self.h, aout, om, h, str(filename).encode(),
                                                 int(bool(use_long_id))), "cg_sim_write_gadget")
 
+    def set_force_filters(self, knots):
+        """Force transfer functions T(|n|): an (nsets, n) array of knots,
+        equally spaced from 0 to sqrt(3) ngrid / 2; set 0 becomes current.
+        None removes them."""
+        if knots is None:
+            _lib.check(self.lib.cg_sim_set_force_filters(self.h, None, 0, 0), "force filters")
+            return
+        k = np.ascontiguousarray(np.atleast_2d(knots), dtype=np.float32)
+        _lib.check(self.lib.cg_sim_set_force_filters(self.h, k.ctypes.data, k.shape[1],
+                                                     k.shape[0]), "force filters")
+
+    def use_force_filter(self, i):
+        """Apply set i in the following force evaluations (-1: none)."""
+        _lib.check(self.lib.cg_sim_use_force_filter(self.h, int(i)), "use force filter")
+
     def set_sort_interval(self, every):
         """Sort the particles into cell order at every `every`-th move (0:
         never); outputs keep the order the particles were given in."""

@@ -89,6 +89,17 @@ int cg_sim_move(cg_sim* s);
  * (cg_sim_get_particles, cg_sim_get_forces, snapshots) is in the order the
  * particles were given in. */
 int cg_sim_set_sort_interval(cg_sim* s, int every);
+/* Isotropic transfer functions of the PM force (no reference counterpart;
+ * the Fourier-space learned correction): the Green step multiplies the
+ * force spectrum by T(|n|), |n| in units of the fundamental mode, given at
+ * n >= 2 equally spaced knots from 0 to sqrt(3) ngrid / 2 (linear between
+ * knots).  cg_sim_set_force_filters copies nsets such functions (host
+ * array, nsets x n floats) to the device and makes set 0 current; n = 0
+ * removes them.  cg_sim_use_force_filter selects the set the following
+ * force evaluations apply (-1: none, the reference's force); it copies
+ * nothing, so a time loop can switch sets per step. */
+int cg_sim_set_force_filters(cg_sim* s, const float* knots, int n, int nsets);
+int cg_sim_use_force_filter(cg_sim* s, int set);
 /* pm_calculate_forces (pm.c:565-596).  If density_sum is non-NULL the
  * stream is synchronised and the mesh sum (check_total_density) returned. */
 int cg_sim_forces(cg_sim* s, double* density_sum);

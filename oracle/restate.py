@@ -371,10 +371,28 @@ def c2r(half, n):
     return np.fft.irfft(g, n=n, axis=2, norm="forward")
 
 
-def force_spectrum(delta_k, ngrid, boxsize, axis):
+def filter_at(den, knots, ngrid):
+    """Force transfer function T(|n|) at |n|^2 = den (no reference
+    counterpart: the Fourier-space learned correction of libcolagpu): knots
+    equally spaced over 0 <= |n| <= sqrt(3) ngrid / 2, linear in between,
+    float32 arithmetic in the device's order."""
+    t = np.asarray(knots, dtype=f32)
+    n = len(t)
+    inv_dn = f32((n - 1) / (math.sqrt(3.0) * ngrid / 2.0))
+    r = (np.sqrt(den.astype(f32)).astype(f32) * inv_dn).astype(f32)
+    i = r.astype(np.int64)
+    last = i >= n - 1
+    ic = np.minimum(i, n - 2)
+    a, b = t[ic], t[ic + 1]
+    v = (a + ((r - ic.astype(f32)).astype(f32) * (b - a).astype(f32)).astype(f32)).astype(f32)
+    return np.where(last, t[n - 1], v).astype(f32)
+
+
+def force_spectrum(delta_k, ngrid, boxsize, axis, knots=None):
     """compute_force_mesh (pm.c:304-346): F = i f2 delta_k,
     f2 = f1 n_axis / |n|^2, f1 = -1/(N^3 * 2 pi/L), signed frequencies with
-    the Nyquist index kept at +N/2 for x and y; F(0) = 0."""
+    the Nyquist index kept at +N/2 for x and y; F(0) = 0.  `knots` (not in
+    the reference) multiplies f2 by filter_at(|n|^2) before n_axis."""
     N = ngrid
     scale = f32(2.0 * math.pi / f64(f32(boxsize)))
     f1 = f32(-1.0 / N ** 3 / f64(scale))
@@ -386,17 +404,20 @@ def force_spectrum(delta_k, ngrid, boxsize, axis):
     den = (K * K + I0 * I0 + J0 * J0)
     den = np.where(den == 0, 1, den)
     di = [I0, J0, K][axis]
-    f2 = ((f1 / den.astype(f32)).astype(f32) * np.asarray(di, dtype=f32)).astype(f32)
+    g = (f1 / den.astype(f32)).astype(f32)
+    if knots is not None:
+        g = (g * filter_at(den, knots, N)).astype(f32)
+    f2 = (g * np.asarray(di, dtype=f32)).astype(f32)
     F = 1j * f2.astype(np.float64) * delta_k
     F[0, 0, 0] = 0.0
     return F
 
 
-def pm_force_meshes(x, ngrid, boxsize, factor):
+def pm_force_meshes(x, ngrid, boxsize, factor, knots=None):
     """Density, check sum and the three real force meshes (float64)."""
     dens = cic_deposit(x, ngrid, boxsize, factor)
     dk = r2c(dens)
-    meshes = [c2r(force_spectrum(dk, ngrid, boxsize, a), ngrid) for a in range(3)]
+    meshes = [c2r(force_spectrum(dk, ngrid, boxsize, a, knots), ngrid) for a in range(3)]
     return dens, dk, meshes
 
 
@@ -433,9 +454,9 @@ def cic_interp(x, mesh32, ngrid, boxsize):
     return f
 
 
-def pm_calculate_forces(x, ngrid, boxsize, factor):
+def pm_calculate_forces(x, ngrid, boxsize, factor, knots=None):
     """pm_calculate_forces (pm.c:565-596): (n,3) float32 forces."""
-    dens, dk, meshes = pm_force_meshes(x, ngrid, boxsize, factor)
+    dens, dk, meshes = pm_force_meshes(x, ngrid, boxsize, factor, knots)
     f = np.stack([cic_interp(x, m.astype(f32), ngrid, boxsize) for m in meshes], axis=1)
     return f.astype(f32), dens
 

@@ -1,0 +1,99 @@
+"""Isotropic force transfer function T(|n|) in the Green step
+(cg_sim_set_force_filters / cg_sim_use_force_filter): the Fourier-space
+form of the learned force correction, checked against the oracle's PM force
+with the same filter."""
+import numpy as np
+import pytest
+
+from oracle import restate as R
+from tests.helpers import lattice_particles
+
+pytestmark = pytest.mark.gpu
+OM = 0.273
+
+
+def _sim(nc, N, L, p):
+    from cola_halo_b200 import Simulation
+    sim = Simulation(nc, N, L, OM)
+    sim.set_particles(p, 0.1, 0.1)
+    sim.move()
+    return sim
+
+
+@pytest.mark.parametrize("nc,factor,L,nk", [(16, 3, 100.0, 9), (32, 2, 64.0, 24)])
+def test_filtered_forces_match_oracle(gpu_lib, bbks_table, nc, factor, L, nk):
+    N = nc * factor
+    p = lattice_particles(nc, L, 40 + nc, OM, 0.1, bbks_table)
+    knots = (1.0 + 0.4 * np.sin(np.linspace(0.0, 5.0, nk))).astype(np.float32)
+    sim = _sim(nc, N, L, p)
+    sim.set_force_filters(knots)
+    sim.forces()
+    f = sim.get_forces()
+    x = R.wrap(p["x"], L)
+    _, _, meshes = R.pm_force_meshes(x, N, L, factor, knots)
+    for a in range(3):
+        m = sim.get_mesh(1 + a)
+        assert np.abs(m - meshes[a]).max() < 2e-5 * np.abs(meshes[a]).max()
+    fo, _ = R.pm_calculate_forces(x, N, L, factor, knots)
+    scale = np.abs(fo).max()
+    assert np.abs(f - fo).max() < 2e-5 * scale
+    # the filter changed the force (the test is not vacuous)
+    f0, _ = R.pm_calculate_forces(x, N, L, factor)
+    assert np.abs(f0 - fo).max() > 1e-2 * scale
+    sim.close()
+
+
+def test_identity_scaling_and_selection(gpu_lib, bbks_table):
+    """T = 1 is the reference's force bit for bit; T = 2 doubles it exactly
+    (power-of-two scaling commutes with every rounding on the path); set
+    selection and removal switch between them without a copy."""
+    nc, N, L = 16, 48, 100.0
+    p = lattice_particles(nc, L, 77, OM, 0.1, bbks_table)
+    sim = _sim(nc, N, L, p)
+    sim.forces()
+    f0 = sim.get_forces()
+    sim.set_force_filters(np.stack([np.ones(6), 2 * np.ones(6),
+                                    np.linspace(1.0, 0.0, 6)]).astype(np.float32))
+    sim.forces()
+    np.testing.assert_array_equal(sim.get_forces(), f0)            # set 0 is current
+    sim.use_force_filter(1)
+    sim.forces()
+    np.testing.assert_array_equal(sim.get_forces(), 2 * f0)
+    sim.use_force_filter(2)
+    sim.forces()
+    f2 = sim.get_forces()
+    assert np.abs(f2).max() < np.abs(f0).max()
+    sim.use_force_filter(-1)
+    sim.forces()
+    np.testing.assert_array_equal(sim.get_forces(), f0)
+    from cola_halo_b200._lib import ColaGpuError
+    with pytest.raises(ColaGpuError):
+        sim.use_force_filter(3)
+    sim.set_force_filters(None)
+    with pytest.raises(ColaGpuError):
+        sim.use_force_filter(0)
+    sim.forces()
+    np.testing.assert_array_equal(sim.get_forces(), f0)
+    sim.close()
+
+
+def test_forces_are_linear_in_the_knots(gpu_lib, bbks_table):
+    """F(sum_j T_j e_j) = sum_j T_j F(e_j): the basis the least-squares fit
+    of the transfer function is built on."""
+    nc, N, L = 16, 32, 80.0
+    p = lattice_particles(nc, L, 12, OM, 0.1, bbks_table)
+    sim = _sim(nc, N, L, p)
+    nk = 7
+    sim.set_force_filters(np.eye(nk, dtype=np.float32))
+    basis = []
+    for j in range(nk):
+        sim.use_force_filter(j)
+        sim.forces()
+        basis.append(sim.get_forces().astype(np.float64))
+    t = np.linspace(1.3, 0.6, nk).astype(np.float32)
+    sim.set_force_filters(t)
+    sim.forces()
+    f = sim.get_forces()
+    want = np.tensordot(t.astype(np.float64), np.array(basis), axes=1)
+    assert np.abs(f - want).max() < 1e-5 * np.abs(want).max()
+    sim.close()
