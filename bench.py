@@ -804,6 +804,14 @@ def run_batch(args):
     return 0
 
 
+# coarse runs beside the conv net: (name, mesh, (gradient, laplacian,
+# deconvolve), fitted transfer functions)
+LEARNED_VARIANTS = (("deconv2_128", 128, (0, 0, 2), False),
+                    ("filtered_192", 192, (0, 0, 0), True),
+                    ("filtered_fd4_192", 192, (4, 0, 1), True),
+                    ("filtered_256", 256, (0, 0, 0), True))
+
+
 def run_learned(args):
     """Learned coarse-mesh run vs the plain factor-3 run (128^3 particles,
     L = 300 Mpc/h, coarse 128^3 / fine 384^3 mesh, 10 steps from z = 49):
@@ -821,7 +829,7 @@ def run_learned(args):
     net2 = ConvNet(nc, seed=8)
     res = evaluate(nc, L, sched, net, list(range(1, args.train_seeds + 1)),
                    list(range(1001, 1001 + args.eval_seeds)), table, epochs=args.epochs,
-                   filter_nk=16, net2=net2,
+                   filter_nk=16, net2=net2, variants=LEARNED_VARIANTS,
                    log=lambda s: print(s, file=sys.stderr, flush=True))
     seeds = res["seeds"]
     fine_s = float(np.mean([r["fine_s"] for r in seeds]))
@@ -859,7 +867,7 @@ def run_learned(args):
     # the Fourier-space correction: per-step transfer functions T_s(|n|) of
     # the coarse force (16 knots, least squares on 4 training seeds), alone
     # and with a second net trained on the filtered force
-    for name in ("filtered", "filtered_net"):
+    for name in ["filtered", "filtered_net"] + [v[0] for v in LEARNED_VARIANTS]:
         if "err_" + name in seeds[0]:
             t = float(np.mean([r[name + "_s"] for r in seeds]))
             out[name] = {"s": t, "speedup_vs_plain_fine": fine_s / t,
@@ -868,6 +876,11 @@ def run_learned(args):
                          "pk_err_max": float(np.max([r["err_" + name] for r in seeds])),
                          "mf_ratio_err": res.get("mf_err_" + name),
                          "mf": res.get("mf_" + name)}
+    for name, ng, kernel, fit in LEARNED_VARIANTS:
+        if name in out:
+            out[name].update({"mesh": ng, "force_kernel": list(kernel), "fitted": fit})
+            if fit:
+                out[name]["fit_s"] = res["fit_s_" + name]
     if "filters" in res:
         out["filter"] = {"knots": 16, "fit_seeds": 4, "fit_s": res["filter_fit_s"],
                          "T_first_last_step": [[round(v, 4) for v in res["filters"][0]],

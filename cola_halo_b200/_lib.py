@@ -55,6 +55,7 @@ SIGNATURES = {
     "cg_sim_set_sort_interval": (i32, [P, i32]),
     "cg_sim_set_force_filters": (i32, [P, P, i32, i32]),
     "cg_sim_use_force_filter": (i32, [P, i32]),
+    "cg_sim_set_force_kernel": (i32, [P, i32, i32, i32]),
     "cg_net_create": (i32, [ctypes.POINTER(P), i32, ctypes.c_ulonglong]),
     "cg_net_destroy": (None, [P]),
     "cg_net_num_params": (i32, []),

@@ -109,6 +109,11 @@ static void sim_free(cg_sim* s) {
   delete s;
 }
 
+static bool force_kernel_ok(int gradient, int laplacian, int deconvolve) {
+  return (gradient == 0 || gradient == 2 || gradient == 4) && (laplacian == 0 || laplacian == 1) &&
+         deconvolve >= 0 && deconvolve <= 2;
+}
+
 extern "C" int cg_sim_create(cg_sim** out, int nc, int ngrid, float boxsize, double omega_m,
                              long long np_capacity) {
   if (!out) return set_err(CG_EINVAL, "cg_sim_create: out is NULL");
@@ -127,6 +132,9 @@ extern "C" int cg_sim_create(cg_sim** out, int nc, int ngrid, float boxsize, dou
   s->ct.reset(new ColaTime(omega_m));
   cudaError_t e = cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = pm_plan_alloc(&s->pm, ngrid, ngrid / nc > 0 ? ngrid / nc : 1, boxsize);
+  // a particle's mass in mesh units, (ngrid / nc)^3 (pm.c:216 for integer
+  // factors; a mesh that is no multiple of nc, e.g. 192 for 128^3, too)
+  if (e == cudaSuccess) s->pm.wpar = (float)pow((double)ngrid / nc, 3.0);
   if (e == cudaSuccess) {
     s->ps.cap = np_capacity;
     e = cudaMalloc(&s->soa_block, sizeof(float) * 15 * (size_t)np_capacity);
@@ -140,6 +148,16 @@ extern "C" int cg_sim_create(cg_sim** out, int nc, int ngrid, float boxsize, dou
   // L2: 256^3 particles gain 0.45 ms a step, 128^3 lose 0.1 ms
   s->sort_every = np_capacity >= (1LL << 23) ? 2 : 0;
   if (const char* ev = getenv("COLAGPU_SORT_EVERY")) s->sort_every = atoi(ev) > 0 ? atoi(ev) : 0;
+  // COLAGPU_FORCE_KERNEL=g,l,d selects the force kernel of every new
+  // realization (cg_sim_set_force_kernel), the drop-in's included
+  if (const char* ev = getenv("COLAGPU_FORCE_KERNEL")) {
+    int g = 0, l = 0, d = 0;
+    if (sscanf(ev, "%d,%d,%d", &g, &l, &d) == 3 && force_kernel_ok(g, l, d)) {
+      if (e == cudaSuccess) e = pm_set_force_kernel(&s->pm, g, l, d);
+    } else {
+      fprintf(stderr, "libcolagpu: COLAGPU_FORCE_KERNEL=%s ignored (want g,l,d)\n", ev);
+    }
+  }
   if (e != cudaSuccess) {
     int rc = cuda_err(e, "cg_sim_create");
     sim_free(s);
@@ -257,6 +275,14 @@ extern "C" int cg_sim_move(cg_sim* s) {
     CG_CHECK(particles_sort_cells(&s->ps, &s->order, s->L, s->st), "cell-order sort");
     s->sorted = true;
   }
+  return CG_OK;
+}
+
+extern "C" int cg_sim_set_force_kernel(cg_sim* s, int gradient, int laplacian, int deconvolve) {
+  if (!s || !force_kernel_ok(gradient, laplacian, deconvolve))
+    return set_err(CG_EINVAL, "cg_sim_set_force_kernel: bad arguments");
+  CG_CHECK(cudaStreamSynchronize(s->st), "sync");    // no queued Green step reads the old tables
+  CG_CHECK(pm_set_force_kernel(&s->pm, gradient, laplacian, deconvolve), "force kernel");
   return CG_OK;
 }
 

@@ -53,6 +53,8 @@ struct PmPlan {
   int kfilt_sets;           //   functions held
   int kfilt_cur;            //   the one the Green step applies; -1 = none
   float kfilt_inv_dn;       //   knots per unit of |n|
+  float* ktab;              // device: gradient | Laplacian | window tables (N each), or
+                            //   NULL for the reference's spectral kernel
 };
 
 // Plain 3-D real transforms on the mesh layouts above (unnormalised, FFTW
@@ -98,6 +100,11 @@ cudaError_t pm_set_filters(PmPlan* p, const float* knots, int n, int nsets);
 // Make set `set` current (-1: none, the reference's force).  False when the
 // plan holds no such set.
 bool pm_use_filter(PmPlan* p, int set);
+// Force kernel of the Green step: gradient 0 spectral (the reference), 2 or
+// 4 the 2- or 4-point central difference; laplacian 0 exact |n|^2 (the
+// reference), 1 the 7-point discrete Laplacian; deconvolve 0, 1 or 2 times
+// the CIC window.  All 0: the reference's kernel, no tables.
+cudaError_t pm_set_force_kernel(PmPlan* p, int gradient, int laplacian, int deconvolve);
 void pm_plan_free(PmPlan* p);
 // Full PM force: deposit -> r2c -> Green/gradient -> 3 c2r -> interpolation.
 // Positions and forces are SoA device arrays of n floats per component.

@@ -410,16 +410,18 @@ __global__ void __launch_bounds__(T) k_fy(float2* __restrict__ spec,
 
 // Load of a kx column scaled by the force component's wavenumber index:
 // SCALE 1 by n_x = I0 (signed, Nyquist at +N/2; the position n along the
-// column), SCALE 2 by n_z = kz (the plane, constant over the CTA).
+// column), SCALE 2 by n_z = kz (the plane, constant over the CTA).  With a
+// gradient table g (finite-difference gradient), g[n] replaces n_x.
 template <int SCALE>
 struct GmemScaled {
   const float2* p;
   size_t es;
   int N;
   float fz;
+  const float* g;
   __device__ __forceinline__ cplx ld(int b, int n) const {
     const float2 v = __ldg(p + b + (size_t)n * es);
-    const float f = SCALE == 1 ? (float)(n <= N / 2 ? n : n - N) : fz;
+    const float f = SCALE == 1 ? (g ? __ldg(g + n) : (float)(n <= N / 2 ? n : n - N)) : fz;
     return cplx{v.x * f, v.y * f};
   }
   static constexpr bool kShared = false;
@@ -427,10 +429,12 @@ struct GmemScaled {
 
 // FX: c2c along kx (stride N), TKV ky columns per CTA, from `in` to `out`
 // (the same array for an in-place pass).  SCALE 0: plain; 1 / 2: the input
-// is first multiplied by n_x / n_z (GmemScaled).
+// is first multiplied by n_x / n_z (GmemScaled; gtab: the gradient table or
+// NULL, unused by SCALE 0).
 template <int N, int DIR, int SCALE, int TKV, int RMX>
 __global__ void __launch_bounds__(T) k_fx(const float2* in, float2* out,
-                                          const float2* __restrict__ twN) {
+                                          const float2* __restrict__ twN,
+                                          const float* __restrict__ gtab) {
   extern __shared__ __align__(16) unsigned char smraw[];
   const SmemCol<TKV> mid{reinterpret_cast<cplx*>(smraw)};
   const size_t off = (size_t)blockIdx.y * N * N + blockIdx.x * TKV;
@@ -439,20 +443,28 @@ __global__ void __launch_bounds__(T) k_fx(const float2* in, float2* out,
     const Gmem gi{const_cast<float2*>(in) + off, 1, (size_t)N};
     cgfft::fft_io<N, TKV, T, false, DIR, RMX>(gi, mid, go, twN);
   } else {
-    const GmemScaled<SCALE> gi{in + off, (size_t)N, N, (float)blockIdx.y};
+    const float fz = SCALE == 2 && gtab ? __ldg(gtab + blockIdx.y) : (float)blockIdx.y;
+    const GmemScaled<SCALE> gi{in + off, (size_t)N, N, fz, gtab};
     cgfft::fft_io<N, TKV, T, false, DIR, RMX>(gi, mid, go, twN);
   }
 }
 
-// Optional isotropic transfer function of the force, T(|n|) (|n| in units
-// of the fundamental), sampled at knots |n| = j / inv_dn, j < n, and
-// interpolated linearly (T = last knot beyond the table): the Fourier-space
-// form of the learned force correction.  t == NULL: no filter, the
-// reference's force unchanged.
-struct KFilter {
+// Options of the Green step beyond the reference's kernel (all off: the
+// reference's exact spectral force).
+//  * t: an isotropic transfer function of the force T(|n|) (|n| in units of
+//    the fundamental), sampled at knots |n| = j / inv_dn, j < n, linear in
+//    between (the last knot beyond the table): the Fourier-space form of
+//    the learned force correction.  NULL: none.
+//  * tab: NULL, or three tables of N floats indexed like the spectrum's
+//    axes (signed index s = i <= N/2 ? i : i - N): the gradient factor that
+//    replaces s (a finite-difference gradient), the per-axis term of the
+//    Laplacian that replaces s^2 in |n|^2 (the discrete Laplacian), and
+//    the per-axis factor that divides out the CIC window.
+struct GreenMods {
   const float* t;
   int n;
   float inv_dn;
+  const float* tab;
   __device__ __forceinline__ float at(int den) const {
     const float r = __fmul_rn(sqrtf((float)den), inv_dn);
     const int i = (int)r;
@@ -470,12 +482,12 @@ struct KFilter {
 // forward-transformed tile: MODE 0 the y component (n_y = J0, the position
 // along the line), MODE 1 the factor without n_a, MODE 2 the y component
 // while it writes the MODE 1 value back in place.
-template <int P, int MODE>
+template <int P, int MODE, bool MODS>
 struct GreenLoad {
   cplx* s;
   int kz, kx0, N;
   float f1;
-  KFilter kf;
+  GreenMods gm;
   __device__ __forceinline__ cplx ld(int b, int n) const {
     const cplx p = s[b * P + n + (n >> 4)];
     const int kx = kx0 + b;
@@ -486,15 +498,26 @@ struct GreenLoad {
       if (MODE == 2) s[b * P + n + (n >> 4)] = cplx{0.0f, 0.0f};
       return cplx{0.0f, 0.0f};
     }
-    float f2 = __fdiv_rn(f1, (float)den);
-    if (kf.t) f2 = __fmul_rn(f2, kf.at(den));
+    // MODS false: the reference's kernel, with none of the options' code
+    const float* tab = MODS ? gm.tab : nullptr;
+    float f2;
+    if (tab) {
+      const float* lap = tab + N;
+      const float* win = tab + 2 * N;
+      f2 = __fdiv_rn(f1, __fadd_rn(__fadd_rn(__ldg(lap + kx), __ldg(lap + n)), __ldg(lap + kz)));
+      if (gm.t) f2 = __fmul_rn(f2, gm.at(den));
+      f2 = __fmul_rn(f2, __fmul_rn(__fmul_rn(__ldg(win + kx), __ldg(win + n)), __ldg(win + kz)));
+    } else {
+      f2 = __fdiv_rn(f1, (float)den);
+      if (MODS && gm.t) f2 = __fmul_rn(f2, gm.at(den));
+    }
     if (MODE == 2) {
       // the shared x/z value replaces the loaded one in place (this thread
       // is the element's only reader in this stage), so the second inverse
       // transform reads it plainly instead of dividing again
       s[b * P + n + (n >> 4)] = cplx{-__fmul_rn(f2, p.y), __fmul_rn(f2, p.x)};
     }
-    if (MODE != 1) f2 = __fmul_rn(f2, (float)J0);
+    if (MODE != 1) f2 = __fmul_rn(f2, tab ? __ldg(tab + n) : (float)J0);
     return cplx{-__fmul_rn(f2, p.y), __fmul_rn(f2, p.x)};
   }
   static constexpr bool kShared = true;
@@ -516,12 +539,12 @@ __device__ __noinline__ void fft_tile_y(const First f, const Mid m, const Last l
 // by the inverse x pass as it loads g2 (k_fx, SCALE 1 and 2): one inverse
 // transform serves both components.  BG lines (kz, kx0 .. kx0+BG-1) per
 // CTA; N is a multiple of BG so the lines of a CTA share kz.
-template <int N, int BG, int RMG, int MINB>
+template <int N, int BG, int RMG, int MINB, bool MODS>
 __global__ void __launch_bounds__(T, MINB) k_green(const float2* __restrict__ spec,
                                                          float2* __restrict__ g1,
                                                          float2* __restrict__ g2,
                                                          const float2* __restrict__ twN,
-                                                         float f1, KFilter kf) {
+                                                         float f1, GreenMods gm) {
   constexpr int P = cgfft::line_pitch<N>();
   extern __shared__ __align__(16) unsigned char smraw[];
   cplx* D = reinterpret_cast<cplx*>(smraw);
@@ -534,7 +557,7 @@ __global__ void __launch_bounds__(T, MINB) k_green(const float2* __restrict__ sp
   const SmemLine<P> d{D}, w{W};
   fft_tile_y<N, BG, RMG, -1>(gin, d, d, twN);
   // the y component's load also leaves the shared x/z value in D
-  const GreenLoad<P, 2> gy{D, kz, kx0, N, f1, kf};
+  const GreenLoad<P, 2, MODS> gy{D, kz, kx0, N, f1, gm};
   const Gmem oy{g1 + off, (size_t)N, 1};
   fft_tile_y<N, BG, RMG, 1>(gy, w, oy, twN);
   __syncthreads();
@@ -646,11 +669,12 @@ struct MeshKernels {
   void (*fz)(const float*, float2*, const float2*, const float2*, double*);
   void (*fyf)(float2*, const float2*);
   void (*fyi)(float2*, const float2*);
-  void (*fxf)(const float2*, float2*, const float2*);
-  void (*fxi)(const float2*, float2*, const float2*);
-  void (*fxi_x)(const float2*, float2*, const float2*);   // inverse, input times n_x
-  void (*fxi_z)(const float2*, float2*, const float2*);   // inverse, input times n_z
-  void (*green)(const float2*, float2*, float2*, const float2*, float, KFilter);
+  void (*fxf)(const float2*, float2*, const float2*, const float*);
+  void (*fxi)(const float2*, float2*, const float2*, const float*);
+  void (*fxi_x)(const float2*, float2*, const float2*, const float*);   // input times n_x
+  void (*fxi_z)(const float2*, float2*, const float2*, const float*);   // input times n_z
+  void (*green)(const float2*, float2*, float2*, const float2*, float, GreenMods);
+  void (*green_mods)(const float2*, float2*, float2*, const float2*, float, GreenMods);
   void (*zi)(const float2*, float*, const float2*, const float2*);
   size_t sm_fz, sm_fy, sm_fx, sm_green, sm_zi;
   int tk;    // ky columns per CTA of the x pass
@@ -671,7 +695,8 @@ void set_fx(MeshKernels* k) {
 template <int N, int V>
 void set_green(MeshKernels* k) {
   constexpr GreenCfg c = kGreenCfg[V];
-  k->green = k_green<N, c.byg, c.rm, c.minb>;
+  k->green = k_green<N, c.byg, c.rm, c.minb, false>;
+  k->green_mods = k_green<N, c.byg, c.rm, c.minb, true>;
   k->sm_green = sizeof(cplx) * 2 * c.byg * cgfft::line_pitch<N>();
   k->byg = c.byg;
 }
@@ -752,6 +777,7 @@ cudaError_t set_all_smem(int N) {
     if (e == cudaSuccess) e = set_smem((const void*)k.fxi_x, k.sm_fx);
     if (e == cudaSuccess) e = set_smem((const void*)k.fxi_z, k.sm_fx);
     if (e == cudaSuccess) e = set_smem((const void*)k.green, k.sm_green);
+    if (e == cudaSuccess) e = set_smem((const void*)k.green_mods, k.sm_green);
     if (e == cudaSuccess) e = set_smem((const void*)k.zi, k.sm_zi);
   }
   return e;
@@ -843,7 +869,7 @@ cudaError_t pm_autotune(PmPlan* p, cudaStream_t st, MeshSched* best, float* ms_g
     e = best_time(st, kReps, [&] {
       prof_mark(st, CG_ST_OTHER);
       k.green<<<(N / 2 + 1) * N / k.byg, T, k.sm_green, st>>>(p->spec, p->gsp[1], p->gsp[2],
-                                                               p->twN, p->f1, KFilter{});
+                                                               p->twN, p->f1, GreenMods{});
     }, &t);
     if (ms_green) ms_green[v] = t;
     if (e == cudaSuccess && t < tbest) {
@@ -858,7 +884,8 @@ cudaError_t pm_autotune(PmPlan* p, cudaStream_t st, MeshSched* best, float* ms_g
     float t = 0.0f;
     e = best_time(st, kReps, [&] {
       prof_mark(st, CG_ST_OTHER);
-      k.fxi_x<<<dim3(N / k.tk, N / 2 + 1), T, k.sm_fx, st>>>(p->gsp[2], p->gsp[0], p->twN);
+      k.fxi_x<<<dim3(N / k.tk, N / 2 + 1), T, k.sm_fx, st>>>(p->gsp[2], p->gsp[0], p->twN,
+                                                             nullptr);
     }, &t);
     if (ms_fx) ms_fx[v] = t;
     if (e == cudaSuccess && t < tbest) {
@@ -958,7 +985,7 @@ cudaError_t mesh_r2c(const MeshFFT* f, const float* real, float2* spec, cudaStre
   prof_mark(st, CG_ST_OTHER);
   k.fyf<<<(N / 2 + 1) * N / BY, T, k.sm_fy, st>>>(spec, f->twN);
   prof_mark(st, CG_ST_FX_FWD);
-  k.fxf<<<dim3(N / k.tk, N / 2 + 1), T, k.sm_fx, st>>>(spec, spec, f->twN);
+  k.fxf<<<dim3(N / k.tk, N / 2 + 1), T, k.sm_fx, st>>>(spec, spec, f->twN, nullptr);
   return cudaGetLastError();
 }
 
@@ -967,7 +994,7 @@ cudaError_t mesh_c2r(const MeshFFT* f, float2* spec, float* real, cudaStream_t s
   if (!get_kernels(f->N, &k)) return cudaErrorInvalidValue;
   const int N = f->N;
   prof_mark(st, CG_ST_FX_INV);
-  k.fxi<<<dim3(N / k.tk, N / 2 + 1), T, k.sm_fx, st>>>(spec, spec, f->twN);
+  k.fxi<<<dim3(N / k.tk, N / 2 + 1), T, k.sm_fx, st>>>(spec, spec, f->twN, nullptr);
   prof_mark(st, CG_ST_OTHER);
   k.fyi<<<(N / 2 + 1) * N / BY, T, k.sm_fy, st>>>(spec, f->twN);
   prof_mark(st, CG_ST_ZI);
@@ -1000,6 +1027,38 @@ cudaError_t pm_set_filters(PmPlan* p, const float* knots, int n, int nsets) {
   return cudaSuccess;
 }
 
+cudaError_t pm_set_force_kernel(PmPlan* p, int gradient, int laplacian, int deconvolve) {
+  if (gradient == 0 && laplacian == 0 && deconvolve == 0) {
+    cudaFree(p->ktab);
+    p->ktab = nullptr;
+    return cudaSuccess;
+  }
+  const int N = p->N;
+  std::vector<float> t(3 * (size_t)N);
+  for (int i = 0; i < N; i++) {
+    const double s = i <= N / 2 ? i : i - N;
+    const double w = M_PI * s / N;               // half the mesh phase k h / 2
+    // gradient: the transfer function of the difference operator, in units
+    // of the fundamental (h = L / N, k = 2 pi s / L, k h = 2 w)
+    double g = s;
+    if (gradient == 2) g = N / (2 * M_PI) * sin(2 * w);
+    if (gradient == 4) g = N / (2 * M_PI) * (8 * sin(2 * w) - sin(4 * w)) / 6;
+    // Laplacian: s^2, or the 3-point second difference's (N / pi sin w)^2
+    const double l = laplacian ? (N / M_PI * sin(w)) * (N / M_PI * sin(w)) : s * s;
+    // CIC window per axis sinc^2(w); divided out `deconvolve` times
+    const double sinc = i == 0 ? 1.0 : sin(w) / w;
+    const double c = pow(sinc * sinc, -(double)deconvolve);
+    t[i] = (float)g;
+    t[N + i] = (float)l;
+    t[2 * N + i] = (float)c;
+  }
+  if (!p->ktab) {
+    cudaError_t e = cudaMalloc(&p->ktab, sizeof(float) * t.size());
+    if (e != cudaSuccess) return e;
+  }
+  return cudaMemcpy(p->ktab, t.data(), sizeof(float) * t.size(), cudaMemcpyHostToDevice);
+}
+
 bool pm_use_filter(PmPlan* p, int set) {
   if (set >= p->kfilt_sets) return false;
   p->kfilt_cur = set < 0 ? -1 : set;
@@ -1008,6 +1067,7 @@ bool pm_use_filter(PmPlan* p, int set) {
 
 void pm_plan_free(PmPlan* p) {
   cudaFree(p->kfilt);
+  cudaFree(p->ktab);
   cudaFree(p->dens);
   cudaFree(p->spec);
   for (int a = 0; a < 3; a++) {
@@ -1070,7 +1130,7 @@ cudaError_t pm_r2c(PmPlan* p, cudaStream_t st) {
   prof_mark(st, CG_ST_FZ);
   k.fz<<<dim3(N / TY, N), T, k.sm_fz, st>>>(p->dens, p->spec, p->twH, p->twN, p->dsum);
   prof_mark(st, CG_ST_FX_FWD);
-  k.fxf<<<dim3(N / k.tk, N / 2 + 1), T, k.sm_fx, st>>>(p->spec, p->spec, p->twN);
+  k.fxf<<<dim3(N / k.tk, N / 2 + 1), T, k.sm_fx, st>>>(p->spec, p->spec, p->twN, nullptr);
   return cudaGetLastError();
 }
 
@@ -1080,24 +1140,24 @@ cudaError_t pm_green_c2r(PmPlan* p, cudaStream_t st) {
   const int N = p->N;
   // gsp[1] <- y component, gsp[2] <- the shared x/z spectrum
   prof_mark(st, CG_ST_GREEN);
-  const KFilter kf{p->kfilt_cur >= 0 ? p->kfilt + (size_t)p->kfilt_cur * p->kfilt_n : nullptr,
-                   p->kfilt_n, p->kfilt_inv_dn};
-  k.green<<<(N / 2 + 1) * N / k.byg, T, k.sm_green, st>>>(p->spec, p->gsp[1], p->gsp[2],
-                                                           p->twN, p->f1, kf);
+  const GreenMods gm{p->kfilt_cur >= 0 ? p->kfilt + (size_t)p->kfilt_cur * p->kfilt_n : nullptr,
+                     p->kfilt_n, p->kfilt_inv_dn, p->ktab};
+  (gm.t || gm.tab ? k.green_mods : k.green)<<<(N / 2 + 1) * N / k.byg, T, k.sm_green, st>>>(
+      p->spec, p->gsp[1], p->gsp[2], p->twN, p->f1, gm);
   const dim3 gx(N / k.tk, N / 2 + 1), gz(N / TY, N);
   // x: n_x * gsp[2] -> gsp[0] (gsp[2] is still needed for z)
   prof_mark(st, CG_ST_FX_INV);
-  k.fxi_x<<<gx, T, k.sm_fx, st>>>(p->gsp[2], p->gsp[0], p->twN);
+  k.fxi_x<<<gx, T, k.sm_fx, st>>>(p->gsp[2], p->gsp[0], p->twN, p->ktab);
   prof_mark(st, CG_ST_ZI);
   k.zi<<<gz, T, k.sm_zi, st>>>(p->gsp[0], p->fmesh[0], p->twH, p->twN);
   // y: in place
   prof_mark(st, CG_ST_FX_INV);
-  k.fxi<<<gx, T, k.sm_fx, st>>>(p->gsp[1], p->gsp[1], p->twN);
+  k.fxi<<<gx, T, k.sm_fx, st>>>(p->gsp[1], p->gsp[1], p->twN, nullptr);
   prof_mark(st, CG_ST_ZI);
   k.zi<<<gz, T, k.sm_zi, st>>>(p->gsp[1], p->fmesh[1], p->twH, p->twN);
   // z: n_z * gsp[2], in place
   prof_mark(st, CG_ST_FX_INV);
-  k.fxi_z<<<gx, T, k.sm_fx, st>>>(p->gsp[2], p->gsp[2], p->twN);
+  k.fxi_z<<<gx, T, k.sm_fx, st>>>(p->gsp[2], p->gsp[2], p->twN, p->ktab);
   prof_mark(st, CG_ST_ZI);
   k.zi<<<gz, T, k.sm_zi, st>>>(p->gsp[2], p->fmesh[2], p->twH, p->twN);
   return cudaGetLastError();
@@ -1135,7 +1195,7 @@ cudaError_t pm_power_spectrum(PmPlan* p, const float* const x[3], long long n, i
   prof_mark(st, CG_ST_FZ);
   k.fz<<<dim3(N / TY, N), T, k.sm_fz, st>>>(p->dens, p->spec, p->twH, p->twN, p->dsum);
   prof_mark(st, CG_ST_FX_FWD);
-  k.fxf<<<dim3(N / k.tk, N / 2 + 1), T, k.sm_fx, st>>>(p->spec, p->spec, p->twN);
+  k.fxf<<<dim3(N / k.tk, N / 2 + 1), T, k.sm_fx, st>>>(p->spec, p->spec, p->twN, nullptr);
   prof_mark(st, CG_ST_OTHER);
   k.fyf<<<(N / 2 + 1) * N / BY, T, k.sm_fy, st>>>(p->spec, p->twN);
   cudaMemsetAsync(acc, 0, sizeof(double) * 3 * nbins, st);

@@ -238,7 +238,8 @@ def pk_error(k, p, p_ref, kmax):
 
 
 def evaluate(nc, boxsize, sched, net, train_seeds, eval_seeds, table, *, omega_m=0.273,
-             epochs=1, lr=2e-3, filter_nk=16, filter_seeds=4, net2=None, log=None):
+             epochs=1, lr=2e-3, filter_nk=16, filter_seeds=4, net2=None, variants=(),
+             log=None):
     """Train on PM pairs, then judge plain-coarse and learned-coarse runs
     against the plain factor-3 run on held-out seeds: P(k) error up to half
     the particle Nyquist wavenumber, and the device time of each run's time
@@ -247,7 +248,12 @@ def evaluate(nc, boxsize, sched, net, train_seeds, eval_seeds, table, *, omega_m
     filter_nk > 0 also fits per-step force transfer functions of filter_nk
     knots on the first `filter_seeds` training seeds (fit_force_filter) and
     judges the filtered coarse run; `net2`, when given, is trained on the
-    filtered coarse force and judged as filter + net."""
+    filtered coarse force and judged as filter + net.  Each
+    (name, ngrid, kernel, fit) in `variants` adds a run on an ngrid mesh
+    with the Green-step options `kernel` = (gradient, laplacian,
+    deconvolve) and, when `fit`, its own fitted transfer functions (knots
+    at the coarse mesh's spacing in |n|): the error-versus-time curve
+    between the coarse and the fine mesh."""
     import time
 
     from .sim import Simulation
@@ -274,6 +280,18 @@ def evaluate(nc, boxsize, sched, net, train_seeds, eval_seeds, table, *, omega_m
             res["train2_s"] = time.perf_counter() - t0
             res["loss2_last"] = float(np.mean(h2[-10:]))
             coarse.set_force_filters(None)
+    extra = []                 # (name, realization, filters or None)
+    for name, ng, kernel, fit in variants:
+        sim = Simulation(nc, ng, boxsize, omega_m)
+        sim.set_force_kernel(*kernel)
+        fl = None
+        if fit:
+            t0 = time.perf_counter()
+            fl = fit_force_filter(sim, fine, sched, train_seeds[:filter_seeds], table,
+                                  nk=max(filter_nk, filter_nk * ng // nc), omega_m=omega_m,
+                                  log=log)
+            res["fit_s_" + name] = time.perf_counter() - t0
+        extra.append((name, sim, fl))
 
     lib = _lib.load()
     nst = _lib.NSTAGES
@@ -318,13 +336,15 @@ def evaluate(nc, boxsize, sched, net, train_seeds, eval_seeds, table, *, omega_m
              "halos_learned": int(mf_l.sum())}
         runs = []
         if filters is not None:
-            runs.append(("filtered", None))
+            runs.append(("filtered", coarse, filters, None))
             if net2 is not None:
-                runs.append(("filtered_net", net2))
-        for name, nt in runs:
-            coarse.set_particles(p, sched.a_init, sched.a_init)
-            s_x, t_x, w_x = timed_run(coarse, filtered_force(coarse, filters, nt))
-            coarse.set_force_filters(None)
+                runs.append(("filtered_net", coarse, filters, net2))
+        runs += [(name, sim, fl, None) for name, sim, fl in extra]
+        for name, sim, fl, nt in runs:
+            sim.set_particles(p, sched.a_init, sched.a_init)
+            s_x, t_x, w_x = timed_run(sim, sim.forces if fl is None else
+                                      filtered_force(sim, fl, nt))
+            sim.set_force_filters(None)
             _, px, _ = power_spectrum_on(fine, s_x["x"], 1.0)
             mf_x = halo_counts(s_x, boxsize, nc)
             res["mf_" + name] = res.get("mf_" + name, 0) + mf_x
@@ -335,8 +355,10 @@ def evaluate(nc, boxsize, sched, net, train_seeds, eval_seeds, table, *, omega_m
             log(str(r))
     fine.close()
     coarse.close()
+    for _, sim, _ in extra:
+        sim.close()
     if "mf_fine" in res:
-        for name in ("coarse", "learned", "filtered", "filtered_net"):
+        for name in ["coarse", "learned", "filtered", "filtered_net"] + [e[0] for e in extra]:
             if "mf_" + name in res:
                 res["mf_err_" + name] = mf_ratio_error(res["mf_" + name], res["mf_fine"])
         for key in [k for k in res if k.startswith("mf_") and not k.startswith("mf_err")]:

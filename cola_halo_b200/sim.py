@@ -135,6 +135,13 @@ class Simulation:
         _lib.check(self.lib.cg_sim_write_gadget(self.h, aout, om, h, str(filename).encode(),
                                                 int(bool(use_long_id))), "cg_sim_write_gadget")
 
+    def set_force_kernel(self, gradient=0, laplacian=0, deconvolve=0):
+        """Green-step options: gradient 0 (spectral, the reference), 2 or 4
+        (central differences); laplacian 0 (exact) or 1 (discrete);
+        deconvolve 0, 1 or 2 (times the CIC window)."""
+        _lib.check(self.lib.cg_sim_set_force_kernel(self.h, gradient, laplacian, deconvolve),
+                   "force kernel")
+
     def set_force_filters(self, knots):
         """Force transfer functions T(|n|): an (nsets, n) array of knots,
         equally spaced from 0 to sqrt(3) ngrid / 2; set 0 becomes current.

@@ -60,8 +60,9 @@ void* cg_host_alloc(size_t bytes);
 void cg_host_free(void* p);
 
 /* Create a realization: nc^3 particles capacity np_capacity (>= nc^3),
- * PM mesh of ngrid^3 cells (ngrid = factor * nc), periodic box boxsize.
- * Replaces pm_init (pm.c:87-198) for one handle. */
+ * PM mesh of ngrid^3 cells (ngrid = factor * nc in the reference; any
+ * built mesh size here, a particle weighing (ngrid/nc)^3 mesh units),
+ * periodic box boxsize.  Replaces pm_init (pm.c:87-198) for one handle. */
 int cg_sim_create(cg_sim** out, int nc, int ngrid, float boxsize, double omega_m,
                   long long np_capacity);
 void cg_sim_destroy(cg_sim* s);
@@ -89,6 +90,19 @@ int cg_sim_move(cg_sim* s);
  * (cg_sim_get_particles, cg_sim_get_forces, snapshots) is in the order the
  * particles were given in. */
 int cg_sim_set_sort_interval(cg_sim* s, int every);
+/* Force kernel of the Green step (no reference counterpart; the
+ * reference's kernel, pm.c:304-346, is the default: exact spectral gradient
+ * i n_a, exact 1/|n|^2, no window correction).  gradient: 0 spectral, 2 the
+ * 2-point or 4 the 4-point central difference of the potential (applied in
+ * Fourier space as the difference operator's transfer function, identical
+ * to the real-space stencil on the periodic mesh); laplacian: 0 exact, 1 the
+ * 7-point discrete Laplacian; deconvolve: divide the force by the CIC
+ * window sinc^2 per axis 0, 1 (deposit) or 2 (deposit and interpolation)
+ * times.  The environment variable COLAGPU_FORCE_KERNEL=g,l,d sets it for
+ * every realization created afterwards, the drop-in's included.
+ * CG_EINVAL for other values. */
+int cg_sim_set_force_kernel(cg_sim* s, int gradient, int laplacian, int deconvolve);
+
 /* Isotropic transfer functions of the PM force (no reference counterpart;
  * the Fourier-space learned correction): the Green step multiplies the
  * force spectrum by T(|n|), |n| in units of the fundamental mode, given at

@@ -388,11 +388,37 @@ def filter_at(den, knots, ngrid):
     return np.where(last, t[n - 1], v).astype(f32)
 
 
-def force_spectrum(delta_k, ngrid, boxsize, axis, knots=None):
+def force_kernel_tables(ngrid, gradient=0, laplacian=0, deconvolve=0):
+    """Per-axis tables of the Green step's options (no reference
+    counterpart; libcolagpu's cg_sim_set_force_kernel), float32 from float64
+    formulas, indexed by the FFT index i (signed s = i <= N/2 ? i : i - N):
+    gradient factor (s; 2-point N/2pi sin 2w; 4-point N/2pi (8 sin 2w -
+    sin 4w)/6, w = pi s/N), Laplacian term (s^2 or (N/pi sin w)^2) and the
+    CIC window correction sinc(w)^(-2 deconvolve)."""
+    N = ngrid
+    i = np.arange(N)
+    s = np.where(i <= N // 2, i, i - N).astype(np.float64)
+    w = np.pi * s / N
+    if gradient == 2:
+        g = N / (2 * np.pi) * np.sin(2 * w)
+    elif gradient == 4:
+        g = N / (2 * np.pi) * (8 * np.sin(2 * w) - np.sin(4 * w)) / 6
+    else:
+        g = s
+    lap = (N / np.pi * np.sin(w)) ** 2 if laplacian else s * s
+    sinc = np.where(i == 0, 1.0, np.sin(w) / np.where(w == 0, 1.0, w))
+    c = (sinc * sinc) ** (-float(deconvolve))
+    return g.astype(f32), lap.astype(f32), c.astype(f32)
+
+
+def force_spectrum(delta_k, ngrid, boxsize, axis, knots=None, kernel=(0, 0, 0)):
     """compute_force_mesh (pm.c:304-346): F = i f2 delta_k,
     f2 = f1 n_axis / |n|^2, f1 = -1/(N^3 * 2 pi/L), signed frequencies with
-    the Nyquist index kept at +N/2 for x and y; F(0) = 0.  `knots` (not in
-    the reference) multiplies f2 by filter_at(|n|^2) before n_axis."""
+    the Nyquist index kept at +N/2 for x and y; F(0) = 0.  Beyond the
+    reference: `knots` multiplies f2 by filter_at(|n|^2) before n_axis, and
+    kernel = (gradient, laplacian, deconvolve) replaces n_axis, |n|^2 and
+    the window factor by force_kernel_tables' entries, in the device's
+    float32 order."""
     N = ngrid
     scale = f32(2.0 * math.pi / f64(f32(boxsize)))
     f1 = f32(-1.0 / N ** 3 / f64(scale))
@@ -404,20 +430,33 @@ def force_spectrum(delta_k, ngrid, boxsize, axis, knots=None):
     den = (K * K + I0 * I0 + J0 * J0)
     den = np.where(den == 0, 1, den)
     di = [I0, J0, K][axis]
-    g = (f1 / den.astype(f32)).astype(f32)
-    if knots is not None:
-        g = (g * filter_at(den, knots, N)).astype(f32)
-    f2 = (g * np.asarray(di, dtype=f32)).astype(f32)
+    if tuple(kernel) == (0, 0, 0):
+        g = (f1 / den.astype(f32)).astype(f32)
+        if knots is not None:
+            g = (g * filter_at(den, knots, N)).astype(f32)
+        f2 = (g * np.asarray(di, dtype=f32)).astype(f32)
+    else:
+        gt, lt, wt = force_kernel_tables(N, *kernel)
+        ix = idx[:, None, None]
+        iy = idx[None, :, None]
+        iz = np.arange(N // 2 + 1)[None, None, :]
+        dl = ((lt[ix] + lt[iy]).astype(f32) + lt[iz]).astype(f32)
+        g = (f1 / np.where(dl == 0, f32(1), dl)).astype(f32)
+        if knots is not None:
+            g = (g * filter_at(den, knots, N)).astype(f32)
+        g = (g * ((wt[ix] * wt[iy]).astype(f32) * wt[iz]).astype(f32)).astype(f32)
+        f2 = (g * [gt[ix], gt[iy], gt[iz]][axis]).astype(f32)
     F = 1j * f2.astype(np.float64) * delta_k
     F[0, 0, 0] = 0.0
     return F
 
 
-def pm_force_meshes(x, ngrid, boxsize, factor, knots=None):
+def pm_force_meshes(x, ngrid, boxsize, factor, knots=None, kernel=(0, 0, 0)):
     """Density, check sum and the three real force meshes (float64)."""
     dens = cic_deposit(x, ngrid, boxsize, factor)
     dk = r2c(dens)
-    meshes = [c2r(force_spectrum(dk, ngrid, boxsize, a, knots), ngrid) for a in range(3)]
+    meshes = [c2r(force_spectrum(dk, ngrid, boxsize, a, knots, kernel), ngrid)
+              for a in range(3)]
     return dens, dk, meshes
 
 
@@ -454,9 +493,9 @@ def cic_interp(x, mesh32, ngrid, boxsize):
     return f
 
 
-def pm_calculate_forces(x, ngrid, boxsize, factor, knots=None):
+def pm_calculate_forces(x, ngrid, boxsize, factor, knots=None, kernel=(0, 0, 0)):
     """pm_calculate_forces (pm.c:565-596): (n,3) float32 forces."""
-    dens, dk, meshes = pm_force_meshes(x, ngrid, boxsize, factor, knots)
+    dens, dk, meshes = pm_force_meshes(x, ngrid, boxsize, factor, knots, kernel)
     f = np.stack([cic_interp(x, m.astype(f32), ngrid, boxsize) for m in meshes], axis=1)
     return f.astype(f32), dens
 

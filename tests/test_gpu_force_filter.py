@@ -97,3 +97,56 @@ def test_forces_are_linear_in_the_knots(gpu_lib, bbks_table):
     want = np.tensordot(t.astype(np.float64), np.array(basis), axes=1)
     assert np.abs(f - want).max() < 1e-5 * np.abs(want).max()
     sim.close()
+
+
+@pytest.mark.parametrize("kernel", [(2, 0, 0), (4, 0, 0), (0, 1, 0), (0, 0, 1), (0, 0, 2),
+                                    (4, 1, 2)])
+def test_force_kernels_match_oracle(gpu_lib, bbks_table, kernel):
+    """Finite-difference gradients, the discrete Laplacian and the CIC
+    window correction (cg_sim_set_force_kernel) against the oracle's force
+    with the same tables."""
+    nc, factor, L = 16, 3, 100.0
+    N = nc * factor
+    p = lattice_particles(nc, L, 31, OM, 0.1, bbks_table)
+    sim = _sim(nc, N, L, p)
+    sim.set_force_kernel(*kernel)
+    sim.forces()
+    f = sim.get_forces()
+    x = R.wrap(p["x"], L)
+    _, _, meshes = R.pm_force_meshes(x, N, L, factor, kernel=kernel)
+    for a in range(3):
+        m = sim.get_mesh(1 + a)
+        assert np.abs(m - meshes[a]).max() < 2e-5 * np.abs(meshes[a]).max()
+    fo, _ = R.pm_calculate_forces(x, N, L, factor, kernel=kernel)
+    scale = np.abs(fo).max()
+    assert np.abs(f - fo).max() < 2e-5 * scale
+    f0, _ = R.pm_calculate_forces(x, N, L, factor)
+    assert np.abs(f0 - fo).max() > 1e-3 * scale          # the mode changed the force
+    # back to the reference's kernel, bit for bit
+    sim.set_force_kernel(0, 0, 0)
+    sim.forces()
+    g = sim.get_forces()
+    sim2 = _sim(nc, N, L, p)
+    sim2.forces()
+    np.testing.assert_array_equal(g, sim2.get_forces())
+    sim.close()
+    sim2.close()
+
+
+def test_force_kernel_with_filter_matches_oracle(gpu_lib, bbks_table):
+    nc, factor, L = 16, 2, 64.0
+    N = nc * factor
+    p = lattice_particles(nc, L, 9, OM, 0.1, bbks_table)
+    knots = np.linspace(1.2, 0.7, 10).astype(np.float32)
+    sim = _sim(nc, N, L, p)
+    sim.set_force_kernel(4, 0, 2)
+    sim.set_force_filters(knots)
+    sim.forces()
+    f = sim.get_forces()
+    fo, _ = R.pm_calculate_forces(R.wrap(p["x"], L), N, L, factor, knots=knots, kernel=(4, 0, 2))
+    assert np.abs(f - fo).max() < 2e-5 * np.abs(fo).max()
+    from cola_halo_b200._lib import ColaGpuError
+    for bad in ((1, 0, 0), (0, 2, 0), (0, 0, 3), (-2, 0, 0)):
+        with pytest.raises(ColaGpuError):
+            sim.set_force_kernel(*bad)
+    sim.close()
