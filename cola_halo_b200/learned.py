@@ -180,6 +180,76 @@ def fit_force_filter(coarse, fine, sched, seeds, table, *, nk=16, sample=1 << 18
     return T.astype(np.float32)
 
 
+def _final_positions(sim, sched, force):
+    """Positions at a = 1 of the reference time loop on `sim`."""
+    aout = output_scale_factors((0.0,))
+    snaps = []
+    run_time_loop(sched, aout, move=sim.move, force=force, kick=sim.kick, drift=sim.drift,
+                  snapshot=lambda a, i: snaps.append(sim.snapshot(a)),
+                  kick_drift=sim.kick_drift)
+    return snaps[-1]["x"]
+
+
+def calibrate_force_filter(sim, fine, sched, seeds, table, *, nk=16, base=None, iters=10,
+                           gamma=0.5, kmax=None, omega_m=0.273, log=None):
+    """Calibrate the transfer function of `sim`'s force on its final P(k):
+    T_s(|n|) = base_s(|n|) C(|n|) with one C shared by all steps, updated
+    multiplicatively from the ratio of the a = 1 power spectra of `sim` and
+    of the fine realization on the training seeds,
+        C <- C (P_sim / P_fine)^(-g),
+    the ratio averaged over the seeds and read at each knot by linear
+    interpolation in |n| over the bins up to `kmax` (h/Mpc; default the
+    particle Nyquist wavenumber), held at its last value beyond.  An update
+    that does not lower the training error (max over k <= kmax / 2 of
+    |P/P_fine - 1|, mean over seeds) is discarded and retried with g
+    halved (g starts at `gamma`).  Returns the best iterate as an
+    (nsteps, nk) float32 array, with the error history of the `iters`
+    evaluations."""
+    nc, L, ng = fine.nc, fine.boxsize, sim.ngrid
+    kmax = kmax or np.pi * nc / L
+    if base is None:
+        base = np.ones((sched.nloop - 1, nk), dtype=np.float32)
+    nk = base.shape[1]
+    knot_n = np.arange(nk) * (np.sqrt(3.0) * ng / 2) / (nk - 1)
+    truth = []
+    for seed in seeds:
+        p = _lpt_particles(nc, L, seed, omega_m, sched.a_init, table)
+        fine.set_particles(p, sched.a_init, sched.a_init)
+        k, pf, _ = power_spectrum_on(fine, _final_positions(fine, sched, fine.forces), 1.0)
+        truth.append((p, pf))
+    n_of_k = k * L / (2 * np.pi)
+    fit = (k > 0) & (k <= kmax)
+
+    def trial(C):
+        filt = (base * C[None, :]).astype(np.float32)
+        ratios, errs = [], []
+        for p, pf in truth:
+            sim.set_particles(p, sched.a_init, sched.a_init)
+            x = _final_positions(sim, sched, filtered_force(sim, filt))
+            sim.set_force_filters(None)
+            _, pc, _ = power_spectrum_on(fine, x, 1.0)
+            ratios.append(pc / np.where(pf > 0, pf, 1.0))
+            errs.append(pk_error(k, pc, pf, 0.5 * kmax))
+        return float(np.mean(errs)), np.mean(ratios, axis=0), filt
+
+    err, ratio, filt = trial(np.ones(nk))
+    best = (err, ratio, np.ones(nk), filt)
+    hist = [err]
+    g = gamma
+    for it in range(iters - 1):
+        rk = np.interp(knot_n, n_of_k[fit], best[1][fit])
+        C = best[2] * np.clip(rk, 0.5, 2.0) ** (-g)
+        err, ratio, filt = trial(C)
+        hist.append(err)
+        if log:
+            log("calibration %d (g %.3g): training P(k) error %.4f" % (it, g, err))
+        if err < best[0]:
+            best = (err, ratio, C, filt)
+        else:
+            g *= 0.5
+    return best[3], hist
+
+
 def filtered_force(sim, filters, net=None):
     """A force callback for run_time_loop that applies filters[s] at the
     s-th force evaluation (the last one beyond the table), plus the conv
@@ -249,11 +319,13 @@ def evaluate(nc, boxsize, sched, net, train_seeds, eval_seeds, table, *, omega_m
     knots on the first `filter_seeds` training seeds (fit_force_filter) and
     judges the filtered coarse run; `net2`, when given, is trained on the
     filtered coarse force and judged as filter + net.  Each
-    (name, ngrid, kernel, fit) in `variants` adds a run on an ngrid mesh
-    with the Green-step options `kernel` = (gradient, laplacian,
-    deconvolve) and, when `fit`, its own fitted transfer functions (knots
-    at the coarse mesh's spacing in |n|): the error-versus-time curve
-    between the coarse and the fine mesh."""
+    (name, ngrid, kernel, fit, calibrate, nk) in `variants` adds a run on an
+    ngrid mesh with the Green-step options `kernel` = (gradient, laplacian,
+    deconvolve), with transfer functions of nk knots: least-squares fitted
+    on forces when `fit` (fit_force_filter), then calibrated on the final
+    P(k) when `calibrate` (calibrate_force_filter), both on the first
+    `filter_seeds` training seeds: the error-versus-time curve between the
+    coarse and the fine mesh."""
     import time
 
     from .sim import Simulation
@@ -281,16 +353,21 @@ def evaluate(nc, boxsize, sched, net, train_seeds, eval_seeds, table, *, omega_m
             res["loss2_last"] = float(np.mean(h2[-10:]))
             coarse.set_force_filters(None)
     extra = []                 # (name, realization, filters or None)
-    for name, ng, kernel, fit in variants:
+    for name, ng, kernel, fit, calibrate, nk in variants:
         sim = Simulation(nc, ng, boxsize, omega_m)
         sim.set_force_kernel(*kernel)
         fl = None
+        t0 = time.perf_counter()
         if fit:
-            t0 = time.perf_counter()
-            fl = fit_force_filter(sim, fine, sched, train_seeds[:filter_seeds], table,
-                                  nk=max(filter_nk, filter_nk * ng // nc), omega_m=omega_m,
-                                  log=log)
+            fl = fit_force_filter(sim, fine, sched, train_seeds[:filter_seeds], table, nk=nk,
+                                  omega_m=omega_m, log=log)
+        if calibrate:
+            fl, hist = calibrate_force_filter(sim, fine, sched, train_seeds[:filter_seeds], table,
+                                              nk=nk, base=fl, omega_m=omega_m, log=log)
+            res["cal_hist_" + name] = hist
+        if fit or calibrate:
             res["fit_s_" + name] = time.perf_counter() - t0
+            res["filters_" + name] = fl.tolist()
         extra.append((name, sim, fl))
 
     lib = _lib.load()
