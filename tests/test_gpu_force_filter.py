@@ -191,3 +191,32 @@ def test_fitted_transfer_function_gains_over_the_plain_coarse_mesh(gpu_lib, bbks
     assert e["cal"] < 0.5 * e["coarse"], e
     for s in (fine, coarse, deconv):
         s.close()
+
+
+def test_force_kernel_from_the_environment(gpu_lib, bbks_table, tmp_path):
+    """COLAGPU_FORCE_KERNEL=g,l,d sets the kernel of every realization a
+    process creates (the drop-in's included): a child process with it set
+    gives the forces that cg_sim_set_force_kernel gives here."""
+    import os
+    import subprocess
+    import sys
+    nc, N, L = 16, 32, 64.0
+    p = lattice_particles(nc, L, 4, OM, 0.1, bbks_table)
+    np.save(tmp_path / "p.npy", p)
+    sim = _sim(nc, N, L, p)
+    sim.set_force_kernel(4, 0, 2)
+    sim.forces()
+    want = sim.get_forces()
+    sim.close()
+    code = ("import numpy as np, sys; sys.path.insert(0, %r)\n"
+            "from cola_halo_b200 import Simulation\n"
+            "p = np.load(%r)\n"
+            "s = Simulation(%d, %d, %r, %r); s.set_particles(p, 0.1, 0.1); s.move(); s.forces()\n"
+            "np.save(%r, s.get_forces())\n"
+            % (os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
+               str(tmp_path / "p.npy"), nc, N, L, OM, str(tmp_path / "f.npy")))
+    env = dict(os.environ, COLAGPU_FORCE_KERNEL="4,0,2")
+    r = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True,
+                       timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    np.testing.assert_array_equal(np.load(tmp_path / "f.npy"), want)
