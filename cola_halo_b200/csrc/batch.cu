@@ -90,6 +90,7 @@ PmPlan view(const PmPlan& bufs, const MeshFFT& tab, int N, int factor, float L) 
   p.twH = tab.twH;
   p.mesh_bytes = sizeof(float) * (size_t)N * N * N;
   p.spec_bytes = sizeof(float2) * (size_t)(N / 2 + 1) * N * N;
+  p.ztm_ok = false;    // the stream's TMA maps describe its largest mesh, not this one
   return p;
 }
 

@@ -311,6 +311,10 @@ static int check_err_word(cg_sim* s) {
   CG_CHECK(cudaMemcpyAsync(&err, s->pm.err, sizeof(unsigned), cudaMemcpyDeviceToHost, s->st),
            "read error word");
   CG_CHECK(cudaStreamSynchronize(s->st), "sync");
+  if (err & CG_ERR_TMA_WAIT) {
+    cudaMemsetAsync(s->pm.err, 0, sizeof(unsigned), s->st);
+    return set_err(CG_ECUDA, "z transform: a TMA gather did not complete (error word 0x%x)", err);
+  }
   if (err) {
     cudaMemsetAsync(s->pm.err, 0, sizeof(unsigned), s->st);
     return set_err(CG_EPARTICLE, "particle position %s (device error word 0x%x)",

@@ -1,5 +1,6 @@
 // Internal declarations shared by the CUDA translation units of libcolagpu.
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stddef.h>
 #include <stdint.h>
@@ -20,6 +21,7 @@ void prof_mark(cudaStream_t st, int stage);
 enum {
   CG_ERR_BAD_CELL = 1,      // a particle's y or z cell index was negative
   CG_ERR_NONFINITE = 2,     // a particle position was NaN or infinite
+  CG_ERR_TMA_WAIT = 4,      // a TMA gather of the z transform did not complete
 };
 
 // Mesh transform plan: every buffer of one PM mesh size.
@@ -55,6 +57,8 @@ struct PmPlan {
   float kfilt_inv_dn;       //   knots per unit of |n|
   float* ktab;              // device: gradient | Laplacian | window tables (N each), or
                             //   NULL for the reference's spectral kernel
+  CUtensorMap ztm[3];       // TMA maps of gsp[0..2] for the z transform's gather
+  bool ztm_ok;              //   valid (else the cp.async gather runs)
 };
 
 // Plain 3-D real transforms on the mesh layouts above (unnormalised, FFTW
