@@ -145,8 +145,10 @@ extern "C" int cg_sim_create(cg_sim** out, int nc, int ngrid, float boxsize, dou
   s->ps.id = s->id_alloc;
   s->ps.orig = s->orig_alloc;
   // the sort pays only where the particles and meshes are far larger than
-  // L2: 256^3 particles gain 0.45 ms a step, 128^3 lose 0.1 ms
-  s->sort_every = np_capacity >= (1LL << 23) ? 2 : 0;
+  // L2 (128^3 particles lose 0.1 ms a step), and there every sixth move:
+  // 10-step runs of 256^3 particles take 11.57 ms a step against 11.89 sorting
+  // every second move and 11.87 never; 512^3 on 1024^3, 38.3 against 40.6 ms
+  s->sort_every = np_capacity >= (1LL << 23) ? 6 : 0;
   if (const char* ev = getenv("COLAGPU_SORT_EVERY")) s->sort_every = atoi(ev) > 0 ? atoi(ev) : 0;
   // COLAGPU_FORCE_KERNEL=g,l,d selects the force kernel of every new
   // realization (cg_sim_set_force_kernel), the drop-in's included
