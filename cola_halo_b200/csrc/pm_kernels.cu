@@ -841,7 +841,7 @@ MeshKernels make_kernels(MeshSched s) {
   return k;
 }
 
-#define CG_MESH_SIZES(X) X(16) X(32) X(48) X(64) X(96) X(128) X(192) X(256) X(384) X(512) X(768) X(1024)
+#define CG_MESH_SIZES(X) X(16) X(32) X(48) X(64) X(96) X(128) X(144) X(192) X(256) X(384) X(512) X(768) X(1024)
 
 bool kernels_with(int N, MeshSched s, MeshKernels* out) {
   switch (N) {

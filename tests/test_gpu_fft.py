@@ -7,7 +7,7 @@ from oracle import restate as R
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("n", [16, 32, 48, 96, 192])
+@pytest.mark.parametrize("n", [16, 32, 48, 96, 144, 192])
 def test_r2c_matches_numpy(gpu_lib, n):
     from cola_halo_b200 import fft_r2c
     rng = np.random.default_rng(n)
@@ -18,7 +18,7 @@ def test_r2c_matches_numpy(gpu_lib, n):
     assert err < 2e-6, err
 
 
-@pytest.mark.parametrize("n", [16, 32, 48, 96, 192])
+@pytest.mark.parametrize("n", [16, 32, 48, 96, 144, 192])
 def test_c2r_non_hermitian_matches_fftw_convention(gpu_lib, n):
     """Random (non-Hermitian) half spectra: c2c over x, y then a z c2r that
     ignores Im of kz = 0 and kz = n/2 (pm.c:325-353 relies on this)."""

@@ -12,7 +12,7 @@ OM = 0.273
 
 
 @pytest.mark.parametrize("nc,factor,L", [(16, 3, 100.0), (32, 3, 200.0), (16, 2, 64.0),
-                                         (32, 1, 300.0)])
+                                         (32, 1, 300.0), (48, 3, 150.0)])
 def test_forces_match_oracle(gpu_lib, bbks_table, nc, factor, L):
     from cola_halo_b200 import Simulation
     N = nc * factor
