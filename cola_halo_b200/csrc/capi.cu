@@ -501,6 +501,11 @@ extern "C" int cg_sim_power_spectrum(cg_sim* s, int nbins, int flags, double* k,
 
 extern "C" int cg_sim_get_mesh(cg_sim* s, int which, float* out) {
   if (!s || !out || which < 0 || which > 3) return set_err(CG_EINVAL, "cg_sim_get_mesh: bad args");
+  if (which == 0 && s->pm.dens_reset) {
+    // the force step consumed the density: deposit the current positions again
+    const float* x[3] = {s->ps.x[0], s->ps.x[1], s->ps.x[2]};
+    CG_CHECK(pm_deposit(&s->pm, x, s->ps.n, s->st), "deposit");
+  }
   const float* src = which == 0 ? s->pm.dens : s->pm.fmesh[which - 1];
   CG_CHECK(cudaMemcpyAsync(out, src, s->pm.mesh_bytes, cudaMemcpyDeviceToHost, s->st), "get mesh");
   CG_CHECK(cudaStreamSynchronize(s->st), "sync");
@@ -649,6 +654,7 @@ extern "C" int cg_net_train_step(cg_net* h, cg_sim* coarse, cg_sim* fine, float 
                                  double* loss) {
   if (!h || !coarse || !fine || coarse->pm.N != h->n.N || coarse->ps.n != fine->ps.n)
     return set_err(CG_EINVAL, "cg_net_train_step: bad arguments");
+  coarse->pm.keep_dens = true;   // the net's features read the density after the force
   int rc = cg_sim_forces(coarse, nullptr);
   if (!rc) rc = cg_sim_forces(fine, nullptr);
   if (rc) return rc;
@@ -674,6 +680,7 @@ extern "C" int cg_net_train_step(cg_net* h, cg_sim* coarse, cg_sim* fine, float 
 // Forces of the coarse realization with the learned correction added.
 extern "C" int cg_net_forces(cg_net* h, cg_sim* coarse) {
   if (!h || !coarse || coarse->pm.N != h->n.N) return set_err(CG_EINVAL, "cg_net_forces: bad");
+  coarse->pm.keep_dens = true;   // the net's features read the density after the force
   int rc = cg_sim_forces(coarse, nullptr);
   if (rc) return rc;
   cudaStream_t st = coarse->st;   // stay on the realization's stream

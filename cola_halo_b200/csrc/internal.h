@@ -57,6 +57,9 @@ struct PmPlan {
   float kfilt_inv_dn;       //   knots per unit of |n|
   float* ktab;              // device: gradient | Laplacian | window tables (N each), or
                             //   NULL for the reference's spectral kernel
+  bool keep_dens;           // the density must survive the force step (else the z r2c
+                            //   resets it to -1 for the next deposit)
+  bool dens_reset;          // dens holds -1 everywhere, not the last density
   CUtensorMap ztm[3];       // TMA maps of gsp[0..2] for the z transform's gather
   bool ztm_ok;              //   valid (else the cp.async gather runs)
 };

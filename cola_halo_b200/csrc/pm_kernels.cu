@@ -368,7 +368,9 @@ __host__ __device__ constexpr int fx_rm(int N, int v) {
 // stored transposed into S[kz][x][y].  The sum of the mesh
 // (check_total_density, pm.c:535-562) is the sum over lines of
 // Re Z_0 + Im Z_0, accumulated in double.
-template <int N>
+// RESET: once its lines are in shared memory, the CTA writes them back as
+// -1, the value the next deposit starts from, so that no fill pass is needed.
+template <int N, bool RESET>
 __global__ void __launch_bounds__(T) k_fz(const float* __restrict__ dens,
                                           float2* __restrict__ spec,
                                           const float2* __restrict__ twH,
@@ -382,6 +384,11 @@ __global__ void __launch_bounds__(T) k_fz(const float* __restrict__ dens,
   const Gmem gin{reinterpret_cast<float2*>(const_cast<float*>(dens)) + ((size_t)x * N + y0) * H,
                  (size_t)H, 1};
   cgfft::fft_io<H, TY, T, true, -1>(gin, mid, mid, twH);
+  if constexpr (RESET) {
+    __syncthreads();    // every thread's loads of the lines are done
+    float4* line = reinterpret_cast<float4*>(const_cast<float*>(dens) + ((size_t)x * N + y0) * N);
+    for (int i = threadIdx.x; i < TY * N / 4; i += T) line[i] = make_float4(-1.f, -1.f, -1.f, -1.f);
+  }
   double acc = 0.0;
   for (int idx = threadIdx.x; idx < (H + 1) * TY; idx += T) {
     const int b = idx % TY, k = idx / TY;
@@ -773,6 +780,7 @@ __global__ void __launch_bounds__(T) k_pk_bin(const float2* __restrict__ spec, i
 // ------------------------------------------------------- dispatch table
 struct MeshKernels {
   void (*fz)(const float*, float2*, const float2*, const float2*, double*);
+  void (*fz_reset)(const float*, float2*, const float2*, const float2*, double*);
   void (*fyf)(float2*, const float2*);
   void (*fyi)(float2*, const float2*);
   void (*fxf)(const float2*, float2*, const float2*, const float*);
@@ -811,7 +819,8 @@ void set_green(MeshKernels* k) {
 template <int N>
 MeshKernels make_kernels(MeshSched s) {
   MeshKernels k;
-  k.fz = k_fz<N>;
+  k.fz = k_fz<N, false>;
+  k.fz_reset = k_fz<N, true>;
   k.fyf = k_fy<N, -1>;
   k.fyi = k_fy<N, 1>;
   k.zi = k_zi<N>;
@@ -879,6 +888,7 @@ cudaError_t set_all_smem(int N) {
     if (!kernels_with(N, MeshSched{v < ng ? v : 0, v < nv ? v : 0}, &k))
       return cudaErrorInvalidValue;
     if (e == cudaSuccess) e = set_smem((const void*)k.fz, k.sm_fz);
+    if (e == cudaSuccess) e = set_smem((const void*)k.fz_reset, k.sm_fz);
     if (e == cudaSuccess) e = set_smem((const void*)k.fyf, k.sm_fy);
     if (e == cudaSuccess) e = set_smem((const void*)k.fyi, k.sm_fy);
     if (e == cudaSuccess) e = set_smem((const void*)k.fxf, k.sm_fx);
@@ -1205,12 +1215,18 @@ cudaError_t pm_deposit(PmPlan* p, const float* const x[3], long long n, cudaStre
       getenv("COLAGPU_DEPOSIT") && getenv("COLAGPU_DEPOSIT")[0] == 't';
   if (tiled_deposit) {
     cudaError_t e = pm_deposit_tiled(p, x, n, st);
-    if (e != cudaErrorNotSupported) return e;
+    if (e != cudaErrorNotSupported) {
+      p->dens_reset = false;
+      return e;
+    }
   }
   // scatter with global float atomics into a mesh filled with -1
   const size_t n4 = (size_t)p->N * p->N * p->N / 4;
-  prof_mark(st, CG_ST_FILL);
-  k_fill<<<grid_for((long long)n4), T, 0, st>>>(reinterpret_cast<float4*>(p->dens), n4, -1.0f);
+  if (!p->dens_reset) {   // else the last z r2c left the mesh at -1 already
+    prof_mark(st, CG_ST_FILL);
+    k_fill<<<grid_for((long long)n4), T, 0, st>>>(reinterpret_cast<float4*>(p->dens), n4, -1.0f);
+  }
+  p->dens_reset = false;
   if (n > 0) {
     prof_mark(st, CG_ST_DEPOSIT);
     static const bool plain = getenv("COLAGPU_DEPOSIT") && getenv("COLAGPU_DEPOSIT")[0] == 'p';
@@ -1241,7 +1257,9 @@ cudaError_t pm_r2c(PmPlan* p, cudaStream_t st) {
   const int N = p->N;
   cudaMemsetAsync(p->dsum, 0, sizeof(double), st);
   prof_mark(st, CG_ST_FZ);
-  k.fz<<<dim3(N / TY, N), T, k.sm_fz, st>>>(p->dens, p->spec, p->twH, p->twN, p->dsum);
+  (p->keep_dens ? k.fz : k.fz_reset)<<<dim3(N / TY, N), T, k.sm_fz, st>>>(p->dens, p->spec,
+                                                                            p->twH, p->twN, p->dsum);
+  p->dens_reset = !p->keep_dens;
   prof_mark(st, CG_ST_FX_FWD);
   k.fxf<<<dim3(N / k.tk, N / 2 + 1), T, k.sm_fx, st>>>(p->spec, p->spec, p->twN, nullptr);
   return cudaGetLastError();
