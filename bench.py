@@ -181,14 +181,17 @@ def dist_setup(args):
     return rank, world, local
 
 
-def algorithmic_bytes(stage, N, npart):
-    """Algorithmic bytes per launch of each stage (each tensor counted once)."""
+def algorithmic_bytes(stage, N, npart, reset=True):
+    """Algorithmic bytes per launch of each stage (each tensor counted once):
+    the deposit reads the positions and writes the mesh once; the z r2c reads
+    the mesh, writes the half spectrum and (reset) writes -1 back over the
+    mesh for the next deposit."""
     Mr = 4.0 * N ** 3
     Ms = 8.0 * (N // 2 + 1) * N * N
     return {
         "fill": Mr,
-        "deposit": 12.0 * npart,
-        "fz_r2c": Mr + Ms,
+        "deposit": 12.0 * npart + Mr,
+        "fz_r2c": Mr + Ms + (Mr if reset else 0.0),
         "fx_fwd": 2 * Ms,
         "green_y": 3 * Ms,
         "fx_inv": 2 * Ms,
@@ -420,6 +423,16 @@ def run_b200(args, cfg):
                 "achieved": ab / (per_launch_ms / 1e3) / 1e9, "peak": hbm, "unit": "GB/s",
                 "frac": ab / (per_launch_ms / 1e3) / 1e9 / hbm, "traffic": traffic,
                 "algorithmic_bytes": ab, "peak_source": peak_kind}
+    # the same figures for every stage with an algorithmic-byte count
+    stage_roofline = {}
+    for name, st in stages.items():
+        b = algorithmic_bytes(name, N, npart)
+        if b is None or not st["launches"]:
+            continue
+        t = st["ms"] / st["launches"] / 1e3
+        stage_roofline[name] = {"ms_per_launch": round(t * 1e3, 4),
+                                "gbs": round(b / t / 1e9, 1), "frac": round(b / t / 1e9 / hbm, 3)}
+    roofline["stages"] = stage_roofline
 
     # ---- end to end through the drop-in C ABI with host buffers
     sim.close()

@@ -48,6 +48,7 @@ SIGNATURES = {
     "cg_sim_snapshot": (i32, [P, f64, f32, P]),
     "cg_sim_sync": (i32, [P]),
     "cg_sim_get_mesh": (i32, [P, i32, P]),
+    "cg_sim_keep_density": (i32, [P, i32]),
     "cg_sim_power_spectrum": (i32, [P, i32, i32, P, P, P]),
     "cg_pk_bins_noalloc": (i32, [P, i32, f32, i32, i32, P, P, P, i64, P]),
     "cg_sim_stream": (P, [P]),

@@ -499,6 +499,12 @@ extern "C" int cg_sim_power_spectrum(cg_sim* s, int nbins, int flags, double* k,
   return CG_OK;
 }
 
+extern "C" int cg_sim_keep_density(cg_sim* s, int keep) {
+  if (!s) return set_err(CG_EINVAL, "cg_sim_keep_density: null handle");
+  s->pm.keep_dens = keep != 0;
+  return CG_OK;
+}
+
 extern "C" int cg_sim_get_mesh(cg_sim* s, int which, float* out) {
   if (!s || !out || which < 0 || which > 3) return set_err(CG_EINVAL, "cg_sim_get_mesh: bad args");
   if (which == 0 && s->pm.dens_reset) {

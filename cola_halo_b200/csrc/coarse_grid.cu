@@ -24,14 +24,6 @@ namespace {
 
 constexpr int T = CG_THREADS;
 
-int grid_for(long long n) {
-  long long b = (n + T - 1) / T;
-  const long long cap = 148LL * 16;
-  if (b > cap) b = cap;
-  if (b < 1) b = 1;
-  return (int)b;
-}
-
 // The eight cells and CIC weights of one particle, in the reference's
 // corner order and arithmetic (coarse_grid.c:101-120).
 __device__ __forceinline__ void cic_corners(const ParticleMinimum& q, float dx_inv, int nc,

@@ -254,9 +254,7 @@ cudaError_t launch_v(const __nv_bfloat16* in, int N, const __nv_bfloat16* w, con
     attr = true;
   }
   const int ntiles = N * N * (N / TILE_M);
-  int dev = 0, sms = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int sms = cg_sm_count();
   const int grid = ntiles < CPS * sms ? ntiles : CPS * sms;
   prof_mark(st, CG_ST_OTHER);
   k_conv_tc<FLIP, STAGES, CPS><<<grid, THREADS, smem_bytes(STAGES), st>>>(in, N, w, bias, act,

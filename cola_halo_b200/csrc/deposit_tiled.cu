@@ -275,14 +275,6 @@ __global__ void __launch_bounds__(T) k_tile(const float4* __restrict__ sorted,
   }
 }
 
-int grid_for(long long n) {
-  long long b = (n + T - 1) / T;
-  const long long cap = 148LL * 16;
-  if (b > cap) b = cap;
-  if (b < 1) b = 1;
-  return (int)b;
-}
-
 }  // namespace
 
 cudaError_t pm_deposit_tiled(PmPlan* p, const float* const x[3], long long n, cudaStream_t st) {

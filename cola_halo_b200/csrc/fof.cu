@@ -47,14 +47,6 @@ struct PMin {
   long long id;
 };
 
-int grid_for(long long n) {
-  long long b = (n + T - 1) / T;
-  const long long cap = 148LL * 16;
-  if (b > cap) b = cap;
-  if (b < 1) b = 1;
-  return (int)b;
-}
-
 __device__ __forceinline__ float wrap1(float x, float L) {
   // one-shot periodic wrap as move.c:34-41
   if (x < 0.0f) x += L;
@@ -423,10 +415,8 @@ cudaError_t wrap_device_and_host(ParticleMinimum* d, ParticleMinimum* h, long lo
   if (e == cudaSuccess) e = cudaMalloc(&d_x, sizeof(float) * 3 * cap);
   if (e == cudaSuccess) e = cudaMemsetAsync(d_count, 0, sizeof(unsigned long long), st);
   if (e == cudaSuccess) {
-    long long blocks = (n + CG_THREADS - 1) / CG_THREADS;
-    if (blocks > 148LL * 16) blocks = 148LL * 16;
     prof_mark(st, CG_ST_WRAP);
-    k_wrap_list<<<(int)blocks, CG_THREADS, 0, st>>>(d, n, L, d_count, cap, d_idx, d_x);
+    k_wrap_list<<<cg_grid(n, 16), CG_THREADS, 0, st>>>(d, n, L, d_count, cap, d_idx, d_x);
     e = cudaGetLastError();
   }
   unsigned long long moved = 0;

@@ -223,10 +223,8 @@ int gadget_write(const char* filename, const void* pmin, bool on_device, long lo
     float* vel = pos + 3 * c;
     void* ids = vel + 3 * c;
     if (r == cudaSuccess) {
-      long long blocks = (c + T - 1) / T;
-      if (blocks > 148LL * 8) blocks = 148LL * 8;
       prof_mark(S.st, CG_ST_OTHER);
-      k_gadget_slices<<<(int)blocks, T, 0, S.st>>>(src, c, vfac, use_long_id, pos, vel, ids);
+      k_gadget_slices<<<cg_grid(c, 8), T, 0, S.st>>>(src, c, vfac, use_long_id, pos, vel, ids);
       r = cudaGetLastError();
     }
     if (r == cudaSuccess)

@@ -17,6 +17,13 @@ enum {
 // records a CUDA event on the launch stream.
 void prof_mark(cudaStream_t st, int stage);
 
+// Streaming multiprocessors of the current device (queried once per device).
+int cg_sm_count();
+// Grid of a grid-stride kernel of CG_THREADS threads over n items: one CTA
+// per CG_THREADS items, at most per_sm CTAs for every SM of the device.
+int cg_grid(long long n, int per_sm);
+inline int grid_for(long long n) { return cg_grid(n, 16); }
+
 // Device error word bits (set by kernels, read by the host after a step).
 enum {
   CG_ERR_BAD_CELL = 1,      // a particle's y or z cell index was negative

@@ -29,14 +29,6 @@ namespace {
 constexpr int T = CG_THREADS;
 constexpr double kUlp48 = 1.0 / 281474976710656.0;   // 2^-48
 
-int grid_for(long long n) {
-  long long b = (n + T - 1) / T;
-  const long long cap = 148LL * 16;
-  if (b > cap) b = cap;
-  if (b < 1) b = 1;
-  return (int)b;
-}
-
 // ------------------------------------------------------------- RANLUX-48
 // Luscher's RANLUX in 48-bit form: x_k = x_{k-5} - x_{k-12} - c (mod 1) on
 // 12 words held as doubles in [0,1); 202 steps per block of 12 delivered

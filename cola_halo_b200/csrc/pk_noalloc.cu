@@ -1,18 +1,22 @@
 // Power-spectrum shell sums that allocate nothing.
 //
 // Some callers cannot allocate device memory at the point where they want a
-// power spectrum: code running inside a memory pool or arena that owns the
-// whole device, a stream-ordered pipeline that must not call cudaMalloc
-// (which synchronises the device), or a host program that has handed every
-// byte of HBM to its meshes.  cg_pk_bins_noalloc bins a half spectrum they
-// already hold in device memory using a fixed scratch array compiled into
-// this library instead of any allocation.
+// power spectrum: code running inside a memory pool or arena that has taken
+// the whole device, or a host program that has handed every byte of HBM to
+// its meshes, where a cudaMalloc would fail or steal memory the pool owns.
+// cg_pk_bins_noalloc bins a half spectrum they already hold in device memory
+// using a fixed scratch array compiled into this library instead of any
+// allocation.  The call is synchronous on the caller's stream: it copies the
+// bin sums into the caller's host arrays and waits for them.
 //
 // Scratch: g_pk_scratch, a file-scope __device__ array of 3 x
 // CG_PK_NOALLOC_MAX_BINS doubles (24 KiB), present on every GPU that loads
 // the library until the process exits.  Host code cannot use the symbol as
-// a device address; the address is looked up once per device with
-// cudaGetSymbolAddress on the first call made with that device current.
+// a device address; the address is looked up with cudaGetSymbolAddress on
+// the first call made with a device current, and again whenever that
+// device's context has changed since (after cudaDeviceReset, the old
+// address no longer belongs to the current context).
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdio.h>
@@ -28,7 +32,38 @@ static __device__ __align__(256) double g_pk_scratch[3 * CG_PK_NOALLOC_MAX_BINS]
 
 constexpr int T = CG_THREADS;
 constexpr int kMaxDevices = 64;
+// per device: the scratch address and the id of the context it belongs to
 double* g_scratch_addr[kMaxDevices] = {};
+unsigned long long g_scratch_ctx[kMaxDevices] = {};
+
+// Id of the current context (unique for the life of the process), or 0 when
+// the driver does not report one.  The runtime makes the primary context
+// current before this is called (cudaGetDevice / cudaFree-free set-up).
+unsigned long long current_context_id() {
+  typedef CUresult (*GetCur)(CUcontext*);
+  typedef CUresult (*GetId)(CUcontext, unsigned long long*);
+  static GetCur get_cur = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      f = nullptr;
+    return reinterpret_cast<GetCur>(f);
+  }();
+  static GetId get_id = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      f = nullptr;
+    return reinterpret_cast<GetId>(f);
+  }();
+  CUcontext c = nullptr;
+  unsigned long long id = 0;
+  if (!get_cur || !get_id || get_cur(&c) != CUDA_SUCCESS || !c || get_id(c, &id) != CUDA_SUCCESS)
+    return 0;
+  return id;
+}
 
 // Same binning as the PM power spectrum (pm_kernels.cu k_pk_bin), for the
 // half-spectrum layout spec[kx][ky][kz], kz = 0..N/2 fastest.
@@ -91,23 +126,26 @@ extern "C" int cg_pk_bins_noalloc(const void* d_spec, int n, float boxsize, int 
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess || dev < 0 || dev >= kMaxDevices)
     return cg_set_error_from_lpt(CG_ECUDA, "cg_pk_bins_noalloc: no current device");
-  if (!g_scratch_addr[dev]) {
-    // one-time set-up on this device: the device address of the scratch
+  // set-up, once per device and context: the device address of the scratch.
+  // cudaGetSymbolAddress also makes the runtime's context current, so the
+  // context id is read after it on the first call.
+  unsigned long long ctx = g_scratch_addr[dev] ? current_context_id() : 0;
+  if (!g_scratch_addr[dev] || ctx != g_scratch_ctx[dev]) {
     void* ptr = nullptr;
     e = cudaGetSymbolAddress(&ptr, g_pk_scratch);
     if (e != cudaSuccess || !ptr)
       return cg_set_error_from_lpt(CG_ECUDA, "cg_pk_bins_noalloc: cudaGetSymbolAddress failed");
     g_scratch_addr[dev] = static_cast<double*>(ptr);
+    g_scratch_ctx[dev] = current_context_id();
   }
   double* acc = g_scratch_addr[dev];
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   // the scratch keeps the previous call's sums: clear what must start at 0
   e = cudaMemsetAsync(acc, 0, sizeof(double) * 3 * nbins, st);
   if (e != cudaSuccess) return cg_set_error_from_lpt(CG_ECUDA, "cg_pk_bins_noalloc: memset");
-  long long blocks = ((long long)n * n * (n / 2 + 1) + T - 1) / T;
-  if (blocks > 148LL * 8) blocks = 148LL * 8;
+  const int blocks = cg_grid((long long)n * n * (n / 2 + 1), 8);
   prof_mark(st, CG_ST_OTHER);
-  k_pk_bin_xyz<<<(int)blocks, T, sizeof(double) * 3 * nbins, st>>>(
+  k_pk_bin_xyz<<<blocks, T, sizeof(double) * 3 * nbins, st>>>(
       static_cast<const float2*>(d_spec), n, nbins, flags & CG_PK_DECONVOLVE_CIC, acc);
   e = cudaGetLastError();
   // sums straight into the caller's arrays: nmodes <- sum w, k <- sum w|n|,

@@ -29,6 +29,7 @@
 #include <string.h>
 
 #include <map>
+#include <type_traits>
 #include <vector>
 #include <mutex>
 
@@ -370,8 +371,12 @@ __host__ __device__ constexpr int fx_rm(int N, int v) {
 // Re Z_0 + Im Z_0, accumulated in double.
 // RESET: once its lines are in shared memory, the CTA writes them back as
 // -1, the value the next deposit starts from, so that no fill pass is needed.
+// The RESET form writes the mesh it reads, so its pointer is neither const
+// nor __restrict__ there.
+template <bool RESET> using DensPtr = typename std::conditional<RESET, float*, const float*>::type;
+
 template <int N, bool RESET>
-__global__ void __launch_bounds__(T) k_fz(const float* __restrict__ dens,
+__global__ void __launch_bounds__(T) k_fz(DensPtr<RESET> dens,
                                           float2* __restrict__ spec,
                                           const float2* __restrict__ twH,
                                           const float2* __restrict__ twN,
@@ -386,7 +391,7 @@ __global__ void __launch_bounds__(T) k_fz(const float* __restrict__ dens,
   cgfft::fft_io<H, TY, T, true, -1>(gin, mid, mid, twH);
   if constexpr (RESET) {
     __syncthreads();    // every thread's loads of the lines are done
-    float4* line = reinterpret_cast<float4*>(const_cast<float*>(dens) + ((size_t)x * N + y0) * N);
+    float4* line = reinterpret_cast<float4*>(dens + ((size_t)x * N + y0) * N);
     for (int i = threadIdx.x; i < TY * N / 4; i += T) line[i] = make_float4(-1.f, -1.f, -1.f, -1.f);
   }
   double acc = 0.0;
@@ -780,7 +785,7 @@ __global__ void __launch_bounds__(T) k_pk_bin(const float2* __restrict__ spec, i
 // ------------------------------------------------------- dispatch table
 struct MeshKernels {
   void (*fz)(const float*, float2*, const float2*, const float2*, double*);
-  void (*fz_reset)(const float*, float2*, const float2*, const float2*, double*);
+  void (*fz_reset)(float*, float2*, const float2*, const float2*, double*);
   void (*fyf)(float2*, const float2*);
   void (*fyi)(float2*, const float2*);
   void (*fxf)(const float2*, float2*, const float2*, const float*);
@@ -908,14 +913,6 @@ void twiddle_table(float2* h, int L) {
     const double a = -2.0 * 3.14159265358979323846264338327950288 * (double)k / (double)L;
     h[k] = make_float2((float)cos(a), (float)sin(a));
   }
-}
-
-int grid_for(long long n) {
-  long long b = (n + T - 1) / T;
-  const long long cap = 148LL * 16;   // 16 resident CTAs of 256 threads per SM
-  if (b > cap) b = cap;
-  if (b < 1) b = 1;
-  return (int)b;
 }
 
 }  // namespace
@@ -1257,8 +1254,10 @@ cudaError_t pm_r2c(PmPlan* p, cudaStream_t st) {
   const int N = p->N;
   cudaMemsetAsync(p->dsum, 0, sizeof(double), st);
   prof_mark(st, CG_ST_FZ);
-  (p->keep_dens ? k.fz : k.fz_reset)<<<dim3(N / TY, N), T, k.sm_fz, st>>>(p->dens, p->spec,
-                                                                            p->twH, p->twN, p->dsum);
+  if (p->keep_dens)
+    k.fz<<<dim3(N / TY, N), T, k.sm_fz, st>>>(p->dens, p->spec, p->twH, p->twN, p->dsum);
+  else
+    k.fz_reset<<<dim3(N / TY, N), T, k.sm_fz, st>>>(p->dens, p->spec, p->twH, p->twN, p->dsum);
   p->dens_reset = !p->keep_dens;
   prof_mark(st, CG_ST_FX_FWD);
   k.fxf<<<dim3(N / k.tk, N / 2 + 1), T, k.sm_fx, st>>>(p->spec, p->spec, p->twN, nullptr);

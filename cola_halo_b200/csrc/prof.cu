@@ -42,6 +42,29 @@ void prof_mark(cudaStream_t st, int stage) {
   g_prof.last = st;
 }
 
+int cg_sm_count() {
+  static std::atomic<int> cache[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) return 1;
+  if (dev < 64) {
+    const int c = cache[dev].load(std::memory_order_relaxed);
+    if (c > 0) return c;
+  }
+  int sms = 0;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1)
+    sms = 1;
+  if (dev < 64) cache[dev].store(sms, std::memory_order_relaxed);
+  return sms;
+}
+
+int cg_grid(long long n, int per_sm) {
+  long long b = (n + CG_THREADS - 1) / CG_THREADS;
+  const long long cap = (long long)cg_sm_count() * per_sm;
+  if (b > cap) b = cap;
+  if (b < 1) b = 1;
+  return (int)b;
+}
+
 extern "C" long long cg_launch_count(void) { return g_launches.load(); }
 
 extern "C" const char* cg_stage_name(int stage) {

@@ -22,14 +22,6 @@ namespace {
 
 constexpr int T = CG_THREADS;
 
-int grid_for(long long n) {
-  long long b = (n + T - 1) / T;
-  const long long cap = 148LL * 16;
-  if (b > cap) b = cap;
-  if (b < 1) b = 1;
-  return (int)b;
-}
-
 struct P3 { float* p[3]; };
 struct C3 { const float* p[3]; };
 

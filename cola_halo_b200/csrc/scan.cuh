@@ -76,8 +76,7 @@ inline void exclusive(const unsigned* in, unsigned* out, long long n, unsigned* 
     if (total) cudaMemsetAsync(total, 0, sizeof(unsigned), st);
     return;
   }
-  long long add_blocks = (n + CG_THREADS - 1) / CG_THREADS;
-  if (add_blocks > 148LL * 16) add_blocks = 148LL * 16;
+  const int add_blocks = cg_grid(n, 16);
   prof_mark(st, stage);
   k_scan_blocks<<<(unsigned)nb, SCAN_B, 0, st>>>(in, out, n, bsum);
   prof_mark(st, stage);

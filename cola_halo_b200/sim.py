@@ -76,6 +76,11 @@ class Simulation:
         _lib.check(self.lib.cg_sim_get_mesh(self.h, which, out.ctypes.data), "cg_sim_get_mesh")
         return out
 
+    def keep_density(self, keep=True):
+        """Keep the density the force step used (get_mesh(0) then returns it);
+        by default the force step resets the mesh for the next deposit."""
+        _lib.check(self.lib.cg_sim_keep_density(self.h, 1 if keep else 0), "cg_sim_keep_density")
+
     def power_spectrum(self, nbins=None, deconvolve_cic=False, subtract_shot=False):
         """(k, P(k), modes) of the current positions' CIC density."""
         nb = nbins or self.ngrid // 2

@@ -147,9 +147,9 @@ int cg_sim_power_spectrum(cg_sim* s, int nbins, int flags, double* k, double* pk
 /* The shell sums of cg_sim_power_spectrum for a half spectrum the caller
  * already holds in device memory, without allocating anything (no reference
  * counterpart).  For callers that cannot allocate device memory where they
- * measure P(k): a caller whose memory pool or arena owns the whole device, a
- * stream-ordered pipeline that must not call cudaMalloc (it synchronises the
- * device), or a program that has given all of HBM to its meshes.
+ * measure P(k): a caller whose memory pool or arena owns the whole device,
+ * or a program that has given all of HBM to its meshes, where cudaMalloc
+ * would fail or take memory the pool counts as its own.
  * d_spec: device, n*n*(n/2+1) interleaved complex [x][y][kz], unnormalised
  * r2c of delta (the cg_fft_r2c layout); n even.  Same bins, flags and units
  * as cg_sim_power_spectrum; np is the particle count for
@@ -160,13 +160,23 @@ int cg_sim_power_spectrum(cg_sim* s, int nbins, int flags, double* k, double* pk
  * on a device shares that one array, so calls that overlap (from two host
  * threads, or on two streams at once) race and must not be made.  The first
  * call on each device, made with that device current, looks the array's
- * device address up; make it before any stream capture. */
+ * device address up; make it before any stream capture.  A later call looks
+ * it up again if the device's context has changed (cudaDeviceReset). */
 #define CG_PK_NOALLOC_MAX_BINS 1024
 int cg_pk_bins_noalloc(const void* d_spec, int n, float boxsize, int nbins, int flags,
                        double* k, double* pk, double* nmodes, long long np, void* stream);
 /* Copy one mesh to host: which = 0 density (delta), 1..3 force x, y, z;
- * ngrid^3 floats, [x][y][z] order. */
+ * ngrid^3 floats, [x][y][z] order.  The force step's z transform resets the
+ * density mesh to -1 for the next deposit, so after cg_sim_forces (unless
+ * the handle keeps its density, cg_sim_keep_density) which = 0 deposits the
+ * particles' CURRENT positions again: after a kick/drift that is not the
+ * density behind the force meshes 1..3 of the same step. */
 int cg_sim_get_mesh(cg_sim* s, int which, float* out);
+/* keep = 1: the force step leaves the density mesh in place (its z transform
+ * does not reset it), so cg_sim_get_mesh(s, 0, ..) returns the density the
+ * last force step used; the next deposit then fills the mesh with -1 first
+ * (one more pass over the mesh).  keep = 0 (the default): the reset. */
+int cg_sim_keep_density(cg_sim* s, int keep);
 /* The CUDA stream (cudaStream_t) the handle queues its work on. */
 void* cg_sim_stream(cg_sim* s);
 

@@ -16,9 +16,12 @@ LIB_PATH = os.path.join(HERE, "_ref", "libcolaref.so")
 _lib = None
 
 
-def build(ref_dir="/root/reference"):
-    """Compile the reference (needs its sources; they are not on GPU hosts)."""
-    if not os.path.isdir(ref_dir):
+def build(ref_dir=None):
+    """Compile the reference from its sources in ref_dir (default: the
+    COLA_REF_DIR environment variable).  Without the sources (GPU hosts) the
+    prebuilt library is used if present."""
+    ref_dir = ref_dir or os.environ.get("COLA_REF_DIR")
+    if not ref_dir or not os.path.isdir(ref_dir):
         return os.path.exists(LIB_PATH)
     subprocess.run(["make", "-s", "-C", HERE, "REF=" + ref_dir], check=True)
     return True

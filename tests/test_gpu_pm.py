@@ -77,3 +77,41 @@ def test_single_particle_mass(gpu_lib):
         assert abs((d + 1.0).sum() - factor ** 3) < 1e-4
         want = R.cic_deposit(np.array([xyz], dtype=np.float32), N, L, factor)
         assert np.abs(d - want).max() < 1e-6
+
+
+def test_reset_then_deposit_matches_kept_density(gpu_lib, bbks_table):
+    """The force step's z transform leaves -1 in the density mesh and the next
+    deposit skips its fill: two force steps in a row (with a kick and drift in
+    between) give the same forces as a handle that keeps its density and
+    fills before every deposit, and both match the oracle."""
+    from cola_halo_b200 import Simulation
+    nc, factor, L = 16, 3, 100.0
+    N = nc * factor
+    p = lattice_particles(nc, L, 77, OM, 0.2, bbks_table)
+    runs = []
+    for keep in (False, True):
+        sim = Simulation(nc, N, L, OM)
+        if keep:
+            sim.keep_density(True)
+        sim.set_particles(p, 0.2, 0.2)
+        sim.move()
+        sim.forces()
+        sim.kick(0.25)
+        sim.drift(0.3)
+        sim.move()
+        sim.forces()
+        runs.append((sim.get_forces(), sim.get_particles()["x"]))
+        if keep:
+            # the kept mesh is the density of the second force step
+            d = sim.get_mesh(0)
+            _, dens = R.pm_calculate_forces(runs[-1][1], N, L, factor)
+            assert np.abs(d - dens).max() < 2e-5 * max(1.0, np.abs(dens).max())
+        sim.close()
+    (f0, x0), (f1, x1) = runs
+    # float atomics: the deposits add in different orders, so the first
+    # step's forces, and the positions they drift to, agree to rounding
+    assert np.abs(x0 - x1).max() < 1e-6 * L
+    scale = np.abs(f1).max()
+    assert np.abs(f0 - f1).max() < 1e-5 * scale
+    fo, _ = R.pm_calculate_forces(x0, N, L, factor)
+    assert np.abs(f0 - fo).max() < 2e-5 * scale
