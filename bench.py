@@ -212,12 +212,52 @@ def load_traffic():
         return {}
 
 
+def _ref_cola_timers(lib):
+    """The reference's own timer breakdown of the COLA category (timer.c:62-83,
+    timer_print), read from what timer_print writes to stdout: seconds per
+    subcategory (fft, assign, force_mesh, pforce, check, comm, evolve).  The
+    timers accumulate over the process; callers difference two readings."""
+    import re
+    fd, path = tempfile.mkstemp()
+    sys.stdout.flush()
+    saved = os.dup(1)
+    try:
+        os.dup2(fd, 1)
+        lib.msg_set_loglevel(3)          # info
+        lib.timer_print()
+        lib.msg_set_loglevel(7)          # silent again
+    finally:
+        sys.stdout.flush()
+        os.dup2(saved, 1)
+        os.close(saved)
+        os.close(fd)
+    text = open(path).read()
+    os.unlink(path)
+    out, cat = {}, None
+    for line in text.splitlines():
+        m = re.match(r"^(\S+)\s+([0-9.]+)\s", line)
+        if m:
+            cat = m.group(1)
+            if cat == "COLA":
+                out["all"] = float(m.group(2))
+            continue
+        m = re.match(r"^\s+(\S+)\s+([0-9.]+)\s", line)
+        if m and cat == "COLA":
+            out[m.group(1)] = float(m.group(2))
+    lib.timer_set_category(2)            # timer_print leaves the Init category; back to COLA
+    return out
+
+
 def cpu_reference_step_time(cfg, parts_aos, table, steps=1, warmup=0):
     """Time the reference's own CPU code (oracle/_ref: pm.c, cola.c, move.c
     built unchanged against the project's MPI/FFTW/GSL shims) for `steps`
-    COLA steps after `warmup` untimed ones.  parts_aos: initial particles
+    COLA steps of the schedule, starting from the initial particles, after
+    `warmup` untimed steps that are then undone (the particles are put back
+    to the initial conditions), so the timed steps are steps 1..`steps` of a
+    realization, as the GPU arm's are.  parts_aos: initial particles
     (reference Particle layout), or None to generate them with the
-    reference's own lpt.c.  Returns (seconds per step, cores)."""
+    reference's own lpt.c.  Returns (seconds per step, cores, the reference's
+    timer breakdown of the timed steps in seconds)."""
     from cola_halo_b200.schedule import Schedule
     from cola_halo_b200.types import HostParticles
     from oracle import ref
@@ -236,6 +276,8 @@ def cpu_reference_step_time(cfg, parts_aos, table, steps=1, warmup=0):
         hp.struct.np_local = nc ** 3
         hp.struct.a_x = sched.a_init
     hp.struct.a_v = sched.a_init
+    ics = hp.p[: nc ** 3].copy()
+    lib.timer_set_category(2)            # COLA (timer.h)
 
     def one(i):
         _, _, avel1, apos1 = sched.times(i % (sched.nloop - 1) + 1)
@@ -245,12 +287,20 @@ def cpu_reference_step_time(cfg, parts_aos, table, steps=1, warmup=0):
         lib.cola_drift(hp.ptr, om, apos1)
     for i in range(warmup):
         one(i)
+    if warmup:
+        hp.p[: nc ** 3] = ics
+        hp.struct.np_local = nc ** 3
+        hp.struct.a_x = sched.a_init
+        hp.struct.a_v = sched.a_init
+    t_before = _ref_cola_timers(lib)
     t0 = time.perf_counter()
     for i in range(steps):
-        one(warmup + i)
+        one(i)
     dt = (time.perf_counter() - t0) / steps
+    t_after = _ref_cola_timers(lib)
+    breakdown = {k: round(t_after[k] - t_before.get(k, 0.0), 3) for k in t_after}
     cores = len(os.sched_getaffinity(0))
-    return dt, cores
+    return dt, cores, breakdown
 
 
 # --------------------------------------------------------------- reference arm
@@ -270,20 +320,32 @@ def run_reference(args, cfg):
         print(json.dumps(dict(base, unavailable="reference build missing: %s" % e)))
         return 0
     table = write_bbks_table(os.path.join(tempfile.mkdtemp(), "bbks.dat"))
-    k_ref = max(1, min(args.steps, 3))
+    # one whole realization: the timed steps are steps 1..nsteps of the
+    # schedule, the same step indices the GPU arm averages over
+    nsteps = cfg["nsteps"]
+    k_ref = max(1, min(args.steps, nsteps))
     w_ref = min(args.warmup, 1)
-    dt, cores = cpu_reference_step_time(cfg, None, table, steps=k_ref, warmup=w_ref)
+    dt, cores, timers = cpu_reference_step_time(cfg, None, table, steps=k_ref, warmup=w_ref)
     value = npart / dt
+    fft_share = (timers.get("fft", 0.0) / timers["all"]) if timers.get("all") else None
     out = dict(base, value=value, n_gpus=args.gpus, steps=k_ref, warmup=w_ref,
                ms_per_step=dt * 1e3, scaling="weak", vs_baseline=None, dtype="f32",
                data="synthetic (seeded 2LPT initial conditions, BBKS P(k))",
                config=dict(workload=args.config_desc, particles=npart,
                            mesh=cfg["nc"] * cfg["factor"], boxsize=cfg["L"],
+                           steps_timed="steps 1..%d of the %d-step schedule (z = 49 -> 0), "
+                                       "from the 2LPT initial conditions" % (k_ref, nsteps),
                            parallelism="1 host, %d OpenMP threads" % cores),
+               reference_timers_s=timers,
+               reference_fft_share=fft_share,
                cpu_baseline={"value": value, "unit": "particle-steps/s", "cores": cores,
                              "kind": "reference",
-                             "sample": "%d COLA step(s) of the %s workload after %d warm-up; "
-                                       "shim-FFT, not FFTW" % (k_ref, args.config, w_ref)},
+                             "sample": "steps 1..%d of one realization of the %s workload "
+                                       "after %d warm-up step (undone); the reference's FFT "
+                                       "is the project's double-precision shim, not FFTW "
+                                       "(its share of the step time: %s)"
+                                       % (k_ref, args.config, w_ref,
+                                          "%.0f%%" % (100 * fft_share) if fft_share else "n/a")},
                e2e={"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0})
     print(json.dumps(out))
@@ -487,11 +549,13 @@ def run_b200(args, cfg):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            dt, cores = cpu_reference_step_time(cfg, ics, table, steps=1)
+            dt, cores, timers = cpu_reference_step_time(cfg, ics, table, steps=2)
             cpu = {"value": npart / dt, "unit": "particle-steps/s", "cores": cores,
                    "kind": "reference",
-                   "sample": "1 COLA step of the %s workload (same 2LPT particles) with the "
-                             "reference pm.c/cola.c/move.c; shim-FFT, not FFTW" % args.config}
+                   "sample": "steps 1-2 of the %s workload's schedule (same 2LPT particles) "
+                             "with the reference pm.c/cola.c/move.c; shim-FFT, not FFTW "
+                             "(fft %.1f s of %.1f s)" % (args.config, timers.get("fft", 0.0),
+                                                         timers.get("all", 0.0))}
         except Exception as e:  # reported, not fatal
             cpu = {"value": None, "unit": "particle-steps/s", "cores": None,
                    "kind": "reference", "sample": "unavailable: %s" % e}

@@ -339,8 +339,10 @@ def cic_deposit(x, ngrid, boxsize, factor):
     mesh = np.zeros(N * N * N, dtype=np.float64)
 
     def put(ix, jy, kz, w, ok):
+        # float64 sums per cell (bincount: the same sums as a sequential
+        # scatter up to float64 rounding, and fast at 768^3)
         idx = (ix[ok] * N + jy[ok]) * N + kz[ok]
-        np.add.at(mesh, idx, w[ok].astype(np.float64))
+        mesh[:] += np.bincount(idx, weights=w[ok].astype(np.float64), minlength=N * N * N)
 
     ok0 = (iI >= 0) & (iI < N)
     ok1 = (I1 >= 0) & (I1 < N)
@@ -644,27 +646,39 @@ def lpt_set_displacement(N, boxsize, seed, omega_m, a_init, power):
 # --------------------------------------------------------------------------
 def power_spectrum(delta, boxsize, nbins=None, deconvolve_cic=False):
     N = delta.shape[0]
-    dk = np.fft.rfftn(delta.astype(np.float64)) / N ** 3
+    try:   # the same float64 transform, on all host threads where scipy has them
+        import scipy.fft
+        dk = scipy.fft.rfftn(delta.astype(np.float64), workers=-1)
+    except ImportError:
+        dk = np.fft.rfftn(delta.astype(np.float64))
+    dk /= N ** 3
     kf = 2 * math.pi / boxsize
     idx = np.arange(N)
     s = np.where(idx <= N // 2, idx, idx - N)
     nz = np.arange(N // 2 + 1)
-    n2 = s[:, None, None] ** 2 + s[None, :, None] ** 2 + nz[None, None, :] ** 2
-    kmag = np.sqrt(n2) * kf
-    p = np.abs(dk) ** 2 * boxsize ** 3
-    if deconvolve_cic:
-        def w(n):
-            x = math.pi * n / N
-            return np.where(n == 0, 1.0, np.sin(x) / np.where(n == 0, 1.0, x)) ** 2
-        p = p / (w(s)[:, None, None] * w(s)[None, :, None] * w(nz)[None, None, :]) ** 2
-    wgt = np.where((nz == 0) | (nz == N // 2), 1.0, 2.0)[None, None, :] * np.ones_like(kmag)
+
+    def w(n):
+        x = math.pi * n / N
+        return np.where(n == 0, 1.0, np.sin(x) / np.where(n == 0, 1.0, x)) ** 2
     if nbins is None:
         nbins = N // 2
-    ib = np.floor(kmag / kf + 0.5).astype(np.int64)   # bin i: |n| in [i-1/2, i+1/2)
-    ok = (ib >= 1) & (ib <= nbins)
-    cnt = np.bincount(ib[ok], weights=wgt[ok], minlength=nbins + 1)[1:]
-    ps = np.bincount(ib[ok], weights=(wgt * p)[ok], minlength=nbins + 1)[1:]
-    ks = np.bincount(ib[ok], weights=(wgt * kmag)[ok], minlength=nbins + 1)[1:]
+    cnt = np.zeros(nbins + 1)
+    ps = np.zeros(nbins + 1)
+    ks = np.zeros(nbins + 1)
+    # one kx plane at a time (bounded memory at 768^3)
+    for i in range(N):
+        n2 = s[i] ** 2 + s[:, None] ** 2 + nz[None, :] ** 2
+        kmag = np.sqrt(n2) * kf
+        p = np.abs(dk[i]) ** 2 * boxsize ** 3
+        if deconvolve_cic:
+            p = p / (w(s[i]) * w(s)[:, None] * w(nz)[None, :]) ** 2
+        wgt = np.where((nz == 0) | (nz == N // 2), 1.0, 2.0)[None, :] * np.ones_like(kmag)
+        ib = np.floor(kmag / kf + 0.5).astype(np.int64)   # bin i: |n| in [i-1/2, i+1/2)
+        ok = (ib >= 1) & (ib <= nbins)
+        cnt += np.bincount(ib[ok], weights=wgt[ok], minlength=nbins + 1)
+        ps += np.bincount(ib[ok], weights=(wgt * p)[ok], minlength=nbins + 1)
+        ks += np.bincount(ib[ok], weights=(wgt * kmag)[ok], minlength=nbins + 1)
+    cnt, ps, ks = cnt[1:], ps[1:], ks[1:]
     with np.errstate(invalid="ignore", divide="ignore"):
         return ks / cnt, ps / cnt, cnt
 
