@@ -91,6 +91,7 @@ PmPlan view(const PmPlan& bufs, const MeshFFT& tab, int N, int factor, float L) 
   p.mesh_bytes = sizeof(float) * (size_t)N * N * N;
   p.spec_bytes = sizeof(float2) * (size_t)(N / 2 + 1) * N * N;
   p.ztm_ok = false;    // the stream's TMA maps describe its largest mesh, not this one
+  p.zsw_ok = false;
   p.keep_dens = true;  // meshes of several sizes share the buffer: fill every step
   p.dens_reset = false;
   return p;

@@ -206,6 +206,22 @@ template <int L, int B> __host__ __device__ constexpr int col_tile_elems() {
   return L * B + (L * B) / 32 + 1;
 }
 
+// Dense tile of 16 lines stored n-major ([n][b], 128-byte rows of 16
+// complex) as a TMA load with the 128-byte swizzle writes it: the 16-byte
+// chunk c of row n sits at chunk c ^ (n mod 8) (the tile starts on a
+// 1024-byte boundary).  Consecutive threads on consecutive lines at one n
+// touch one 128-byte row: conflict-free; consecutive n of one line fall on
+// 8 distinct chunks per 8 rows: two-way conflicts per half-warp.
+struct SmemSw16 {
+  cplx* s;
+  __device__ __forceinline__ int at(int b, int n) const {
+    return (n << 4) + ((((b >> 1) ^ n) & 7) << 1) + (b & 1);
+  }
+  __device__ __forceinline__ cplx ld(int b, int n) const { return s[at(b, n)]; }
+  __device__ __forceinline__ void st(int b, int n, cplx v) const { s[at(b, n)] = v; }
+  static constexpr bool kShared = true;
+};
+
 // Global lines: element n of line b at p[b * ls + n * es].
 struct Gmem {
   float2* p;
@@ -221,6 +237,17 @@ struct Gmem {
   static constexpr bool kShared = false;
 };
 
+// T = 32: the tile belongs to one warp (thread = lane, barriers are warp
+// barriers), so warps of a CTA run their tiles independently.  Otherwise the
+// tile belongs to the CTA's T threads.
+template <int T> __device__ __forceinline__ void tile_sync() {
+  if constexpr (T == 32) __syncwarp();
+  else __syncthreads();
+}
+template <int T> __device__ __forceinline__ int tile_tid() {
+  return T == 32 ? (int)(threadIdx.x & 31) : (int)threadIdx.x;
+}
+
 template <int L, int R, int NS, int B, int T, bool LINE_MAJOR, int DIR, class In, class Out>
 __device__ __forceinline__ void stage_io(const In& in, const Out& out,
                                          const float2* __restrict__ tw, bool inplace) {
@@ -228,7 +255,7 @@ __device__ __forceinline__ void stage_io(const In& in, const Out& out,
   constexpr int TOTAL = NBF * B;
   constexpr int PER = (TOTAL + T - 1) / T;
   cplx v[PER][R];
-  const int tid = threadIdx.x;
+  const int tid = tile_tid<T>();
 #pragma unroll
   for (int q = 0; q < PER; q++) {
     const int idx = tid + q * T;
@@ -239,7 +266,7 @@ __device__ __forceinline__ void stage_io(const In& in, const Out& out,
       for (int r = 0; r < R; r++) v[q][r] = in.ld(b, j + r * NBF);
     }
   }
-  if (inplace) __syncthreads();
+  if (inplace) tile_sync<T>();
 #pragma unroll
   for (int q = 0; q < PER; q++) {
     const int idx = tid + q * T;
@@ -264,7 +291,8 @@ __device__ __forceinline__ void stage_io(const In& in, const Out& out,
 // Stages S..end of an L-point FFT (maximum radix RM): stage 0 reads `first`,
 // the last stage writes `last`, the stages in between work in place on the
 // shared tile `mid`.  Every stage that writes `mid` is followed by a barrier.
-template <int L, int S, int B, int T, bool LM, int DIR, int RM, class First, class Mid,
+// LML: the thread mapping of the last stage (the others use LM).
+template <int L, int S, int B, int T, bool LM, int DIR, int RM, bool LML, class First, class Mid,
           class Last>
 __device__ __forceinline__ void fft_io_from(const First& first, const Mid& mid, const Last& last,
                                             const float2* __restrict__ tw) {
@@ -273,28 +301,30 @@ __device__ __forceinline__ void fft_io_from(const First& first, const Mid& mid, 
   constexpr int NS = ns_before(L, S, RM);
   if constexpr (S == NSTAGE - 1) {
     if constexpr (S == 0)
-      stage_io<L, R, NS, B, T, LM, DIR>(first, last, tw, First::kShared && Last::kShared);
+      stage_io<L, R, NS, B, T, LML, DIR>(first, last, tw, First::kShared && Last::kShared);
     else
-      stage_io<L, R, NS, B, T, LM, DIR>(mid, last, tw, Last::kShared);
-    if constexpr (Last::kShared) __syncthreads();
+      stage_io<L, R, NS, B, T, LML, DIR>(mid, last, tw, Last::kShared);
+    if constexpr (Last::kShared) tile_sync<T>();
   } else {
     if constexpr (S == 0)
       stage_io<L, R, NS, B, T, LM, DIR>(first, mid, tw, First::kShared);
     else
       stage_io<L, R, NS, B, T, LM, DIR>(mid, mid, tw, true);
-    __syncthreads();
-    fft_io_from<L, S + 1, B, T, LM, DIR, RM>(first, mid, last, tw);
+    tile_sync<T>();
+    fft_io_from<L, S + 1, B, T, LM, DIR, RM, LML>(first, mid, last, tw);
   }
 }
 
 // One L-point FFT of each of the B lines of a tile.  LM: consecutive threads
 // take consecutive butterflies of one line (true) or the same butterfly of
-// consecutive lines (false).  DIR = -1 forward, +1 inverse (unnormalised).
-template <int L, int B, int T, bool LM, int DIR, int RM = 16, class First, class Mid, class Last>
+// consecutive lines (false); LML: the same choice for the last stage alone.
+// DIR = -1 forward, +1 inverse (unnormalised).
+template <int L, int B, int T, bool LM, int DIR, int RM = 16, bool LML = LM, class First,
+          class Mid, class Last>
 __device__ __forceinline__ void fft_io(const First& first, const Mid& mid, const Last& last,
                                        const float2* __restrict__ tw) {
   static_assert(supported_length(L, RM), "FFT length must be 2^a 3^b");
-  fft_io_from<L, 0, B, T, LM, DIR, RM>(first, mid, last, tw);
+  fft_io_from<L, 0, B, T, LM, DIR, RM, LML>(first, mid, last, tw);
 }
 
 }  // namespace cgfft

@@ -68,7 +68,9 @@ struct PmPlan {
                             //   resets it to -1 for the next deposit)
   bool dens_reset;          // dens holds -1 everywhere, not the last density
   CUtensorMap ztm[3];       // TMA maps of gsp[0..2] for the z transform's gather
-  bool ztm_ok;              //   valid (else the cp.async gather runs)
+  bool ztm_ok;              //   valid, landing-area form k_zi_tma
+  bool zsw_ok;              //   valid, swizzled-tile form k_zi_sw (else, with neither,
+                            //   the cp.async gather runs)
 };
 
 // Plain 3-D real transforms on the mesh layouts above (unnormalised, FFTW
@@ -86,9 +88,9 @@ cudaError_t mesh_c2r(const MeshFFT* f, float2* spec, float* real, cudaStream_t s
 
 // Schedule of the FFT passes of one mesh size: which compiled variant of the
 // strided x pass and of the fused Green pass runs (pm_kernels.cu kFxCfg,
-// kGreenCfg).  Variants other than 0 exist from 256 up (Green: up to 768).
+// kGreenCfg).  Variants other than 0 exist from 256 up.
 #define PM_NUM_FX_VARIANTS 3
-#define PM_NUM_GREEN_VARIANTS 3
+#define PM_NUM_GREEN_VARIANTS 4
 struct MeshSched {
   int green = 0;
   int fx = 0;
@@ -96,6 +98,9 @@ struct MeshSched {
 
 // pm_kernels.cu
 bool pm_supported_mesh(int N);
+// Gather of the z c2r for plans created afterwards: -1 by mesh size, 0
+// cp.async, 1 TMA landing area, 2 TMA swizzled tile.  -1 on a bad mode.
+int pm_set_z_gather(int mode);
 // Number of schedule variants compiled for mesh size N (1 below 256).
 int pm_num_variants(int N, int* n_green, int* n_fx);
 MeshSched pm_get_schedule(int N);

@@ -28,6 +28,7 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <atomic>
 #include <map>
 #include <type_traits>
 #include <vector>
@@ -350,12 +351,15 @@ __host__ __device__ constexpr int n_fx_variants(int N) {
   return N >= MIN_TUNED_N ? PM_NUM_FX_VARIANTS : 1;
 }
 __host__ __device__ constexpr int n_green_variants(int N) {
-  return N >= MIN_TUNED_N && N <= 768 ? PM_NUM_GREEN_VARIANTS : 1;
+  return N >= MIN_TUNED_N ? PM_NUM_GREEN_VARIANTS : 1;
 }
 struct FxCfg { int tk, rm; };
+// byg = 0: one line per warp (k_green_w), rm its maximum radix, minb its
+// warps per CTA
 struct GreenCfg { int byg, rm, minb; };
 constexpr FxCfg kFxCfg[PM_NUM_FX_VARIANTS] = {{8, 0}, {8, -1}, {16, 16}};
-constexpr GreenCfg kGreenCfg[PM_NUM_GREEN_VARIANTS] = {{4, 16, 3}, {8, 8, 2}, {8, 16, 2}};
+constexpr GreenCfg kGreenCfg[PM_NUM_GREEN_VARIANTS] = {
+    {4, 16, 3}, {8, 8, 2}, {8, 16, 2}, {0, 8, 4}};
 __host__ __device__ constexpr int rm_x_default(int N) { return N >= 768 ? 8 : 16; }
 __host__ __device__ constexpr int fx_rm(int N, int v) {
   return kFxCfg[v].rm == 0 ? rm_x_default(N)
@@ -441,10 +445,18 @@ struct GmemScaled {
   static constexpr bool kShared = false;
 };
 
+// One x-pass transform as a separate (not inlined) call, so that two of
+// them in one kernel keep separate register live ranges.
+template <int N, int TKV, int DIR, int RMX, class First, class Mid, class Last>
+__device__ __noinline__ void fft_col_x(const First f, const Mid m, const Last l,
+                                       const float2* __restrict__ tw) {
+  cgfft::fft_io<N, TKV, T, false, DIR, RMX>(f, m, l, tw);
+}
+
 // FX: c2c along kx (stride N), TKV ky columns per CTA, from `in` to `out`
 // (the same array for an in-place pass).  SCALE 0: plain; 1 / 2: the input
 // is first multiplied by n_x / n_z (GmemScaled; gtab: the gradient table or
-// NULL, unused by SCALE 0).
+// NULL, unused by SCALE 0); 3: both, n_x into `out` and n_z in place.
 template <int N, int DIR, int SCALE, int TKV, int RMX>
 __global__ void __launch_bounds__(T) k_fx(const float2* in, float2* out,
                                           const float2* __restrict__ twN,
@@ -456,6 +468,17 @@ __global__ void __launch_bounds__(T) k_fx(const float2* in, float2* out,
   if constexpr (SCALE == 0) {
     const Gmem gi{const_cast<float2*>(in) + off, 1, (size_t)N};
     cgfft::fft_io<N, TKV, T, false, DIR, RMX>(gi, mid, go, twN);
+  } else if constexpr (SCALE == 3) {
+    // the x and z components from the one shared spectrum: n_x in -> out,
+    // then n_z in -> in (the tile's second read comes from L2, so the
+    // spectrum crosses HBM once for both components)
+    const GmemScaled<1> gx{in + off, (size_t)N, N, 0.0f, gtab};
+    fft_col_x<N, TKV, DIR, RMX>(gx, mid, go, twN);
+    __syncthreads();   // the tile buffer is reused
+    const float fz = gtab ? __ldg(gtab + blockIdx.y) : (float)blockIdx.y;
+    const GmemScaled<2> gz{in + off, (size_t)N, N, fz, gtab};
+    const Gmem gzo{const_cast<float2*>(in) + off, 1, (size_t)N};
+    fft_col_x<N, TKV, DIR, RMX>(gz, mid, gzo, twN);
   } else {
     const float fz = SCALE == 2 && gtab ? __ldg(gtab + blockIdx.y) : (float)blockIdx.y;
     const GmemScaled<SCALE> gi{in + off, (size_t)N, N, fz, gtab};
@@ -577,6 +600,47 @@ __global__ void __launch_bounds__(T, MINB) k_green(const float2* __restrict__ sp
   __syncthreads();
   const Gmem os{g2 + off, (size_t)N, 1};
   fft_tile_y<N, BG, RMG, 1>(d, d, os, twN);
+}
+
+// GREEN with one y line per warp: the same three transforms and the same
+// arithmetic as k_green, but every warp owns its line (two padded line
+// buffers of its own) and synchronises only with itself, so the warps of a
+// CTA never wait for one another between stages.  Grid-stride over the
+// (N/2+1) N lines; radices up to RMW (768 = 8 8 4 3, so every stage keeps
+// all 32 lanes busy).
+template <int N, int RMW, int DIR, class First, class Mid, class Last>
+__device__ __noinline__ void fft_line_w(const First f, const Mid m, const Last l,
+                                        const float2* __restrict__ tw) {
+  cgfft::fft_io<N, 1, 32, true, DIR, RMW>(f, m, l, tw);
+}
+
+template <int N, int WPC, int RMW, bool MODS>
+__global__ void __launch_bounds__(32 * WPC) k_green_w(const float2* __restrict__ spec,
+                                                       float2* __restrict__ g1,
+                                                       float2* __restrict__ g2,
+                                                       const float2* __restrict__ twN,
+                                                       float f1, GreenMods gm) {
+  constexpr int P = cgfft::line_pitch<N>();
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const int warp = (int)(threadIdx.x >> 5);
+  cplx* D = reinterpret_cast<cplx*>(smraw) + (size_t)warp * 2 * P;
+  cplx* W = D + P;
+  const SmemLine<P> d{D}, w{W};
+  const size_t nlines = (size_t)(N / 2 + 1) * N;
+  for (size_t l = (size_t)blockIdx.x * WPC + warp; l < nlines; l += (size_t)gridDim.x * WPC) {
+    const int kz = (int)(l / N), kx = (int)(l % N);
+    const size_t off = l * N;
+    const Gmem gin{const_cast<float2*>(spec) + off, (size_t)N, 1};
+    fft_line_w<N, RMW, -1>(gin, d, d, twN);
+    // the y component's load also leaves the shared x/z value in D
+    const GreenLoad<P, 2, MODS> gy{D, kz, kx, N, f1, gm};
+    const Gmem oy{g1 + off, (size_t)N, 1};
+    fft_line_w<N, RMW, 1>(gy, w, oy, twN);
+    __syncwarp();
+    const Gmem os{g2 + off, (size_t)N, 1};
+    fft_line_w<N, RMW, 1>(d, d, os, twN);
+    __syncwarp();   // the next line's first stage overwrites D
+  }
 }
 
 // ZI: c2r along z of S (lines (x, y0..y0+TY-1) per CTA) into R.  The
@@ -723,16 +787,128 @@ __global__ void __launch_bounds__(T, 2) k_zi_tma(const __grid_constant__ CUtenso
   cgfft::fft_io<H, TY, T, true, 1>(mid, mid, gout, twH);
 }
 
-// TMA gather of the z transform by mesh size: measured alone, it is faster
-// up to 384^3 (256^3: 0.037 vs 0.039 ms, 384^3: 0.114 vs 0.124 ms) and slower
-// beyond (512^3: 0.262 vs 0.249, 768^3: 1.10 vs 0.97), where its landing
-// area halves the resident CTAs.  COLAGPU_ZI_TMA=0 / 1 overrides.
-bool zi_tma_default(int N) {
+// ZI with the transposed gather landing straight in the transform's tile:
+// the tile is dense, n-major ([kz][b], 128-byte rows of TY = 16 complex),
+// written by tiled tensor loads with the 128-byte swizzle (cgfft::SmemSw16
+// undoes it), so no padded copy is needed and the CTA holds one tile only
+// ((N/2+1) x 128 B rounded up to whole boxes: 51 KB at 768^3, four CTAs per
+// SM).  ZSW_NB boxes of ZSW_KR rows (a multiple of 8, so every box starts on
+// a 1024-byte boundary of the tile; rows past N/2 are filled with zeros and
+// never read).  The half-complex combination runs in place on the tile, the
+// inner stages map consecutive threads to consecutive lines (conflict-free
+// on the swizzled rows) and the last stage to consecutive butterflies of a
+// line (coalesced stores).  Same arithmetic as k_zi; bounded wait, error
+// word CG_ERR_TMA_WAIT on a timeout.
+template <int N> __host__ __device__ constexpr int zsw_nbox() { return (N / 2 + 1 + 255) / 256; }
+template <int N> __host__ __device__ constexpr int zsw_krows() {
+  return ((N / 2 + 1 + zsw_nbox<N>() - 1) / zsw_nbox<N>() + 7) / 8 * 8;
+}
+template <int N> __host__ __device__ constexpr size_t zsw_smem() {
+  return (size_t)128 * zsw_nbox<N>() * zsw_krows<N>() + 1024 + 16;   // + alignment, mbarrier
+}
+
+template <int N>
+__global__ void __launch_bounds__(T, N >= 1024 ? 3 : 4) k_zi_sw(const __grid_constant__ CUtensorMap tm,
+                                             float* __restrict__ out,
+                                             const float2* __restrict__ twH,
+                                             const float2* __restrict__ twN,
+                                             unsigned* __restrict__ err) {
+  static_assert(TY == 16, "the swizzled tile holds 16 lines per 128-byte row");
+  constexpr int H = N / 2;
+  constexpr int KR = zsw_krows<N>(), NB = zsw_nbox<N>();
+  constexpr unsigned kBytes = 128u * NB * KR;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  unsigned char* base =
+      smraw + ((1024u - ((unsigned)__cvta_generic_to_shared(smraw) & 1023u)) & 1023u);
+  const cgfft::SmemSw16 t{reinterpret_cast<cplx*>(base)};
+  const unsigned bar = (unsigned)__cvta_generic_to_shared(base + kBytes);
+  const int x = blockIdx.y;
+  const int y0 = blockIdx.x * TY;
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(bar) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar),
+                 "r"(kBytes) : "memory");
+    const unsigned dst0 = (unsigned)__cvta_generic_to_shared(base);
+#pragma unroll
+    for (int h = 0; h < NB; h++) {
+      asm volatile(
+          "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
+          " [%0], [%1, {%2, %3, %4}], [%5];\n" ::"r"(dst0 + 128u * KR * h),
+          "l"(reinterpret_cast<unsigned long long>(&tm)), "r"(2 * y0), "r"(x), "r"(h * KR),
+          "r"(bar)
+          : "memory");
+    }
+  }
+  unsigned done = 0;
+  for (int it = 0; it < (1 << 22) && !done; it++) {
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done) : "r"(bar) : "memory");
+  }
+  if (!done) {
+    if (threadIdx.x == 0) atomicOr(err, (unsigned)CG_ERR_TMA_WAIT);
+    return;
+  }
+  // half-complex combination, rows k and H - k of every line, in place
+  for (int idx = threadIdx.x; idx < (H / 2 + 1) * TY; idx += T) {
+    const int b = idx % TY, k = idx / TY;
+    if (k == 0) {
+      const float x0 = t.ld(b, 0).x, xh = t.ld(b, H).x;
+      t.st(b, 0, cplx{x0 + xh, x0 - xh});
+    } else {
+      const int k2 = H - k;
+      const cplx a = t.ld(b, k), c = t.ld(b, k2);
+      const float2 wa = __ldg(twN + k), wc = __ldg(twN + k2);
+      const cplx sa = {a.x + c.x, a.y - c.y}, da = {a.x - c.x, a.y + c.y};
+      const cplx ra = {da.x * wa.x + da.y * wa.y, da.y * wa.x - da.x * wa.y};
+      const cplx za = {sa.x - ra.y, sa.y + ra.x};
+      const cplx sc = {c.x + a.x, c.y - a.y}, dc = {c.x - a.x, c.y + a.y};
+      const cplx rc = {dc.x * wc.x + dc.y * wc.y, dc.y * wc.x - dc.x * wc.y};
+      const cplx zc = {sc.x - rc.y, sc.y + rc.x};
+      t.st(b, k, za);
+      if (k2 != k) t.st(b, k2, zc);
+    }
+  }
+  __syncthreads();
+  const Gmem gout{reinterpret_cast<float2*>(out) + ((size_t)x * N + y0) * H, (size_t)H, 1};
+  cgfft::fft_io<H, TY, T, false, 1, 16, true>(t, t, gout, twH);
+}
+
+// Gather of the z c2r by mesh size (the plans created afterwards):
+//   0  cp.async (k_zi)
+//   1  TMA into a landing area, copied into the padded tile (k_zi_tma)
+//   2  TMA into the swizzled dense tile itself (k_zi_sw)
+// All three give bit-identical output.  Default: 2, the fastest at 384^3
+// (0.313 ms per launch against 0.344 and 0.373 for 1 and 0) and at 768^3
+// (0.81 ms against 1.15 and 0.97), per launch inside the 10-step runs;
+// cg_set_z_gather, or COLAGPU_ZI=0/1/2, selects one.
+std::atomic<int> g_zmode{-1};
+
+int z_gather_mode(int N, bool* explicit_choice) {
   static const int forced = [] {
-    const char* e = getenv("COLAGPU_ZI_TMA");
+    const char* e = getenv("COLAGPU_ZI");
     return e ? atoi(e) : -1;
   }();
-  return forced >= 0 ? forced != 0 : N <= 384;
+  const int m = forced >= 0 ? forced : g_zmode.load();
+  *explicit_choice = m >= 0 && m <= 2;
+  if (*explicit_choice) return m;
+  (void)N;
+  return 2;
+}
+
+// The x and z components' inverse x passes in one launch (k_fx SCALE 3);
+// COLAGPU_FX_DUAL=0 runs them as two.
+bool fx_dual() {
+  static const bool on = [] {
+    const char* e = getenv("COLAGPU_FX_DUAL");
+    return !(e && e[0] == '0');
+  }();
+  return on;
 }
 
 // ---------------------------------------------------- power spectrum bins
@@ -792,13 +968,16 @@ struct MeshKernels {
   void (*fxi)(const float2*, float2*, const float2*, const float*);
   void (*fxi_x)(const float2*, float2*, const float2*, const float*);   // input times n_x
   void (*fxi_z)(const float2*, float2*, const float2*, const float*);   // input times n_z
+  void (*fxi_xz)(const float2*, float2*, const float2*, const float*);  // both (SCALE 3)
   void (*green)(const float2*, float2*, float2*, const float2*, float, GreenMods);
   void (*green_mods)(const float2*, float2*, float2*, const float2*, float, GreenMods);
   void (*zi)(const float2*, float*, const float2*, const float2*);
   void (*zi_tma)(CUtensorMap, float*, const float2*, const float2*, unsigned*);
-  size_t sm_fz, sm_fy, sm_fx, sm_green, sm_zi, sm_zi_tma;
+  void (*zi_sw)(CUtensorMap, float*, const float2*, const float2*, unsigned*);
+  size_t sm_fz, sm_fy, sm_fx, sm_green, sm_zi, sm_zi_tma, sm_zi_sw;
   int tk;    // ky columns per CTA of the x pass
-  int byg;   // lines per CTA of the Green pass
+  int byg;   // lines per CTA of the Green pass (0: one line per warp, grid-stride)
+  int green_threads;
 };
 
 template <int N, int V>
@@ -808,16 +987,26 @@ void set_fx(MeshKernels* k) {
   k->fxi = k_fx<N, 1, 0, TKV, RMX>;
   k->fxi_x = k_fx<N, 1, 1, TKV, RMX>;
   k->fxi_z = k_fx<N, 1, 2, TKV, RMX>;
+  k->fxi_xz = k_fx<N, 1, 3, TKV, RMX>;
   k->sm_fx = sizeof(cplx) * cgfft::col_tile_elems<N, TKV>();
   k->tk = TKV;
 }
 
 template <int N, int V>
 void set_green(MeshKernels* k) {
-  constexpr GreenCfg c = kGreenCfg[V];
-  k->green = k_green<N, c.byg, c.rm, c.minb, false>;
-  k->green_mods = k_green<N, c.byg, c.rm, c.minb, true>;
-  k->sm_green = sizeof(cplx) * 2 * c.byg * cgfft::line_pitch<N>();
+  // the 8-line variants would spill registers beyond 768: variant 0 there
+  constexpr GreenCfg c = kGreenCfg[(N > 768 && kGreenCfg[V].byg == 8) ? 0 : V];
+  if constexpr (c.byg == 0) {
+    k->green = k_green_w<N, c.minb, c.rm, false>;
+    k->green_mods = k_green_w<N, c.minb, c.rm, true>;
+    k->sm_green = sizeof(cplx) * 2 * c.minb * cgfft::line_pitch<N>();
+    k->green_threads = 32 * c.minb;
+  } else {
+    k->green = k_green<N, c.byg, c.rm, c.minb, false>;
+    k->green_mods = k_green<N, c.byg, c.rm, c.minb, true>;
+    k->sm_green = sizeof(cplx) * 2 * c.byg * cgfft::line_pitch<N>();
+    k->green_threads = T;
+  }
   k->byg = c.byg;
 }
 
@@ -831,6 +1020,8 @@ MeshKernels make_kernels(MeshSched s) {
   k.zi = k_zi<N>;
   k.zi_tma = k_zi_tma<N>;
   k.sm_zi_tma = zi_tma_smem<N>();
+  k.zi_sw = k_zi_sw<N>;
+  k.sm_zi_sw = zsw_smem<N>();
   k.sm_fz = sizeof(cplx) * TY * cgfft::line_pitch<N / 2>();
   k.sm_fy = sizeof(cplx) * BY * cgfft::line_pitch<N>();
   k.sm_zi = sizeof(cplx) * TY * cgfft::line_pitch<N / 2 + 1>();
@@ -847,6 +1038,7 @@ MeshKernels make_kernels(MeshSched s) {
     switch (s.green) {
       case 1: set_green<N, 1>(&k); break;
       case 2: set_green<N, 2>(&k); break;
+      case 3: set_green<N, 3>(&k); break;
       default: set_green<N, 0>(&k);
     }
   } else {
@@ -900,10 +1092,12 @@ cudaError_t set_all_smem(int N) {
     if (e == cudaSuccess) e = set_smem((const void*)k.fxi, k.sm_fx);
     if (e == cudaSuccess) e = set_smem((const void*)k.fxi_x, k.sm_fx);
     if (e == cudaSuccess) e = set_smem((const void*)k.fxi_z, k.sm_fx);
+    if (e == cudaSuccess) e = set_smem((const void*)k.fxi_xz, k.sm_fx);
     if (e == cudaSuccess) e = set_smem((const void*)k.green, k.sm_green);
     if (e == cudaSuccess) e = set_smem((const void*)k.green_mods, k.sm_green);
     if (e == cudaSuccess) e = set_smem((const void*)k.zi, k.sm_zi);
     if (e == cudaSuccess) e = set_smem((const void*)k.zi_tma, k.sm_zi_tma);
+    if (e == cudaSuccess) e = set_smem((const void*)k.zi_sw, k.sm_zi_sw);
   }
   return e;
 }
@@ -916,6 +1110,37 @@ void twiddle_table(float2* h, int L) {
 }
 
 }  // namespace
+
+int pm_set_z_gather(int mode) {
+  if (mode < -1 || mode > 2) return -1;
+  g_zmode.store(mode);
+  return 0;
+}
+
+// Grid of the Green pass: one CTA per byg lines, or for the warp form as
+// many CTAs as are resident at once (it strides over the lines).
+unsigned green_grid(const MeshKernels& k, int N, const void* fn) {
+  const long long lines = (long long)(N / 2 + 1) * N;
+  if (k.byg > 0) return (unsigned)(lines / k.byg);
+  static std::mutex mu;
+  static std::map<const void*, int> per_sm;
+  int b = 0;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = per_sm.find(fn);
+    if (it != per_sm.end()) b = it->second;
+  }
+  if (b == 0) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, k.green_threads, k.sm_green) !=
+            cudaSuccess || b < 1)
+      b = 1;
+    std::lock_guard<std::mutex> lk(mu);
+    per_sm[fn] = b;
+  }
+  const long long warps_needed = (lines + k.green_threads / 32 - 1) / (k.green_threads / 32);
+  long long g = (long long)cg_sm_count() * b;
+  return (unsigned)(g < warps_needed ? g : warps_needed);
+}
 
 bool pm_supported_mesh(int N) {
   MeshKernels k;
@@ -985,8 +1210,8 @@ cudaError_t pm_autotune(PmPlan* p, cudaStream_t st, MeshSched* best, float* ms_g
     float t = 0.0f;
     e = best_time(st, kReps, [&] {
       prof_mark(st, CG_ST_OTHER);
-      k.green<<<(N / 2 + 1) * N / k.byg, T, k.sm_green, st>>>(p->spec, p->gsp[1], p->gsp[2],
-                                                               p->twN, p->f1, GreenMods{});
+      k.green<<<green_grid(k, N, (const void*)k.green), k.green_threads, k.sm_green, st>>>(
+          p->spec, p->gsp[1], p->gsp[2], p->twN, p->f1, GreenMods{});
     }, &t);
     if (ms_green) ms_green[v] = t;
     if (e == cudaSuccess && t < tbest) {
@@ -1014,7 +1239,7 @@ cudaError_t pm_autotune(PmPlan* p, cudaStream_t st, MeshSched* best, float* ms_g
   return e;
 }
 
-bool encode_zi_maps(PmPlan* p);
+bool encode_zi_maps(PmPlan* p, bool swizzled);
 
 cudaError_t pm_plan_alloc(PmPlan* p, int N, int factor, float L) {
   memset(p, 0, sizeof(*p));
@@ -1063,7 +1288,16 @@ cudaError_t pm_plan_alloc(PmPlan* p, int N, int factor, float L) {
   CG_TRY(cudaMemset(p->dsum, 0, sizeof(double)));
   CG_TRY(cudaMemset(p->err, 0, sizeof(unsigned)));
   CG_TRY(set_all_smem(N));
-  p->ztm_ok = zi_tma_default(N) && encode_zi_maps(p);
+  bool zexplicit = false;
+  const int zmode = z_gather_mode(N, &zexplicit);
+  p->zsw_ok = zmode == 2 && encode_zi_maps(p, true);
+  p->ztm_ok = zmode == 1 && encode_zi_maps(p, false);
+  // a TMA gather that was asked for explicitly and cannot be set up is an
+  // error; by default the plan falls back to the cp.async gather
+  if (zexplicit && zmode > 0 && !p->zsw_ok && !p->ztm_ok) {
+    pm_plan_free(p);
+    return cudaErrorNotSupported;
+  }
 #undef CG_TRY
   return cudaSuccess;
 }
@@ -1269,15 +1503,18 @@ cudaError_t pm_r2c(PmPlan* p, cudaStream_t st) {
 void launch_zi(const PmPlan* p, const MeshKernels& k, int a, cudaStream_t st) {
   const int N = p->N;
   const dim3 gz(N / TY, N);
-  if (p->ztm_ok)
+  if (p->zsw_ok)
+    k.zi_sw<<<gz, T, k.sm_zi_sw, st>>>(p->ztm[a], p->fmesh[a], p->twH, p->twN, p->err);
+  else if (p->ztm_ok)
     k.zi_tma<<<gz, T, k.sm_zi_tma, st>>>(p->ztm[a], p->fmesh[a], p->twH, p->twN, p->err);
   else
     k.zi<<<gz, T, k.sm_zi, st>>>(p->gsp[a], p->fmesh[a], p->twH, p->twN);
 }
 
-// Tensor maps of the three spectra for k_zi_tma (see there); false when the
-// driver's encoder is unavailable or refuses the layout.
-bool encode_zi_maps(PmPlan* p) {
+// Tensor maps of the three spectra for k_zi_tma or (swizzled) k_zi_sw (see
+// there); false when the driver's encoder is unavailable or refuses the
+// layout.
+bool encode_zi_maps(PmPlan* p, bool swizzled) {
   static PFN_cuTensorMapEncodeTiled_v12000 enc = [] {
     void* f = nullptr;
     cudaDriverEntryPointQueryResult q;
@@ -1288,14 +1525,20 @@ bool encode_zi_maps(PmPlan* p) {
   }();
   if (!enc) return false;
   const int N = p->N;
-  const int nb = (N / 2 + 1 + 255) / 256, kr = (N / 2 + 1 + nb - 1) / nb;
+  const int nb = (N / 2 + 1 + 255) / 256;
+  // rows per box: the landing form splits the kz rows evenly; the swizzled
+  // form rounds up to a multiple of 8 rows (every box 1024-byte aligned)
+  int kr = (N / 2 + 1 + nb - 1) / nb;
+  if (swizzled) kr = (kr + 7) / 8 * 8;
+  if (kr > 256) return false;
   const cuuint64_t dims[3] = {(cuuint64_t)2 * N, (cuuint64_t)N, (cuuint64_t)(N / 2 + 1)};
   const cuuint64_t strides[2] = {(cuuint64_t)N * 8, (cuuint64_t)N * N * 8};
-  const cuuint32_t box[3] = {2 * TY, 1, (cuuint32_t)kr};
+  const cuuint32_t box[3] = {2 * TY, 1, (cuuint32_t)kr};   // 2 TY floats = 128 bytes
   const cuuint32_t es[3] = {1, 1, 1};
   for (int a = 0; a < 3; a++) {
     if (enc(&p->ztm[a], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, (void*)p->gsp[a], dims, strides, box,
-            es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+            es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+            swizzled ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_NONE,
             CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
       return false;
   }
@@ -1310,24 +1553,35 @@ cudaError_t pm_green_c2r(PmPlan* p, cudaStream_t st) {
   prof_mark(st, CG_ST_GREEN);
   const GreenMods gm{p->kfilt_cur >= 0 ? p->kfilt + (size_t)p->kfilt_cur * p->kfilt_n : nullptr,
                      p->kfilt_n, p->kfilt_inv_dn, p->ktab};
-  (gm.t || gm.tab ? k.green_mods : k.green)<<<(N / 2 + 1) * N / k.byg, T, k.sm_green, st>>>(
+  const auto green = gm.t || gm.tab ? k.green_mods : k.green;
+  green<<<green_grid(k, N, (const void*)green), k.green_threads, k.sm_green, st>>>(
       p->spec, p->gsp[1], p->gsp[2], p->twN, p->f1, gm);
   const dim3 gx(N / k.tk, N / 2 + 1);
-  // x: n_x * gsp[2] -> gsp[0] (gsp[2] is still needed for z)
-  prof_mark(st, CG_ST_FX_INV);
-  k.fxi_x<<<gx, T, k.sm_fx, st>>>(p->gsp[2], p->gsp[0], p->twN, p->ktab);
-  prof_mark(st, CG_ST_ZI);
-  launch_zi(p, k, 0, st);
+  if (fx_dual()) {
+    // x and z: n_x * gsp[2] -> gsp[0] and n_z * gsp[2] in place, one launch
+    prof_mark(st, CG_ST_FX_INV);
+    k.fxi_xz<<<gx, T, k.sm_fx, st>>>(p->gsp[2], p->gsp[0], p->twN, p->ktab);
+    prof_mark(st, CG_ST_ZI);
+    launch_zi(p, k, 0, st);
+    prof_mark(st, CG_ST_ZI);
+    launch_zi(p, k, 2, st);
+  } else {
+    // x: n_x * gsp[2] -> gsp[0] (gsp[2] is still needed for z)
+    prof_mark(st, CG_ST_FX_INV);
+    k.fxi_x<<<gx, T, k.sm_fx, st>>>(p->gsp[2], p->gsp[0], p->twN, p->ktab);
+    prof_mark(st, CG_ST_ZI);
+    launch_zi(p, k, 0, st);
+    // z: n_z * gsp[2], in place
+    prof_mark(st, CG_ST_FX_INV);
+    k.fxi_z<<<gx, T, k.sm_fx, st>>>(p->gsp[2], p->gsp[2], p->twN, p->ktab);
+    prof_mark(st, CG_ST_ZI);
+    launch_zi(p, k, 2, st);
+  }
   // y: in place
   prof_mark(st, CG_ST_FX_INV);
   k.fxi<<<gx, T, k.sm_fx, st>>>(p->gsp[1], p->gsp[1], p->twN, nullptr);
   prof_mark(st, CG_ST_ZI);
   launch_zi(p, k, 1, st);
-  // z: n_z * gsp[2], in place
-  prof_mark(st, CG_ST_FX_INV);
-  k.fxi_z<<<gx, T, k.sm_fx, st>>>(p->gsp[2], p->gsp[2], p->twN, p->ktab);
-  prof_mark(st, CG_ST_ZI);
-  launch_zi(p, k, 2, st);
   return cudaGetLastError();
 }
 

@@ -323,6 +323,11 @@ int cg_autotune(int ngrid, int flags, float* ms_green, float* ms_fx);
 int cg_schedule_variants(int ngrid, int* n_green, int* n_fx);
 int cg_get_schedule(int ngrid, int* green_variant, int* fx_variant);
 int cg_set_schedule(int ngrid, int green_variant, int fx_variant);
+/* How the z c2r of the force step gathers its transposed input, for the
+ * handles created afterwards: 0 cp.async, 1 TMA into a landing area, 2 TMA
+ * into the transform's own swizzled tile, -1 (the default) by mesh size.
+ * The three give bit-identical forces; COLAGPU_ZI=0/1/2 overrides. */
+int cg_set_z_gather(int mode);
 
 /* Kernel accounting (no reference counterpart; the reference's wall-clock
  * timers are timer.c).  cg_launch_count: kernels launched by this library
