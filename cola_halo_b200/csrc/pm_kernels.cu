@@ -351,15 +351,12 @@ __host__ __device__ constexpr int n_fx_variants(int N) {
   return N >= MIN_TUNED_N ? PM_NUM_FX_VARIANTS : 1;
 }
 __host__ __device__ constexpr int n_green_variants(int N) {
-  return N >= MIN_TUNED_N ? PM_NUM_GREEN_VARIANTS : 1;
+  return N >= MIN_TUNED_N && N <= 768 ? PM_NUM_GREEN_VARIANTS : 1;
 }
 struct FxCfg { int tk, rm; };
-// byg = 0: one line per warp (k_green_w), rm its maximum radix, minb its
-// warps per CTA
 struct GreenCfg { int byg, rm, minb; };
 constexpr FxCfg kFxCfg[PM_NUM_FX_VARIANTS] = {{8, 0}, {8, -1}, {16, 16}};
-constexpr GreenCfg kGreenCfg[PM_NUM_GREEN_VARIANTS] = {
-    {4, 16, 3}, {8, 8, 2}, {8, 16, 2}, {0, 8, 4}};
+constexpr GreenCfg kGreenCfg[PM_NUM_GREEN_VARIANTS] = {{4, 16, 3}, {8, 8, 2}, {8, 16, 2}};
 __host__ __device__ constexpr int rm_x_default(int N) { return N >= 768 ? 8 : 16; }
 __host__ __device__ constexpr int fx_rm(int N, int v) {
   return kFxCfg[v].rm == 0 ? rm_x_default(N)
@@ -445,18 +442,10 @@ struct GmemScaled {
   static constexpr bool kShared = false;
 };
 
-// One x-pass transform as a separate (not inlined) call, so that two of
-// them in one kernel keep separate register live ranges.
-template <int N, int TKV, int DIR, int RMX, class First, class Mid, class Last>
-__device__ __noinline__ void fft_col_x(const First f, const Mid m, const Last l,
-                                       const float2* __restrict__ tw) {
-  cgfft::fft_io<N, TKV, T, false, DIR, RMX>(f, m, l, tw);
-}
-
 // FX: c2c along kx (stride N), TKV ky columns per CTA, from `in` to `out`
 // (the same array for an in-place pass).  SCALE 0: plain; 1 / 2: the input
 // is first multiplied by n_x / n_z (GmemScaled; gtab: the gradient table or
-// NULL, unused by SCALE 0); 3: both, n_x into `out` and n_z in place.
+// NULL, unused by SCALE 0).
 template <int N, int DIR, int SCALE, int TKV, int RMX>
 __global__ void __launch_bounds__(T) k_fx(const float2* in, float2* out,
                                           const float2* __restrict__ twN,
@@ -468,17 +457,6 @@ __global__ void __launch_bounds__(T) k_fx(const float2* in, float2* out,
   if constexpr (SCALE == 0) {
     const Gmem gi{const_cast<float2*>(in) + off, 1, (size_t)N};
     cgfft::fft_io<N, TKV, T, false, DIR, RMX>(gi, mid, go, twN);
-  } else if constexpr (SCALE == 3) {
-    // the x and z components from the one shared spectrum: n_x in -> out,
-    // then n_z in -> in (the tile's second read comes from L2, so the
-    // spectrum crosses HBM once for both components)
-    const GmemScaled<1> gx{in + off, (size_t)N, N, 0.0f, gtab};
-    fft_col_x<N, TKV, DIR, RMX>(gx, mid, go, twN);
-    __syncthreads();   // the tile buffer is reused
-    const float fz = gtab ? __ldg(gtab + blockIdx.y) : (float)blockIdx.y;
-    const GmemScaled<2> gz{in + off, (size_t)N, N, fz, gtab};
-    const Gmem gzo{const_cast<float2*>(in) + off, 1, (size_t)N};
-    fft_col_x<N, TKV, DIR, RMX>(gz, mid, gzo, twN);
   } else {
     const float fz = SCALE == 2 && gtab ? __ldg(gtab + blockIdx.y) : (float)blockIdx.y;
     const GmemScaled<SCALE> gi{in + off, (size_t)N, N, fz, gtab};
@@ -600,47 +578,6 @@ __global__ void __launch_bounds__(T, MINB) k_green(const float2* __restrict__ sp
   __syncthreads();
   const Gmem os{g2 + off, (size_t)N, 1};
   fft_tile_y<N, BG, RMG, 1>(d, d, os, twN);
-}
-
-// GREEN with one y line per warp: the same three transforms and the same
-// arithmetic as k_green, but every warp owns its line (two padded line
-// buffers of its own) and synchronises only with itself, so the warps of a
-// CTA never wait for one another between stages.  Grid-stride over the
-// (N/2+1) N lines; radices up to RMW (768 = 8 8 4 3, so every stage keeps
-// all 32 lanes busy).
-template <int N, int RMW, int DIR, class First, class Mid, class Last>
-__device__ __noinline__ void fft_line_w(const First f, const Mid m, const Last l,
-                                        const float2* __restrict__ tw) {
-  cgfft::fft_io<N, 1, 32, true, DIR, RMW>(f, m, l, tw);
-}
-
-template <int N, int WPC, int RMW, bool MODS>
-__global__ void __launch_bounds__(32 * WPC) k_green_w(const float2* __restrict__ spec,
-                                                       float2* __restrict__ g1,
-                                                       float2* __restrict__ g2,
-                                                       const float2* __restrict__ twN,
-                                                       float f1, GreenMods gm) {
-  constexpr int P = cgfft::line_pitch<N>();
-  extern __shared__ __align__(16) unsigned char smraw[];
-  const int warp = (int)(threadIdx.x >> 5);
-  cplx* D = reinterpret_cast<cplx*>(smraw) + (size_t)warp * 2 * P;
-  cplx* W = D + P;
-  const SmemLine<P> d{D}, w{W};
-  const size_t nlines = (size_t)(N / 2 + 1) * N;
-  for (size_t l = (size_t)blockIdx.x * WPC + warp; l < nlines; l += (size_t)gridDim.x * WPC) {
-    const int kz = (int)(l / N), kx = (int)(l % N);
-    const size_t off = l * N;
-    const Gmem gin{const_cast<float2*>(spec) + off, (size_t)N, 1};
-    fft_line_w<N, RMW, -1>(gin, d, d, twN);
-    // the y component's load also leaves the shared x/z value in D
-    const GreenLoad<P, 2, MODS> gy{D, kz, kx, N, f1, gm};
-    const Gmem oy{g1 + off, (size_t)N, 1};
-    fft_line_w<N, RMW, 1>(gy, w, oy, twN);
-    __syncwarp();
-    const Gmem os{g2 + off, (size_t)N, 1};
-    fft_line_w<N, RMW, 1>(d, d, os, twN);
-    __syncwarp();   // the next line's first stage overwrites D
-  }
 }
 
 // ZI: c2r along z of S (lines (x, y0..y0+TY-1) per CTA) into R.  The
@@ -901,16 +838,6 @@ int z_gather_mode(int N, bool* explicit_choice) {
   return 2;
 }
 
-// The x and z components' inverse x passes in one launch (k_fx SCALE 3);
-// COLAGPU_FX_DUAL=0 runs them as two.
-bool fx_dual() {
-  static const bool on = [] {
-    const char* e = getenv("COLAGPU_FX_DUAL");
-    return !(e && e[0] == '0');
-  }();
-  return on;
-}
-
 // ---------------------------------------------------- power spectrum bins
 // Shell average of |delta_k|^2 over the half spectrum S[kz][kx][ky]: bin b
 // holds modes with |n| in [b + 1/2, b + 3/2) (|n| in units of the
@@ -968,7 +895,6 @@ struct MeshKernels {
   void (*fxi)(const float2*, float2*, const float2*, const float*);
   void (*fxi_x)(const float2*, float2*, const float2*, const float*);   // input times n_x
   void (*fxi_z)(const float2*, float2*, const float2*, const float*);   // input times n_z
-  void (*fxi_xz)(const float2*, float2*, const float2*, const float*);  // both (SCALE 3)
   void (*green)(const float2*, float2*, float2*, const float2*, float, GreenMods);
   void (*green_mods)(const float2*, float2*, float2*, const float2*, float, GreenMods);
   void (*zi)(const float2*, float*, const float2*, const float2*);
@@ -976,8 +902,7 @@ struct MeshKernels {
   void (*zi_sw)(CUtensorMap, float*, const float2*, const float2*, unsigned*);
   size_t sm_fz, sm_fy, sm_fx, sm_green, sm_zi, sm_zi_tma, sm_zi_sw;
   int tk;    // ky columns per CTA of the x pass
-  int byg;   // lines per CTA of the Green pass (0: one line per warp, grid-stride)
-  int green_threads;
+  int byg;   // lines per CTA of the Green pass
 };
 
 template <int N, int V>
@@ -987,26 +912,16 @@ void set_fx(MeshKernels* k) {
   k->fxi = k_fx<N, 1, 0, TKV, RMX>;
   k->fxi_x = k_fx<N, 1, 1, TKV, RMX>;
   k->fxi_z = k_fx<N, 1, 2, TKV, RMX>;
-  k->fxi_xz = k_fx<N, 1, 3, TKV, RMX>;
   k->sm_fx = sizeof(cplx) * cgfft::col_tile_elems<N, TKV>();
   k->tk = TKV;
 }
 
 template <int N, int V>
 void set_green(MeshKernels* k) {
-  // the 8-line variants would spill registers beyond 768: variant 0 there
-  constexpr GreenCfg c = kGreenCfg[(N > 768 && kGreenCfg[V].byg == 8) ? 0 : V];
-  if constexpr (c.byg == 0) {
-    k->green = k_green_w<N, c.minb, c.rm, false>;
-    k->green_mods = k_green_w<N, c.minb, c.rm, true>;
-    k->sm_green = sizeof(cplx) * 2 * c.minb * cgfft::line_pitch<N>();
-    k->green_threads = 32 * c.minb;
-  } else {
-    k->green = k_green<N, c.byg, c.rm, c.minb, false>;
-    k->green_mods = k_green<N, c.byg, c.rm, c.minb, true>;
-    k->sm_green = sizeof(cplx) * 2 * c.byg * cgfft::line_pitch<N>();
-    k->green_threads = T;
-  }
+  constexpr GreenCfg c = kGreenCfg[V];
+  k->green = k_green<N, c.byg, c.rm, c.minb, false>;
+  k->green_mods = k_green<N, c.byg, c.rm, c.minb, true>;
+  k->sm_green = sizeof(cplx) * 2 * c.byg * cgfft::line_pitch<N>();
   k->byg = c.byg;
 }
 
@@ -1038,7 +953,6 @@ MeshKernels make_kernels(MeshSched s) {
     switch (s.green) {
       case 1: set_green<N, 1>(&k); break;
       case 2: set_green<N, 2>(&k); break;
-      case 3: set_green<N, 3>(&k); break;
       default: set_green<N, 0>(&k);
     }
   } else {
@@ -1092,7 +1006,6 @@ cudaError_t set_all_smem(int N) {
     if (e == cudaSuccess) e = set_smem((const void*)k.fxi, k.sm_fx);
     if (e == cudaSuccess) e = set_smem((const void*)k.fxi_x, k.sm_fx);
     if (e == cudaSuccess) e = set_smem((const void*)k.fxi_z, k.sm_fx);
-    if (e == cudaSuccess) e = set_smem((const void*)k.fxi_xz, k.sm_fx);
     if (e == cudaSuccess) e = set_smem((const void*)k.green, k.sm_green);
     if (e == cudaSuccess) e = set_smem((const void*)k.green_mods, k.sm_green);
     if (e == cudaSuccess) e = set_smem((const void*)k.zi, k.sm_zi);
@@ -1115,31 +1028,6 @@ int pm_set_z_gather(int mode) {
   if (mode < -1 || mode > 2) return -1;
   g_zmode.store(mode);
   return 0;
-}
-
-// Grid of the Green pass: one CTA per byg lines, or for the warp form as
-// many CTAs as are resident at once (it strides over the lines).
-unsigned green_grid(const MeshKernels& k, int N, const void* fn) {
-  const long long lines = (long long)(N / 2 + 1) * N;
-  if (k.byg > 0) return (unsigned)(lines / k.byg);
-  static std::mutex mu;
-  static std::map<const void*, int> per_sm;
-  int b = 0;
-  {
-    std::lock_guard<std::mutex> lk(mu);
-    auto it = per_sm.find(fn);
-    if (it != per_sm.end()) b = it->second;
-  }
-  if (b == 0) {
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, k.green_threads, k.sm_green) !=
-            cudaSuccess || b < 1)
-      b = 1;
-    std::lock_guard<std::mutex> lk(mu);
-    per_sm[fn] = b;
-  }
-  const long long warps_needed = (lines + k.green_threads / 32 - 1) / (k.green_threads / 32);
-  long long g = (long long)cg_sm_count() * b;
-  return (unsigned)(g < warps_needed ? g : warps_needed);
 }
 
 bool pm_supported_mesh(int N) {
@@ -1210,8 +1098,8 @@ cudaError_t pm_autotune(PmPlan* p, cudaStream_t st, MeshSched* best, float* ms_g
     float t = 0.0f;
     e = best_time(st, kReps, [&] {
       prof_mark(st, CG_ST_OTHER);
-      k.green<<<green_grid(k, N, (const void*)k.green), k.green_threads, k.sm_green, st>>>(
-          p->spec, p->gsp[1], p->gsp[2], p->twN, p->f1, GreenMods{});
+      k.green<<<(N / 2 + 1) * N / k.byg, T, k.sm_green, st>>>(p->spec, p->gsp[1], p->gsp[2],
+                                                               p->twN, p->f1, GreenMods{});
     }, &t);
     if (ms_green) ms_green[v] = t;
     if (e == cudaSuccess && t < tbest) {
@@ -1553,35 +1441,24 @@ cudaError_t pm_green_c2r(PmPlan* p, cudaStream_t st) {
   prof_mark(st, CG_ST_GREEN);
   const GreenMods gm{p->kfilt_cur >= 0 ? p->kfilt + (size_t)p->kfilt_cur * p->kfilt_n : nullptr,
                      p->kfilt_n, p->kfilt_inv_dn, p->ktab};
-  const auto green = gm.t || gm.tab ? k.green_mods : k.green;
-  green<<<green_grid(k, N, (const void*)green), k.green_threads, k.sm_green, st>>>(
+  (gm.t || gm.tab ? k.green_mods : k.green)<<<(N / 2 + 1) * N / k.byg, T, k.sm_green, st>>>(
       p->spec, p->gsp[1], p->gsp[2], p->twN, p->f1, gm);
   const dim3 gx(N / k.tk, N / 2 + 1);
-  if (fx_dual()) {
-    // x and z: n_x * gsp[2] -> gsp[0] and n_z * gsp[2] in place, one launch
-    prof_mark(st, CG_ST_FX_INV);
-    k.fxi_xz<<<gx, T, k.sm_fx, st>>>(p->gsp[2], p->gsp[0], p->twN, p->ktab);
-    prof_mark(st, CG_ST_ZI);
-    launch_zi(p, k, 0, st);
-    prof_mark(st, CG_ST_ZI);
-    launch_zi(p, k, 2, st);
-  } else {
-    // x: n_x * gsp[2] -> gsp[0] (gsp[2] is still needed for z)
-    prof_mark(st, CG_ST_FX_INV);
-    k.fxi_x<<<gx, T, k.sm_fx, st>>>(p->gsp[2], p->gsp[0], p->twN, p->ktab);
-    prof_mark(st, CG_ST_ZI);
-    launch_zi(p, k, 0, st);
-    // z: n_z * gsp[2], in place
-    prof_mark(st, CG_ST_FX_INV);
-    k.fxi_z<<<gx, T, k.sm_fx, st>>>(p->gsp[2], p->gsp[2], p->twN, p->ktab);
-    prof_mark(st, CG_ST_ZI);
-    launch_zi(p, k, 2, st);
-  }
+  // x: n_x * gsp[2] -> gsp[0] (gsp[2] is still needed for z)
+  prof_mark(st, CG_ST_FX_INV);
+  k.fxi_x<<<gx, T, k.sm_fx, st>>>(p->gsp[2], p->gsp[0], p->twN, p->ktab);
+  prof_mark(st, CG_ST_ZI);
+  launch_zi(p, k, 0, st);
   // y: in place
   prof_mark(st, CG_ST_FX_INV);
   k.fxi<<<gx, T, k.sm_fx, st>>>(p->gsp[1], p->gsp[1], p->twN, nullptr);
   prof_mark(st, CG_ST_ZI);
   launch_zi(p, k, 1, st);
+  // z: n_z * gsp[2], in place
+  prof_mark(st, CG_ST_FX_INV);
+  k.fxi_z<<<gx, T, k.sm_fx, st>>>(p->gsp[2], p->gsp[2], p->twN, p->ktab);
+  prof_mark(st, CG_ST_ZI);
+  launch_zi(p, k, 2, st);
   return cudaGetLastError();
 }
 
