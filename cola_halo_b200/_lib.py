@@ -87,6 +87,7 @@ SIGNATURES = {
     "cg_get_schedule": (i32, [i32, ctypes.POINTER(i32), ctypes.POINTER(i32)]),
     "cg_set_schedule": (i32, [i32, i32, i32]),
     "cg_set_z_gather": (i32, [i32]),
+    "cg_set_x_gather": (i32, [i32]),
     "cg_fft_r2c": (i32, [i32, P, P]),
     "cg_fft_c2r": (i32, [i32, P, P]),
     "cg_fft_time": (i32, [i32, i32, fptr, fptr]),

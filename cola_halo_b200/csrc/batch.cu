@@ -92,6 +92,7 @@ PmPlan view(const PmPlan& bufs, const MeshFFT& tab, int N, int factor, float L) 
   p.spec_bytes = sizeof(float2) * (size_t)(N / 2 + 1) * N * N;
   p.ztm_ok = false;    // the stream's TMA maps describe its largest mesh, not this one
   p.zsw_ok = false;
+  p.xsw_ok = false;
   p.keep_dens = true;  // meshes of several sizes share the buffer: fill every step
   p.dens_reset = false;
   return p;

@@ -222,6 +222,19 @@ struct SmemSw16 {
   static constexpr bool kShared = true;
 };
 
+// The same for 8 columns in 64-byte rows ([n][b]) as a TMA load with the
+// 64-byte swizzle writes them: chunk c of row n sits at chunk
+// c ^ ((n / 2) mod 4) (the tile starts on a 1024-byte boundary).
+struct SmemSw8 {
+  cplx* s;
+  __device__ __forceinline__ int at(int b, int n) const {
+    return (n << 3) + ((((b >> 1) ^ (n >> 1)) & 3) << 1) + (b & 1);
+  }
+  __device__ __forceinline__ cplx ld(int b, int n) const { return s[at(b, n)]; }
+  __device__ __forceinline__ void st(int b, int n, cplx v) const { s[at(b, n)] = v; }
+  static constexpr bool kShared = true;
+};
+
 // Global lines: element n of line b at p[b * ls + n * es].
 struct Gmem {
   float2* p;

@@ -71,6 +71,9 @@ struct PmPlan {
   bool ztm_ok;              //   valid, landing-area form k_zi_tma
   bool zsw_ok;              //   valid, swizzled-tile form k_zi_sw (else, with neither,
                             //   the cp.async gather runs)
+  CUtensorMap xtm[3];       // TMA maps of spec, gsp[1], gsp[2] for the x pass's gather
+  bool xsw_ok;              //   valid (else the x pass loads directly)
+  int xtm_tk;               //   the columns per CTA the maps were encoded for
 };
 
 // Plain 3-D real transforms on the mesh layouts above (unnormalised, FFTW
@@ -101,6 +104,9 @@ bool pm_supported_mesh(int N);
 // Gather of the z c2r for plans created afterwards: -1 by mesh size, 0
 // cp.async, 1 TMA landing area, 2 TMA swizzled tile.  -1 on a bad mode.
 int pm_set_z_gather(int mode);
+// Gather of the x pass for plans created afterwards: -1 default, 0 direct
+// loads, 1 TMA into a swizzled tile.  -1 on a bad mode.
+int pm_set_x_gather(int mode);
 // Number of schedule variants compiled for mesh size N (1 below 256).
 int pm_num_variants(int N, int* n_green, int* n_fx);
 MeshSched pm_get_schedule(int N);

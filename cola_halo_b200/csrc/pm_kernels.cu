@@ -39,6 +39,9 @@
 
 using cgfft::cplx;
 
+// TMA maps of the x pass for tk columns per CTA (encoded on demand).
+bool x_maps_for(PmPlan* p, int tk);
+
 namespace {
 
 constexpr int T = CG_THREADS;
@@ -464,6 +467,94 @@ __global__ void __launch_bounds__(T) k_fx(const float2* in, float2* out,
   }
 }
 
+// FX with the strided column gather done by TMA: the CTA's TKV ky columns
+// of one kz plane (N rows of TKV complex, 64 or 128 bytes) land densely in
+// the transform's own tile by tiled tensor loads with the 64- or 128-byte
+// swizzle (cgfft::SmemSw8 / SmemSw16 undo it), in NB boxes of KR rows; the
+// first stage then reads the tile, scaled by n_x or n_z as k_fx's loads
+// scale them.  Same arithmetic as k_fx; bounded wait, CG_ERR_TMA_WAIT on a
+// timeout.  The tensor map views the spectrum as floats (2N, N, N/2+1).
+template <int N> __host__ __device__ constexpr int fx_nbox() { return (N + 255) / 256; }
+template <int N> __host__ __device__ constexpr int fx_krows() { return N / fx_nbox<N>(); }
+template <int N, int TKV> __host__ __device__ constexpr size_t fx_sw_smem() {
+  return sizeof(float2) * (size_t)N * TKV + 1024 + 16;
+}
+template <int TKV> struct SwTile;
+template <> struct SwTile<8> { using type = cgfft::SmemSw8; };
+template <> struct SwTile<16> { using type = cgfft::SmemSw16; };
+
+// Shared tile element scaled on load like GmemScaled (SCALE 1: n_x or the
+// gradient table at n; 2: the plane's n_z).
+template <class S, int SCALE>
+struct SmemScaled {
+  S t;
+  int N;
+  float fz;
+  const float* g;
+  __device__ __forceinline__ cplx ld(int b, int n) const {
+    const cplx v = t.ld(b, n);
+    const float f = SCALE == 1 ? (g ? __ldg(g + n) : (float)(n <= N / 2 ? n : n - N)) : fz;
+    return cplx{v.x * f, v.y * f};
+  }
+  __device__ __forceinline__ void st(int b, int n, cplx v) const { t.st(b, n, v); }
+  static constexpr bool kShared = true;
+};
+
+template <int N, int DIR, int SCALE, int TKV, int RMX>
+__global__ void __launch_bounds__(T) k_fx_sw(const __grid_constant__ CUtensorMap tm,
+                                             float2* out, const float2* __restrict__ twN,
+                                             const float* __restrict__ gtab,
+                                             unsigned* __restrict__ err) {
+  static_assert(N % fx_nbox<N>() == 0 && fx_krows<N>() % 8 == 0, "box rows");
+  constexpr int KR = fx_krows<N>(), NB = fx_nbox<N>();
+  constexpr unsigned kBytes = (unsigned)(sizeof(float2) * N * TKV);
+  extern __shared__ __align__(16) unsigned char smraw[];
+  unsigned char* base =
+      smraw + ((1024u - ((unsigned)__cvta_generic_to_shared(smraw) & 1023u)) & 1023u);
+  using Tile = typename SwTile<TKV>::type;
+  const Tile t{reinterpret_cast<cplx*>(base)};
+  const unsigned bar = (unsigned)__cvta_generic_to_shared(base + kBytes);
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(bar) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar),
+                 "r"(kBytes) : "memory");
+    const unsigned dst0 = (unsigned)__cvta_generic_to_shared(base);
+#pragma unroll
+    for (int h = 0; h < NB; h++) {
+      asm volatile(
+          "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
+          " [%0], [%1, {%2, %3, %4}], [%5];\n" ::"r"(dst0 + (unsigned)(sizeof(float2) * TKV * KR * h)),
+          "l"(reinterpret_cast<unsigned long long>(&tm)), "r"((int)(2 * TKV * blockIdx.x)),
+          "r"(h * KR), "r"((int)blockIdx.y), "r"(bar)
+          : "memory");
+    }
+  }
+  unsigned done = 0;
+  for (int it = 0; it < (1 << 22) && !done; it++) {
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done) : "r"(bar) : "memory");
+  }
+  if (!done) {
+    if (threadIdx.x == 0) atomicOr(err, (unsigned)CG_ERR_TMA_WAIT);
+    return;
+  }
+  const size_t off = (size_t)blockIdx.y * N * N + blockIdx.x * TKV;
+  const Gmem go{out + off, 1, (size_t)N};
+  if constexpr (SCALE == 0) {
+    cgfft::fft_io<N, TKV, T, false, DIR, RMX>(t, t, go, twN);
+  } else {
+    const float fz = SCALE == 2 && gtab ? __ldg(gtab + blockIdx.y) : (float)blockIdx.y;
+    const SmemScaled<Tile, SCALE> ts{t, N, fz, gtab};
+    cgfft::fft_io<N, TKV, T, false, DIR, RMX>(ts, t, go, twN);
+  }
+}
+
 // Options of the Green step beyond the reference's kernel (all off: the
 // reference's exact spectral force).
 //  * t: an isotropic transfer function of the force T(|n|) (|n| in units of
@@ -826,6 +917,24 @@ __global__ void __launch_bounds__(T, N >= 1024 ? 3 : 4) k_zi_sw(const __grid_con
 // cg_set_z_gather, or COLAGPU_ZI=0/1/2, selects one.
 std::atomic<int> g_zmode{-1};
 
+// Gather of the strided x pass in the force step (plans created afterwards):
+// 0 direct loads (k_fx), 1 TMA into the swizzled tile (k_fx_sw).
+// cg_set_x_gather, or COLAGPU_FXG=0/1, selects one; both give bit-identical
+// output.
+std::atomic<int> g_xmode{-1};
+
+int x_gather_mode(int N, bool* explicit_choice) {
+  static const int forced = [] {
+    const char* e = getenv("COLAGPU_FXG");
+    return e ? atoi(e) : -1;
+  }();
+  const int m = forced >= 0 ? forced : g_xmode.load();
+  *explicit_choice = m == 0 || m == 1;
+  if (*explicit_choice) return m;
+  (void)N;
+  return 1;
+}
+
 int z_gather_mode(int N, bool* explicit_choice) {
   static const int forced = [] {
     const char* e = getenv("COLAGPU_ZI");
@@ -895,6 +1004,12 @@ struct MeshKernels {
   void (*fxi)(const float2*, float2*, const float2*, const float*);
   void (*fxi_x)(const float2*, float2*, const float2*, const float*);   // input times n_x
   void (*fxi_z)(const float2*, float2*, const float2*, const float*);   // input times n_z
+  // the same four with the TMA gather (k_fx_sw)
+  void (*fxf_sw)(CUtensorMap, float2*, const float2*, const float*, unsigned*);
+  void (*fxi_sw)(CUtensorMap, float2*, const float2*, const float*, unsigned*);
+  void (*fxi_x_sw)(CUtensorMap, float2*, const float2*, const float*, unsigned*);
+  void (*fxi_z_sw)(CUtensorMap, float2*, const float2*, const float*, unsigned*);
+  size_t sm_fx_sw;
   void (*green)(const float2*, float2*, float2*, const float2*, float, GreenMods);
   void (*green_mods)(const float2*, float2*, float2*, const float2*, float, GreenMods);
   void (*zi)(const float2*, float*, const float2*, const float2*);
@@ -912,6 +1027,11 @@ void set_fx(MeshKernels* k) {
   k->fxi = k_fx<N, 1, 0, TKV, RMX>;
   k->fxi_x = k_fx<N, 1, 1, TKV, RMX>;
   k->fxi_z = k_fx<N, 1, 2, TKV, RMX>;
+  k->fxf_sw = k_fx_sw<N, -1, 0, TKV, RMX>;
+  k->fxi_sw = k_fx_sw<N, 1, 0, TKV, RMX>;
+  k->fxi_x_sw = k_fx_sw<N, 1, 1, TKV, RMX>;
+  k->fxi_z_sw = k_fx_sw<N, 1, 2, TKV, RMX>;
+  k->sm_fx_sw = fx_sw_smem<N, TKV>();
   k->sm_fx = sizeof(cplx) * cgfft::col_tile_elems<N, TKV>();
   k->tk = TKV;
 }
@@ -1006,6 +1126,10 @@ cudaError_t set_all_smem(int N) {
     if (e == cudaSuccess) e = set_smem((const void*)k.fxi, k.sm_fx);
     if (e == cudaSuccess) e = set_smem((const void*)k.fxi_x, k.sm_fx);
     if (e == cudaSuccess) e = set_smem((const void*)k.fxi_z, k.sm_fx);
+    if (e == cudaSuccess) e = set_smem((const void*)k.fxf_sw, k.sm_fx_sw);
+    if (e == cudaSuccess) e = set_smem((const void*)k.fxi_sw, k.sm_fx_sw);
+    if (e == cudaSuccess) e = set_smem((const void*)k.fxi_x_sw, k.sm_fx_sw);
+    if (e == cudaSuccess) e = set_smem((const void*)k.fxi_z_sw, k.sm_fx_sw);
     if (e == cudaSuccess) e = set_smem((const void*)k.green, k.sm_green);
     if (e == cudaSuccess) e = set_smem((const void*)k.green_mods, k.sm_green);
     if (e == cudaSuccess) e = set_smem((const void*)k.zi, k.sm_zi);
@@ -1027,6 +1151,12 @@ void twiddle_table(float2* h, int L) {
 int pm_set_z_gather(int mode) {
   if (mode < -1 || mode > 2) return -1;
   g_zmode.store(mode);
+  return 0;
+}
+
+int pm_set_x_gather(int mode) {
+  if (mode < -1 || mode > 1) return -1;
+  g_xmode.store(mode);
   return 0;
 }
 
@@ -1111,11 +1241,16 @@ cudaError_t pm_autotune(PmPlan* p, cudaStream_t st, MeshSched* best, float* ms_g
   for (int v = 0; v < nf && e == cudaSuccess; v++) {
     MeshKernels k;
     kernels_with(N, MeshSched{0, v}, &k);
+    const bool xsw = x_maps_for(p, k.tk);   // time the gather the plan uses
     float t = 0.0f;
     e = best_time(st, kReps, [&] {
       prof_mark(st, CG_ST_OTHER);
-      k.fxi_x<<<dim3(N / k.tk, N / 2 + 1), T, k.sm_fx, st>>>(p->gsp[2], p->gsp[0], p->twN,
-                                                             nullptr);
+      if (xsw)
+        k.fxi_x_sw<<<dim3(N / k.tk, N / 2 + 1), T, k.sm_fx_sw, st>>>(p->xtm[2], p->gsp[0],
+                                                                     p->twN, nullptr, p->err);
+      else
+        k.fxi_x<<<dim3(N / k.tk, N / 2 + 1), T, k.sm_fx, st>>>(p->gsp[2], p->gsp[0], p->twN,
+                                                               nullptr);
     }, &t);
     if (ms_fx) ms_fx[v] = t;
     if (e == cudaSuccess && t < tbest) {
@@ -1128,6 +1263,7 @@ cudaError_t pm_autotune(PmPlan* p, cudaStream_t st, MeshSched* best, float* ms_g
 }
 
 bool encode_zi_maps(PmPlan* p, bool swizzled);
+bool encode_x_maps(PmPlan* p, int tk);
 
 cudaError_t pm_plan_alloc(PmPlan* p, int N, int factor, float L) {
   memset(p, 0, sizeof(*p));
@@ -1183,6 +1319,12 @@ cudaError_t pm_plan_alloc(PmPlan* p, int N, int factor, float L) {
   // a TMA gather that was asked for explicitly and cannot be set up is an
   // error; by default the plan falls back to the cp.async gather
   if (zexplicit && zmode > 0 && !p->zsw_ok && !p->ztm_ok) {
+    pm_plan_free(p);
+    return cudaErrorNotSupported;
+  }
+  bool xexplicit = false;
+  p->xsw_ok = x_gather_mode(N, &xexplicit) == 1 && encode_x_maps(p, k.tk);
+  if (xexplicit && x_gather_mode(N, &xexplicit) == 1 && !p->xsw_ok) {
     pm_plan_free(p);
     return cudaErrorNotSupported;
   }
@@ -1382,7 +1524,11 @@ cudaError_t pm_r2c(PmPlan* p, cudaStream_t st) {
     k.fz_reset<<<dim3(N / TY, N), T, k.sm_fz, st>>>(p->dens, p->spec, p->twH, p->twN, p->dsum);
   p->dens_reset = !p->keep_dens;
   prof_mark(st, CG_ST_FX_FWD);
-  k.fxf<<<dim3(N / k.tk, N / 2 + 1), T, k.sm_fx, st>>>(p->spec, p->spec, p->twN, nullptr);
+  if (x_maps_for(p, k.tk))
+    k.fxf_sw<<<dim3(N / k.tk, N / 2 + 1), T, k.sm_fx_sw, st>>>(p->xtm[0], p->spec, p->twN,
+                                                               nullptr, p->err);
+  else
+    k.fxf<<<dim3(N / k.tk, N / 2 + 1), T, k.sm_fx, st>>>(p->spec, p->spec, p->twN, nullptr);
   return cudaGetLastError();
 }
 
@@ -1433,6 +1579,49 @@ bool encode_zi_maps(PmPlan* p, bool swizzled) {
   return true;
 }
 
+// Tensor maps of the x pass's inputs (spec, gsp[1], gsp[2]) for k_fx_sw
+// with tk columns per CTA: floats (2N, N, N/2+1), box (2 tk, N / nbox, 1),
+// swizzled like the tile.
+bool encode_x_maps(PmPlan* p, int tk) {
+  static PFN_cuTensorMapEncodeTiled_v12000 enc = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) !=
+            cudaSuccess || q != cudaDriverEntryPointSuccess)
+      f = nullptr;
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+  }();
+  if (!enc) return false;
+  const int N = p->N;
+  const int nb = (N + 255) / 256;
+  if (N % nb || (N / nb) % 8 || (tk != 8 && tk != 16)) return false;
+  const cuuint64_t dims[3] = {(cuuint64_t)2 * N, (cuuint64_t)N, (cuuint64_t)(N / 2 + 1)};
+  const cuuint64_t strides[2] = {(cuuint64_t)N * 8, (cuuint64_t)N * N * 8};
+  const cuuint32_t box[3] = {(cuuint32_t)(2 * tk), (cuuint32_t)(N / nb), 1};
+  const cuuint32_t es[3] = {1, 1, 1};
+  float2* const src[3] = {p->spec, p->gsp[1], p->gsp[2]};
+  for (int a = 0; a < 3; a++) {
+    if (enc(&p->xtm[a], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, (void*)src[a], dims, strides, box,
+            es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+            tk == 8 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_128B,
+            CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+      return false;
+  }
+  p->xtm_tk = tk;
+  return true;
+}
+
+// The x pass's TMA maps for the columns per CTA of the schedule in use (a
+// schedule may change after the plan exists); false: load directly.
+bool x_maps_for(PmPlan* p, int tk) {
+  if (!p->xsw_ok) return false;
+  if (p->xtm_tk != tk && !encode_x_maps(p, tk)) {
+    p->xsw_ok = false;
+    return false;
+  }
+  return true;
+}
+
 cudaError_t pm_green_c2r(PmPlan* p, cudaStream_t st) {
   MeshKernels k;
   get_kernels(p->N, &k);
@@ -1444,19 +1633,29 @@ cudaError_t pm_green_c2r(PmPlan* p, cudaStream_t st) {
   (gm.t || gm.tab ? k.green_mods : k.green)<<<(N / 2 + 1) * N / k.byg, T, k.sm_green, st>>>(
       p->spec, p->gsp[1], p->gsp[2], p->twN, p->f1, gm);
   const dim3 gx(N / k.tk, N / 2 + 1);
+  const bool xsw = x_maps_for(p, k.tk);
   // x: n_x * gsp[2] -> gsp[0] (gsp[2] is still needed for z)
   prof_mark(st, CG_ST_FX_INV);
-  k.fxi_x<<<gx, T, k.sm_fx, st>>>(p->gsp[2], p->gsp[0], p->twN, p->ktab);
+  if (xsw)
+    k.fxi_x_sw<<<gx, T, k.sm_fx_sw, st>>>(p->xtm[2], p->gsp[0], p->twN, p->ktab, p->err);
+  else
+    k.fxi_x<<<gx, T, k.sm_fx, st>>>(p->gsp[2], p->gsp[0], p->twN, p->ktab);
   prof_mark(st, CG_ST_ZI);
   launch_zi(p, k, 0, st);
   // y: in place
   prof_mark(st, CG_ST_FX_INV);
-  k.fxi<<<gx, T, k.sm_fx, st>>>(p->gsp[1], p->gsp[1], p->twN, nullptr);
+  if (xsw)
+    k.fxi_sw<<<gx, T, k.sm_fx_sw, st>>>(p->xtm[1], p->gsp[1], p->twN, nullptr, p->err);
+  else
+    k.fxi<<<gx, T, k.sm_fx, st>>>(p->gsp[1], p->gsp[1], p->twN, nullptr);
   prof_mark(st, CG_ST_ZI);
   launch_zi(p, k, 1, st);
   // z: n_z * gsp[2], in place
   prof_mark(st, CG_ST_FX_INV);
-  k.fxi_z<<<gx, T, k.sm_fx, st>>>(p->gsp[2], p->gsp[2], p->twN, p->ktab);
+  if (xsw)
+    k.fxi_z_sw<<<gx, T, k.sm_fx_sw, st>>>(p->xtm[2], p->gsp[2], p->twN, p->ktab, p->err);
+  else
+    k.fxi_z<<<gx, T, k.sm_fx, st>>>(p->gsp[2], p->gsp[2], p->twN, p->ktab);
   prof_mark(st, CG_ST_ZI);
   launch_zi(p, k, 2, st);
   return cudaGetLastError();

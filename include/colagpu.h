@@ -328,6 +328,11 @@ int cg_set_schedule(int ngrid, int green_variant, int fx_variant);
  * into the transform's own swizzled tile, -1 (the default) by mesh size.
  * The three give bit-identical forces; COLAGPU_ZI=0/1/2 overrides. */
 int cg_set_z_gather(int mode);
+/* How the strided x pass of the force step gathers its columns, for the
+ * handles created afterwards: 0 direct loads, 1 TMA into the transform's
+ * own swizzled tile, -1 (the default) by mesh size.  Bit-identical forces;
+ * COLAGPU_FXG=0/1 overrides. */
+int cg_set_x_gather(int mode);
 
 /* Kernel accounting (no reference counterpart; the reference's wall-clock
  * timers are timer.c).  cg_launch_count: kernels launched by this library
