@@ -72,6 +72,7 @@ SIGNATURES = {
     "cg_batch_destroy": (None, [P]),
     "cg_batch_set_particles": (i32, [P, i32, P, i64]),
     "cg_batch_run": (i32, [P]),
+    "cg_batch_set_sort_interval": (i32, [P, i32]),
     "cg_batch_get_snapshot": (i32, [P, i32, P]),
     "cg_batch_power_spectrum": (i32, [P, i32, P, P, P]),
     "cg_batch_num_nodes": (i32, [P, ctypes.POINTER(sz)]),

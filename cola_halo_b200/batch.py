@@ -31,6 +31,12 @@ class Batch:
         _lib.check(self.lib.cg_batch_set_particles(self.h, i, p.ctypes.data, len(p)),
                    "cg_batch_set_particles")
 
+    def set_sort_interval(self, every):
+        """Cell-order sort at every `every`-th move inside the graph (0:
+        never); before the first run."""
+        _lib.check(self.lib.cg_batch_set_sort_interval(self.h, int(every)),
+                   "cg_batch_set_sort_interval")
+
     def run(self):
         _lib.check(self.lib.cg_batch_run(self.h), "cg_batch_run")
 

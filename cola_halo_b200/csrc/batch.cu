@@ -33,6 +33,9 @@ struct Real {
   cg_realization_spec spec;
   ParticleSoA ps{};
   float* soa = nullptr;
+  long long* id_alloc = nullptr;  // the allocations behind ps.id / ps.orig (a sort
+  int* orig_alloc = nullptr;      // exchanges ps's pointers with order's scratch)
+  ParticleOrder order;            // cell-order sort scratch (sorting batches only)
   void* ics = nullptr;          // initial Particle[] (device)
   void* snap = nullptr;         // ParticleMinimum[] (device)
   double* dsum = nullptr;       // one density sum per force evaluation
@@ -51,6 +54,7 @@ struct StreamBufs {
 
 struct cg_batch {
   double omega_m = 0;
+  int sort_every = 0;              // cell-order sort at every sort_every-th move
   std::unique_ptr<ColaTime> ct;
   std::vector<Real> reals;
   std::vector<StreamBufs> streams;
@@ -111,6 +115,7 @@ cudaError_t record_realization(cg_batch* b, Real& r, StreamBufs& sb) {
   float a_x = (float)sp.a_init, a_v = (float)sp.a_init;
   const float aout = sp.aout;
   bool written = false;
+  // the particles' working arrays; a cell-order sort exchanges them
   const float* cx[3] = {r.ps.x[0], r.ps.x[1], r.ps.x[2]};
   const float* cv[3] = {r.ps.v[0], r.ps.v[1], r.ps.v[2]};
   const float* cf[3] = {r.ps.f[0], r.ps.f[1], r.ps.f[2]};
@@ -123,6 +128,18 @@ cudaError_t record_realization(cg_batch* b, Real& r, StreamBufs& sb) {
     const double avel1 = sp.a_init + (istep - 0.5) * da;
     const double apos1 = sp.a_init + istep * da;
     if ((e = dev_wrap(r.ps.x, r.ps.n, sp.boxsize, st)) != cudaSuccess) return e;
+    if (b->sort_every > 0 && istep % b->sort_every == 0) {
+      // cell order, as cg_sim_move sorts (the pointers the captured kernels
+      // get follow the exchange, so every relaunch repeats it)
+      if ((e = particles_sort_cells(&r.ps, &r.order, sp.boxsize, st)) != cudaSuccess) return e;
+      for (int a = 0; a < 3; a++) {
+        cx[a] = r.ps.x[a];
+        cv[a] = r.ps.v[a];
+        cf[a] = r.ps.f[a];
+        c1[a] = r.ps.dx1[a];
+        c2[a] = r.ps.dx2[a];
+      }
+    }
     p.dsum = r.dsum + iforce++;
     if ((e = pm_forces(&p, cx, r.ps.n, r.ps.f, st)) != cudaSuccess) return e;
     auto snapshot = [&]() -> cudaError_t {
@@ -134,7 +151,7 @@ cudaError_t record_realization(cg_batch* b, Real& r, StreamBufs& sb) {
       const float Dv2 = (float)b->ct->D2v((double)aout);
       written = true;
       return dev_snapshot(cx, cv, cf, c1, c2, r.ps.n, b->ct->om32, dda, q1, q2, Dv, Dv2, dyyy,
-                          da1, da2, vfac, r.ps.id, nullptr, r.snap, st);
+                          da1, da2, vfac, r.ps.id, r.ps.orig, r.snap, st);
     };
     if (avel0 <= aout && aout <= apos0) {
       if ((e = snapshot()) != cudaSuccess) return e;
@@ -168,7 +185,9 @@ void free_batch(cg_batch* b) {
   if (b->graph) cudaGraphDestroy(b->graph);
   for (auto& r : b->reals) {
     cudaFree(r.soa);
-    cudaFree(r.ps.id);
+    cudaFree(r.id_alloc);
+    cudaFree(r.orig_alloc);
+    particle_order_free(&r.order);
     cudaFree(r.ics);
     cudaFree(r.snap);
     cudaFree(r.dsum);
@@ -201,6 +220,13 @@ extern "C" int cg_batch_create(cg_batch** out, int nreal, const cg_realization_s
   }
   cg_batch* b = new cg_batch();
   b->omega_m = omega_m;
+  // the cell-order sort policy of cg_sim: every sixth move from 2^23
+  // particles per realization (COLAGPU_SORT_EVERY overrides)
+  long long npmax = 0;
+  for (int i = 0; i < nreal; i++)
+    npmax = std::max(npmax, (long long)specs[i].nc * specs[i].nc * specs[i].nc);
+  b->sort_every = npmax >= (1LL << 23) ? 6 : 0;
+  if (const char* ev = getenv("COLAGPU_SORT_EVERY")) b->sort_every = atoi(ev) > 0 ? atoi(ev) : 0;
   b->ct.reset(new ColaTime(omega_m));
   b->reals.resize(nreal);
   if (nstreams > nreal) nstreams = nreal;
@@ -239,7 +265,10 @@ extern "C" int cg_batch_create(cg_batch** out, int nreal, const cg_realization_s
     r.ps.n = np;
     r.ps.cap = np;
     e = cudaMalloc(&r.soa, sizeof(float) * 15 * (size_t)np);
-    if (e == cudaSuccess) e = cudaMalloc(&r.ps.id, sizeof(long long) * (size_t)np);
+    if (e == cudaSuccess) e = cudaMalloc(&r.id_alloc, sizeof(long long) * (size_t)np);
+    if (e == cudaSuccess) e = cudaMalloc(&r.orig_alloc, sizeof(int) * (size_t)np);
+    r.ps.id = r.id_alloc;
+    r.ps.orig = r.orig_alloc;
     if (e == cudaSuccess) e = cudaMalloc(&r.ics, 56 * (size_t)np);
     if (e == cudaSuccess) e = cudaMalloc(&r.snap, 32 * (size_t)np);
     if (e == cudaSuccess) e = cudaMalloc(&r.dsum, sizeof(double) * (r.spec.nsteps + 2));
@@ -276,12 +305,24 @@ extern "C" int cg_batch_set_particles(cg_batch* b, int i, const void* particles,
   return CG_OK;
 }
 
+extern "C" int cg_batch_set_sort_interval(cg_batch* b, int every) {
+  if (!b || every < 0) return fail(CG_EINVAL, "cg_batch_set_sort_interval: bad arguments");
+  if (b->exec) return fail(CG_EINVAL, "cg_batch_set_sort_interval: the batch is recorded already");
+  b->sort_every = every;
+  return CG_OK;
+}
+
 extern "C" int cg_batch_run(cg_batch* b) {
   if (!b) return fail(CG_EINVAL, "cg_batch_run: NULL");
   for (auto& r : b->reals)
     if (!r.loaded) return fail(CG_EINVAL, "cg_batch_run: a realization has no particles");
   cudaError_t e = cudaSuccess;
   if (!b->exec) {
+    // the sort's scratch, allocated before the capture (which allocates nothing)
+    for (auto& r : b->reals)
+      if (b->sort_every > 0 && (e = particle_order_reserve(&r.order, r.ps.cap)) != cudaSuccess)
+        return fail(e == cudaErrorMemoryAllocation ? CG_ENOMEM : CG_ECUDA,
+                    "cg_batch_run: sort scratch", e);
     const int ns = (int)b->streams.size();
     b->events.resize(ns + 1);
     for (auto& ev : b->events)

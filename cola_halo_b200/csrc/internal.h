@@ -225,6 +225,10 @@ struct ParticleOrder {
   unsigned* bsum = nullptr; // scan scratch
 };
 void particle_order_free(ParticleOrder* o);
+// Allocate o's arrays for up to cap particles now (before a stream capture,
+// which must not allocate); a later sort of at most cap particles then
+// allocates nothing.
+cudaError_t particle_order_reserve(ParticleOrder* o, long long cap);
 // Sort s into cell order, allocating o's arrays on first use (o's
 // capacity is s->cap).  s's array pointers are exchanged with o's scratch
 // set, so the owner of s must free its arrays through the allocations it

@@ -440,7 +440,9 @@ struct GmemScaled {
   __device__ __forceinline__ cplx ld(int b, int n) const {
     const float2 v = __ldg(p + b + (size_t)n * es);
     const float f = SCALE == 1 ? (g ? __ldg(g + n) : (float)(n <= N / 2 ? n : n - N)) : fz;
-    return cplx{v.x * f, v.y * f};
+    // rounded products (never fused into the transform's first additions),
+    // so that every gather of the pass gives the same bits
+    return cplx{__fmul_rn(v.x, f), __fmul_rn(v.y, f)};
   }
   static constexpr bool kShared = false;
 };
@@ -494,7 +496,7 @@ struct SmemScaled {
   __device__ __forceinline__ cplx ld(int b, int n) const {
     const cplx v = t.ld(b, n);
     const float f = SCALE == 1 ? (g ? __ldg(g + n) : (float)(n <= N / 2 ? n : n - N)) : fz;
-    return cplx{v.x * f, v.y * f};
+    return cplx{__fmul_rn(v.x, f), __fmul_rn(v.y, f)};
   }
   __device__ __forceinline__ void st(int b, int n, cplx v) const { t.st(b, n, v); }
   static constexpr bool kShared = true;

@@ -112,49 +112,73 @@ void particle_order_free(ParticleOrder* o) {
   *o = ParticleOrder{};
 }
 
+namespace {
+// Bins per side for n particles: about eight particles per bin (a bin is
+// then two lattice spacings on a side, six mesh cells at a PM factor of 3),
+// at most 1024 per side.
+int bins_per_side(long long n) {
+  int nb = (int)llround(cbrt((double)n) / 2.0);
+  if (nb < 1) nb = 1;
+  if (nb > 1024) nb = 1024;
+  return nb;
+}
+
+cudaError_t order_alloc(ParticleOrder* o, long long cap) {
+  const size_t c = (size_t)cap;
+  cudaError_t e = cudaMalloc(&o->alloc, sizeof(float) * 15 * c);
+  if (e == cudaSuccess) e = cudaMalloc(&o->alloc_id, sizeof(long long) * c);
+  if (e == cudaSuccess) e = cudaMalloc(&o->alloc_orig, sizeof(int) * c);
+  if (e == cudaSuccess) e = cudaMalloc(&o->key, sizeof(unsigned) * 2 * c);   // key, rank
+  if (e != cudaSuccess) {
+    particle_order_free(o);
+    return e;
+  }
+  for (int a = 0; a < 3; a++) {
+    o->x[a] = o->alloc + (0 + a) * c;
+    o->v[a] = o->alloc + (3 + a) * c;
+    o->dx1[a] = o->alloc + (6 + a) * c;
+    o->dx2[a] = o->alloc + (9 + a) * c;
+    o->f[a] = o->alloc + (12 + a) * c;
+  }
+  o->id = o->alloc_id;
+  o->orig = o->alloc_orig;
+  o->cap = cap;
+  return cudaSuccess;
+}
+
+cudaError_t order_bins(ParticleOrder* o, long long nbins) {
+  if (o->nbins >= nbins) return cudaSuccess;
+  release(o->cnt);
+  release(o->bsum);
+  o->nbins = 0;
+  cudaError_t e = cudaMalloc(&o->cnt, sizeof(unsigned) * (size_t)nbins);
+  if (e == cudaSuccess)
+    e = cudaMalloc(&o->bsum, sizeof(unsigned) * (size_t)cgscan::scratch_entries(nbins));
+  if (e != cudaSuccess) return e;
+  o->nbins = nbins;
+  return cudaSuccess;
+}
+}  // namespace
+
+cudaError_t particle_order_reserve(ParticleOrder* o, long long cap) {
+  cudaError_t e = cudaSuccess;
+  if (!o->alloc) e = order_alloc(o, cap);
+  else if (o->cap < cap) return cudaErrorInvalidValue;
+  const long long nb = bins_per_side(cap);
+  if (e == cudaSuccess) e = order_bins(o, nb * nb * nb);
+  return e;
+}
+
 cudaError_t particles_sort_cells(ParticleSoA* s, ParticleOrder* o, float L, cudaStream_t st) {
   const long long n = s->n;
   if (n < 2 || !(L > 0.0f)) return cudaSuccess;
   if (n > 0x7fffffffLL || !s->orig) return cudaErrorInvalidValue;
-  // about eight particles per bin (a bin is then two lattice spacings on a
-  // side, six mesh cells at a PM factor of 3), at most 1024 per side
-  int nb = (int)llround(cbrt((double)n) / 2.0);
-  if (nb < 1) nb = 1;
-  if (nb > 1024) nb = 1024;
+  const int nb = bins_per_side(n);
   const long long nbins = (long long)nb * nb * nb;
   cudaError_t e = cudaSuccess;
-  if (!o->alloc) {
-    const size_t c = (size_t)s->cap;
-    e = cudaMalloc(&o->alloc, sizeof(float) * 15 * c);
-    if (e == cudaSuccess) e = cudaMalloc(&o->alloc_id, sizeof(long long) * c);
-    if (e == cudaSuccess) e = cudaMalloc(&o->alloc_orig, sizeof(int) * c);
-    if (e == cudaSuccess) e = cudaMalloc(&o->key, sizeof(unsigned) * 2 * c);   // key, rank
-    if (e != cudaSuccess) {
-      particle_order_free(o);
-      return e;
-    }
-    for (int a = 0; a < 3; a++) {
-      o->x[a] = o->alloc + (0 + a) * c;
-      o->v[a] = o->alloc + (3 + a) * c;
-      o->dx1[a] = o->alloc + (6 + a) * c;
-      o->dx2[a] = o->alloc + (9 + a) * c;
-      o->f[a] = o->alloc + (12 + a) * c;
-    }
-    o->id = o->alloc_id;
-    o->orig = o->alloc_orig;
-    o->cap = s->cap;
-  }
+  if (!o->alloc && (e = order_alloc(o, s->cap)) != cudaSuccess) return e;
   if (n > o->cap) return cudaErrorInvalidValue;
-  if (o->nbins < nbins) {
-    release(o->cnt);
-    release(o->bsum);
-    o->nbins = 0;
-    e = cudaMalloc(&o->cnt, sizeof(unsigned) * (size_t)nbins);
-    if (e == cudaSuccess)
-      e = cudaMalloc(&o->bsum, sizeof(unsigned) * (size_t)cgscan::scratch_entries(nbins));
-    if (e != cudaSuccess) return e;
-    o->nbins = nbins;
-  }
+  if ((e = order_bins(o, nbins)) != cudaSuccess) return e;
   e = cudaMemsetAsync(o->cnt, 0, sizeof(unsigned) * (size_t)nbins, st);
   if (e != cudaSuccess) return e;
   const C3 x{{s->x[0], s->x[1], s->x[2]}};

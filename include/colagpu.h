@@ -235,6 +235,10 @@ int cg_batch_create(cg_batch** out, int nreal, const cg_realization_spec* specs,
 void cg_batch_destroy(cg_batch* b);
 /* Initial particles of realization i: nc^3 reference Particle structs. */
 int cg_batch_set_particles(cg_batch* b, int i, const void* particles, long long np);
+/* Cell-order sort of every realization's particles at every every-th move,
+ * inside the graph (0: never).  Default: the cg_sim policy (every sixth
+ * move from 2^23 particles).  Only before the first cg_batch_run. */
+int cg_batch_set_sort_interval(cg_batch* b, int every);
 /* Launch (recording first if needed) and wait; checks every density sum. */
 int cg_batch_run(cg_batch* b);
 int cg_batch_get_snapshot(cg_batch* b, int i, void* pmin_out);

@@ -46,3 +46,50 @@ def test_batch_matches_single_runs(gpu_lib, bbks_table):
         assert np.abs(p[ok] / ps[ok] - 1).max() < 1e-3
         sim.close()
     b.close()
+
+
+def _close_enough(got, ref, L):
+    """Positions of two float-atomic runs of the same realization: the bar
+    of the one-GPU workload's parity test (all but 1 in 10^5 particles
+    within 1e-5 of the box, none beyond 5e-5)."""
+    d = periodic_diff(got["x"], ref["x"], L).max(axis=1) / L
+    return (d > 1e-5).sum() <= len(d) // 100000 and d.max() <= 5e-5, d.max()
+
+
+@pytest.mark.parametrize("sort_every", [0, 3])
+def test_batch_at_batched_workload_sizes(gpu_lib, bbks_table, sort_every):
+    """Realizations of the batched workload's shape (128^3 particles on 384^3
+    meshes, L in 250-400 Mpc/h, 5-20 steps from z = 49) against the single
+    run of each, with the cell-order sort inside the graph (every third
+    move) and without it."""
+    from cola_halo_b200 import Simulation
+    from cola_halo_b200.batch import Batch
+    rng = np.random.default_rng(7)
+    specs, ics = [], []
+    for i in range(3):
+        L = float(rng.uniform(250, 400))
+        nsteps = int(rng.integers(5, 21))
+        specs.append(dict(nc=128, ngrid=384, boxsize=L, a_init=0.02, nsteps=nsteps, aout=1.0))
+        ics.append(lattice_particles(128, L, 300 + i, OM, 0.02, bbks_table))
+    b = Batch(specs, OM, nstreams=2)
+    b.set_sort_interval(sort_every)
+    for i, p in enumerate(ics):
+        b.set_particles(i, p)
+    b.run()
+    for i, s in enumerate(specs):
+        L = s["boxsize"]
+        got = b.snapshot(i)
+        sim = Simulation(128, 384, L, OM)
+        sim.set_sort_interval(sort_every)
+        sim.set_particles(ics[i], 0.02, 0.02)
+        ref = sim.run(Schedule.linear(0.02, 1.0, s["nsteps"]), zout=(0.0,))[-1][1]
+        ok, dmax = _close_enough(got, ref, L)
+        assert ok, (i, s, dmax)
+        np.testing.assert_array_equal(got["id"], ref["id"])
+        k, p, m = b.power_spectrum(i)
+        ks, ps, ms = sim.power_spectrum()
+        np.testing.assert_array_equal(m, ms)
+        upto = (np.arange(1, len(m) + 1) <= 64) & (m > 0)   # to the particle Nyquist
+        assert np.abs(p[upto] / ps[upto] - 1).max() < 1e-3
+        sim.close()
+    b.close()
