@@ -89,6 +89,10 @@ SIGNATURES = {
     "cg_set_schedule": (i32, [i32, i32, i32]),
     "cg_set_z_gather": (i32, [i32]),
     "cg_set_x_gather": (i32, [i32]),
+    "cg_deposit_variants": (i32, []),
+    "cg_get_deposit_variant": (i32, [i32]),
+    "cg_set_deposit_variant": (i32, [i32, i32]),
+    "cg_sim_tune_deposit": (i32, [P, P]),
     "cg_fft_r2c": (i32, [i32, P, P]),
     "cg_fft_c2r": (i32, [i32, P, P]),
     "cg_fft_time": (i32, [i32, i32, fptr, fptr]),

@@ -105,11 +105,28 @@ extern "C" int cg_get_schedule(int ngrid, int* green_variant, int* fx_variant) {
 }
 
 extern "C" int cg_set_schedule(int ngrid, int green_variant, int fx_variant) {
-  MeshSched s;
+  MeshSched s = pm_get_schedule(ngrid);   // keeps the deposit shape
   s.green = green_variant;
   s.fx = fx_variant;
   if (!valid(ngrid, s))
     return cg_set_error_from_lpt(CG_EINVAL, "cg_set_schedule: no such variant for this mesh size");
+  pm_set_schedule(ngrid, s);
+  return CG_OK;
+}
+
+extern "C" int cg_deposit_variants(void) { return PM_NUM_DEP_VARIANTS; }
+
+extern "C" int cg_get_deposit_variant(int ngrid) {
+  if (!pm_supported_mesh(ngrid))
+    return cg_set_error_from_lpt(CG_EUNSUPPORTED, "cg_get_deposit_variant: mesh size not built");
+  return pm_get_schedule(ngrid).dep;
+}
+
+extern "C" int cg_set_deposit_variant(int ngrid, int variant) {
+  if (!pm_supported_mesh(ngrid) || variant < 0 || variant >= PM_NUM_DEP_VARIANTS)
+    return cg_set_error_from_lpt(CG_EINVAL, "cg_set_deposit_variant: bad arguments");
+  MeshSched s = pm_get_schedule(ngrid);
+  s.dep = variant;
   pm_set_schedule(ngrid, s);
   return CG_OK;
 }
@@ -134,7 +151,7 @@ extern "C" int cg_autotune(int ngrid, int flags, float* ms_green, float* ms_fx) 
   std::lock_guard<std::mutex> lk(g_mu);
   if (!(flags & CG_TUNE_FORCE)) {
     if (g_tuned.count({dev, ngrid})) return CG_OK;
-    MeshSched c;
+    MeshSched c = pm_get_schedule(ngrid);
     if (cache_lookup(dev, ngrid, &c) && valid(ngrid, c)) {
       pm_set_schedule(ngrid, c);
       g_tuned.insert({dev, ngrid});
@@ -142,7 +159,9 @@ extern "C" int cg_autotune(int ngrid, int flags, float* ms_green, float* ms_fx) 
     }
   }
   if (ng == 1 && nf == 1) {   // nothing to choose below 256
-    pm_set_schedule(ngrid, MeshSched{});
+    MeshSched c = pm_get_schedule(ngrid);
+    c.green = c.fx = 0;
+    pm_set_schedule(ngrid, c);
     g_tuned.insert({dev, ngrid});
     return CG_OK;
   }
@@ -154,6 +173,7 @@ extern "C" int cg_autotune(int ngrid, int flags, float* ms_green, float* ms_fx) 
   e = pm_autotune(&p, 0, &best, ms_green, ms_fx);
   pm_plan_free(&p);
   if (e != cudaSuccess) return fail(CG_ECUDA, "cg_autotune", e);
+  best.dep = pm_get_schedule(ngrid).dep;
   pm_set_schedule(ngrid, best);
   g_tuned.insert({dev, ngrid});
   cache_store(dev, ngrid, best);

@@ -499,6 +499,17 @@ extern "C" int cg_sim_power_spectrum(cg_sim* s, int nbins, int flags, double* k,
   return CG_OK;
 }
 
+extern "C" int cg_sim_tune_deposit(cg_sim* s, float* ms) {
+  if (!s || s->ps.n < 1) return set_err(CG_EINVAL, "cg_sim_tune_deposit: no particles");
+  const float* x[3] = {s->ps.x[0], s->ps.x[1], s->ps.x[2]};
+  int best = 0;
+  CG_CHECK(pm_tune_deposit(&s->pm, x, s->ps.n, s->st, &best, ms), "tune deposit");
+  MeshSched m = pm_get_schedule(s->pm.N);
+  m.dep = best;
+  pm_set_schedule(s->pm.N, m);
+  return best;
+}
+
 extern "C" int cg_sim_keep_density(cg_sim* s, int keep) {
   if (!s) return set_err(CG_EINVAL, "cg_sim_keep_density: null handle");
   s->pm.keep_dens = keep != 0;

@@ -94,9 +94,11 @@ cudaError_t mesh_c2r(const MeshFFT* f, float2* spec, float* real, cudaStream_t s
 // kGreenCfg).  Variants other than 0 exist from 256 up (Green: up to 768).
 #define PM_NUM_FX_VARIANTS 3
 #define PM_NUM_GREEN_VARIANTS 3
+#define PM_NUM_DEP_VARIANTS 6
 struct MeshSched {
   int green = 0;
   int fx = 0;
+  int dep = 0;   // deposit shape (pm_kernels.cu kDepCfg)
 };
 
 // pm_kernels.cu
@@ -137,6 +139,11 @@ cudaError_t pm_forces(PmPlan* p, const float* const x[3], long long n,
                       float* const f[3], cudaStream_t st);
 // Individual stages (exposed for tests and timing).
 cudaError_t pm_deposit(PmPlan* p, const float* const x[3], long long n, cudaStream_t st);
+// Time every deposit variant on these positions (best of 3, each after a
+// fill) and return the fastest in *best, the times in ms[PM_NUM_DEP_VARIANTS]
+// (may be NULL).  Does not install it; leaves a deposit in the mesh.
+cudaError_t pm_tune_deposit(PmPlan* p, const float* const x[3], long long n, cudaStream_t st,
+                            int* best, float* ms);
 // deposit_tiled.cu: the same density mesh, each cell written once by the CTA
 // owning its 16^3 tile (particles binned by tile, warp-aggregated counts).
 cudaError_t pm_deposit_tiled(PmPlan* p, const float* const x[3], long long n, cudaStream_t st);

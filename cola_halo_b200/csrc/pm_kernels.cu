@@ -168,8 +168,13 @@ __global__ void __launch_bounds__(T) k_deposit(const float* __restrict__ x0,
 // only the order of the float additions changes.  Particles whose cloud
 // wraps in y or z, leaves the mesh in x, or has a buffer copy (x > x_right)
 // take the global path, as does every particle of a CTA whose box is large.
-constexpr int DEP_CHUNK = 512;                  // particles per CTA
-constexpr int DEP_VMAX = 3072;                   // cells: 12 KB of shared memory
+// Shapes of the box deposit (particles per CTA, box cells of shared memory),
+// a schedule parameter per mesh size chosen by cg_sim_tune_deposit on the
+// particles of a run (variant 0 by default); chunk 0: every cloud takes the
+// global atomics (k_deposit).
+struct DepCfg { int chunk, vmax; };
+constexpr DepCfg kDepCfg[PM_NUM_DEP_VARIANTS] = {
+    {512, 3072}, {256, 3072}, {1024, 6144}, {2048, 12288}, {512, 6144}, {0, 0}};
 
 __device__ __forceinline__ void deposit_one_box(float* __restrict__ box, const Cic& c, int bx,
                                                 int by, int bz, int ny, int nz, float wpar) {
@@ -202,7 +207,7 @@ __global__ void __launch_bounds__(T) k_deposit_box(const float* __restrict__ x0,
                                                    float* __restrict__ dens, int N, float scale,
                                                    float wpar, float x_right, float shiftx,
                                                    unsigned* __restrict__ err) {
-  __shared__ float box[VMAX];
+  extern __shared__ float box[];                  // VMAX cells
   __shared__ int red[6][T / 32];
   const long long base = (long long)blockIdx.x * CHUNK;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -1162,6 +1167,48 @@ int pm_set_x_gather(int mode) {
   return 0;
 }
 
+template <int V>
+void deposit_variant(PmPlan* p, const float* const x[3], long long n, cudaStream_t st) {
+  constexpr DepCfg c = kDepCfg[V];
+  prof_mark(st, CG_ST_DEPOSIT);
+  if constexpr (c.chunk == 0) {
+    k_deposit<<<grid_for(n), T, 0, st>>>(x[0], x[1], x[2], n, p->dens, p->N, p->scale, p->wpar,
+                                         p->x_right, p->shiftx, p->err);
+  } else {
+    k_deposit_box<c.chunk, c.vmax><<<(unsigned)((n + c.chunk - 1) / c.chunk), T,
+                                     sizeof(float) * c.vmax, st>>>(
+        x[0], x[1], x[2], n, p->dens, p->N, p->scale, p->wpar, p->x_right, p->shiftx, p->err);
+  }
+}
+
+template <int V>
+cudaError_t deposit_smem_attr() {
+  constexpr DepCfg c = kDepCfg[V];
+  if constexpr (c.chunk == 0) return cudaSuccess;
+  else return set_smem((const void*)k_deposit_box<c.chunk, c.vmax>, sizeof(float) * c.vmax);
+}
+
+// The CIC scatter into the mesh (which holds -1) with deposit variant v.
+void launch_deposit(PmPlan* p, const float* const x[3], long long n, int v, cudaStream_t st) {
+  static const cudaError_t attr = [] {
+    cudaError_t e = deposit_smem_attr<0>();
+    if (e == cudaSuccess) e = deposit_smem_attr<1>();
+    if (e == cudaSuccess) e = deposit_smem_attr<2>();
+    if (e == cudaSuccess) e = deposit_smem_attr<3>();
+    if (e == cudaSuccess) e = deposit_smem_attr<4>();
+    return e;
+  }();
+  (void)attr;
+  switch (v) {
+    case 1: deposit_variant<1>(p, x, n, st); break;
+    case 2: deposit_variant<2>(p, x, n, st); break;
+    case 3: deposit_variant<3>(p, x, n, st); break;
+    case 4: deposit_variant<4>(p, x, n, st); break;
+    case 5: deposit_variant<5>(p, x, n, st); break;
+    default: deposit_variant<0>(p, x, n, st);
+  }
+}
+
 bool pm_supported_mesh(int N) {
   MeshKernels k;
   return get_kernels(N, &k);
@@ -1491,25 +1538,8 @@ cudaError_t pm_deposit(PmPlan* p, const float* const x[3], long long n, cudaStre
   }
   p->dens_reset = false;
   if (n > 0) {
-    prof_mark(st, CG_ST_DEPOSIT);
     static const bool plain = getenv("COLAGPU_DEPOSIT") && getenv("COLAGPU_DEPOSIT")[0] == 'p';
-    if (plain)
-      k_deposit<<<grid_for(n), T, 0, st>>>(x[0], x[1], x[2], n, p->dens, p->N, p->scale,
-                                           p->wpar, p->x_right, p->shiftx, p->err);
-    else {
-      static const int chunk = getenv("COLAGPU_DEPOSIT_CHUNK") ? atoi(getenv("COLAGPU_DEPOSIT_CHUNK"))
-                                                               : DEP_CHUNK;
-      if (chunk == 256)
-        k_deposit_box<256, 3072><<<(unsigned)((n + 255) / 256), T, 0, st>>>(
-            x[0], x[1], x[2], n, p->dens, p->N, p->scale, p->wpar, p->x_right, p->shiftx, p->err);
-      else if (chunk == 1024)
-        k_deposit_box<1024, 6144><<<(unsigned)((n + 1023) / 1024), T, 0, st>>>(
-            x[0], x[1], x[2], n, p->dens, p->N, p->scale, p->wpar, p->x_right, p->shiftx, p->err);
-      else
-        k_deposit_box<DEP_CHUNK, DEP_VMAX><<<(unsigned)((n + DEP_CHUNK - 1) / DEP_CHUNK), T, 0,
-                                            st>>>(x[0], x[1], x[2], n, p->dens, p->N, p->scale,
-                                                  p->wpar, p->x_right, p->shiftx, p->err);
-    }
+    launch_deposit(p, x, n, plain ? PM_NUM_DEP_VARIANTS - 1 : sched_for(p->N).dep, st);
   }
   return cudaGetLastError();
 }
@@ -1681,6 +1711,46 @@ cudaError_t pm_forces(PmPlan* p, const float* const x[3], long long n, float* co
   if ((e = pm_r2c(p, st)) != cudaSuccess) return e;
   if ((e = pm_green_c2r(p, st)) != cudaSuccess) return e;
   return pm_interp(p, x, n, f, st);
+}
+
+cudaError_t pm_tune_deposit(PmPlan* p, const float* const x[3], long long n, cudaStream_t st,
+                            int* best, float* ms) {
+  if (n < 1) return cudaErrorInvalidValue;
+  const size_t n4 = (size_t)p->N * p->N * p->N / 4;
+  cudaEvent_t a, b;
+  cudaError_t e = cudaEventCreate(&a);
+  if (e != cudaSuccess) return e;
+  if ((e = cudaEventCreate(&b)) != cudaSuccess) {
+    cudaEventDestroy(a);
+    return e;
+  }
+  float tbest = 1e30f;
+  int vbest = 0;
+  for (int v = 0; v < PM_NUM_DEP_VARIANTS && e == cudaSuccess; v++) {
+    float t = 1e30f;
+    for (int r = 0; r < 3 && e == cudaSuccess; r++) {
+      prof_mark(st, CG_ST_FILL);
+      k_fill<<<grid_for((long long)n4), T, 0, st>>>(reinterpret_cast<float4*>(p->dens), n4, -1.0f);
+      cudaEventRecord(a, st);
+      launch_deposit(p, x, n, v, st);
+      cudaEventRecord(b, st);
+      e = cudaEventSynchronize(b);
+      float tr = 0.0f;
+      if (e == cudaSuccess) e = cudaEventElapsedTime(&tr, a, b);
+      if (e == cudaSuccess && tr < t) t = tr;
+    }
+    if (ms) ms[v] = t;
+    if (e == cudaSuccess && t < tbest) {
+      tbest = t;
+      vbest = v;
+    }
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  if (e == cudaSuccess) e = cudaGetLastError();
+  p->dens_reset = false;   // the mesh holds the last timed deposit
+  *best = vbest;
+  return e;
 }
 
 cudaError_t pm_power_spectrum(PmPlan* p, const float* const x[3], long long n, int nbins,

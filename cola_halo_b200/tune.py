@@ -1,0 +1,70 @@
+"""Run-level tuning of a realization's schedule choices that depend on the
+particles, not only on the mesh size (no reference counterpart).
+
+The FFT pass variants are tuned per mesh size on an empty plan
+(``cg_autotune``).  Two choices depend on how clustered the particles are,
+so they are tuned on a running realization:
+
+* the deposit shape (particles per CTA and shared-memory box,
+  ``cg_sim_tune_deposit``), timed on the particles of a partly evolved
+  realization;
+* the cell-order sort interval (``cg_sim_set_sort_interval``), which trades
+  the sort's cost against the locality it gives the deposit and the
+  interpolation over a whole realization.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+
+
+def _device_ms(lib, fn, max_marks):
+    """Device time of the library's kernels queued by fn() (event profile)."""
+    lib.cg_prof_begin(max_marks)
+    fn()
+    ms = (ctypes.c_double * _lib.NSTAGES)()
+    cnt = (ctypes.c_int * _lib.NSTAGES)()
+    lib.cg_prof_end(ms, cnt, _lib.NSTAGES)
+    return float(np.sum(np.frombuffer(ms, dtype=np.float64)))
+
+
+def tune_deposit(sim):
+    """Time every deposit shape on sim's current particles; installs the
+    fastest for sim's mesh size.  Returns (variant, ms per variant)."""
+    lib = sim.lib
+    nv = lib.cg_deposit_variants()
+    ms = (ctypes.c_float * nv)()
+    best = lib.cg_sim_tune_deposit(sim.h, ms)
+    if best < 0:
+        raise RuntimeError("cg_sim_tune_deposit: %s" % lib.cg_last_error().decode())
+    return best, [float(t) for t in ms]
+
+
+def tune_sort_interval(sim, reset, sched, candidates=(0, 2, 3, 4, 6, 8, 10)):
+    """Run one whole realization per candidate sort interval and keep the
+    fastest.  reset() puts the initial particles back; sched is the
+    realization's Schedule.  Steps are move, force, fused kick + drift (the
+    loop of main.c:162-206 without outputs).  Returns (interval, ms per
+    candidate); the fastest is installed on sim."""
+    lib = sim.lib
+    nsteps = sched.nloop - 1
+    times = {}
+
+    def realization():
+        for j in range(nsteps):
+            _, _, avel1, apos1 = sched.times(j + 1)
+            sim.move()
+            sim.forces()
+            sim.kick_drift(avel1, apos1)
+
+    for every in candidates:
+        sim.set_sort_interval(every)
+        reset()
+        realization()           # warm: first use allocates the sort's scratch
+        reset()
+        times[every] = _device_ms(lib, realization, 64 * nsteps)
+    best = min(times, key=times.get)
+    sim.set_sort_interval(best)
+    reset()
+    return best, times

@@ -332,6 +332,20 @@ int cg_set_schedule(int ngrid, int green_variant, int fx_variant);
  * into the transform's own swizzled tile, -1 (the default) by mesh size.
  * The three give bit-identical forces; COLAGPU_ZI=0/1/2 overrides. */
 int cg_set_z_gather(int mode);
+/* Shape of the CIC deposit per mesh size (no reference counterpart; the
+ * reference's PtoMesh is pm.c:209-279): variant v of cg_deposit_variants()
+ * sets the particles per CTA and the shared-memory box (512 / 3,072 cells,
+ * 256 / 3,072, 1,024 / 6,144, 2,048 / 12,288, 512 / 6,144, or global
+ * atomics only).  cg_sim_tune_deposit times every variant on the handle's
+ * current particles (best of 3 CUDA-event timings), installs the fastest
+ * for the handle's mesh size and returns it (or a negative CG_E* code); ms
+ * (may be NULL) receives each variant's time.  It leaves a deposit of the
+ * current positions in the density mesh.  All variants give the same
+ * density to float rounding. */
+int cg_deposit_variants(void);
+int cg_get_deposit_variant(int ngrid);
+int cg_set_deposit_variant(int ngrid, int variant);
+int cg_sim_tune_deposit(cg_sim* s, float* ms);
 /* How the strided x pass of the force step gathers its columns, for the
  * handles created afterwards: 0 direct loads, 1 TMA into the transform's
  * own swizzled tile, -1 (the default) by mesh size.  Bit-identical forces;

@@ -115,3 +115,38 @@ def test_reset_then_deposit_matches_kept_density(gpu_lib, bbks_table):
     assert np.abs(f0 - f1).max() < 1e-5 * scale
     fo, _ = R.pm_calculate_forces(x0, N, L, factor)
     assert np.abs(f0 - fo).max() < 2e-5 * scale
+
+
+def test_deposit_variants_match_oracle(gpu_lib, bbks_table):
+    """Every deposit shape (particles per CTA, shared-memory box, or global
+    atomics only) gives the oracle's density to float rounding, and the
+    tuner picks one of them."""
+    from cola_halo_b200 import Simulation
+    nc, factor, L = 32, 3, 200.0
+    N = nc * factor
+    p = lattice_particles(nc, L, 9, OM, 0.5, bbks_table)
+    x = R.wrap(p["x"], L)
+    _, dens = R.pm_calculate_forces(x, N, L, factor)
+    old = gpu_lib.cg_get_deposit_variant(N)
+    try:
+        for v in range(gpu_lib.cg_deposit_variants()):
+            assert gpu_lib.cg_set_deposit_variant(N, v) == 0
+            sim = Simulation(nc, N, L, OM)
+            sim.keep_density(True)
+            sim.set_particles(p, 0.5, 0.5)
+            sim.move()
+            sim.forces()
+            d = sim.get_mesh(0)
+            assert np.abs(d - dens).max() < 2e-5 * max(1.0, np.abs(dens).max()), v
+            sim.close()
+        sim = Simulation(nc, N, L, OM)
+        sim.set_particles(p, 0.5, 0.5)
+        sim.move()
+        from cola_halo_b200.tune import tune_deposit
+        best, ms = tune_deposit(sim)
+        assert 0 <= best < len(ms) and gpu_lib.cg_get_deposit_variant(N) == best
+        assert min(ms) == ms[best]
+        sim.close()
+    finally:
+        gpu_lib.cg_set_deposit_variant(N, old)
+    assert gpu_lib.cg_set_deposit_variant(N, 99) != 0
