@@ -64,6 +64,7 @@ SIGNATURES = {
     "cg_net_set_params": (i32, [P, P]),
     "cg_net_set_scales": (i32, [P, f32, f32, f32]),
     "cg_net_set_tensor_cores": (i32, [P, i32]),
+    "cg_net_set_conv_variant": (i32, [i32]),
     "cg_net_forward_host": (i32, [P, P, P]),
     "cg_net_backward_host": (i32, [P, P, P, P]),
     "cg_net_train_step": (i32, [P, P, P, f32, dptr]),

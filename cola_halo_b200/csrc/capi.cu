@@ -501,6 +501,8 @@ extern "C" int cg_sim_power_spectrum(cg_sim* s, int nbins, int flags, double* k,
 
 extern "C" int cg_sim_tune_deposit(cg_sim* s, float* ms) {
   if (!s || s->ps.n < 1) return set_err(CG_EINVAL, "cg_sim_tune_deposit: no particles");
+  // the deposit takes positions inside the box, as after cg_sim_move
+  CG_CHECK(dev_wrap(s->ps.x, s->ps.n, s->L, s->st), "wrap");
   const float* x[3] = {s->ps.x[0], s->ps.x[1], s->ps.x[2]};
   int best = 0;
   CG_CHECK(pm_tune_deposit(&s->pm, x, s->ps.n, s->st, &best, ms), "tune deposit");
@@ -583,6 +585,12 @@ extern "C" void cg_net_destroy(cg_net* h) {
 extern "C" int cg_net_set_tensor_cores(cg_net* h, int on) {
   if (!h) return set_err(CG_EINVAL, "cg_net_set_tensor_cores: NULL");
   h->n.use_tc = on ? 1 : 0;
+  return CG_OK;
+}
+
+extern "C" int cg_net_set_conv_variant(int variant) {
+  if (conv_tc_set_variant(variant) != 0)
+    return set_err(CG_EINVAL, "cg_net_set_conv_variant: variant must be -1, 0, 1 or 2");
   return CG_OK;
 }
 

@@ -61,3 +61,6 @@ cudaError_t conv_tc_backward_data(const __nv_bfloat16* g, int N, const __nv_bflo
                                   float* out_f, cudaStream_t st);
 // Device error word of the tensor-core kernels (bounded waits that gave up).
 unsigned conv_tc_error_word();
+// Pipeline of the tensor-core convolutions: -1 by mesh size, 0 two stages,
+// 1 one stage, 2 the line ring (128^3 only).  -1 returned on a bad value.
+int conv_tc_set_variant(int v);

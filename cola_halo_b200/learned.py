@@ -309,7 +309,7 @@ def pk_error(k, p, p_ref, kmax):
 
 def evaluate(nc, boxsize, sched, net, train_seeds, eval_seeds, table, *, omega_m=0.273,
              epochs=1, lr=2e-3, filter_nk=16, filter_seeds=4, net2=None, variants=(),
-             log=None):
+             net_variants=(), log=None):
     """Train on PM pairs, then judge plain-coarse and learned-coarse runs
     against the plain factor-3 run on held-out seeds: P(k) error up to half
     the particle Nyquist wavenumber, and the device time of each run's time
@@ -325,7 +325,10 @@ def evaluate(nc, boxsize, sched, net, train_seeds, eval_seeds, table, *, omega_m
     on forces when `fit` (fit_force_filter), then calibrated on the final
     P(k) when `calibrate` (calibrate_force_filter), both on the first
     `filter_seeds` training seeds: the error-versus-time curve between the
-    coarse and the fine mesh."""
+    coarse and the fine mesh.  Each (variant name, net) in `net_variants`
+    trains that net on the named variant's corrected force (its kernel and
+    transfer functions) over all training seeds, and judges the variant
+    with the net's correction added as "<name>_net"."""
     import time
 
     from .sim import Simulation
@@ -369,6 +372,17 @@ def evaluate(nc, boxsize, sched, net, train_seeds, eval_seeds, table, *, omega_m
             res["fit_s_" + name] = time.perf_counter() - t0
             res["filters_" + name] = fl.tolist()
         extra.append((name, sim, fl))
+    nets_on = []               # (name, realization, filters, net)
+    for base, nt in net_variants:
+        _, sim, fl = next(e for e in extra if e[0] == base)
+        t0 = time.perf_counter()
+        h3 = train_online(nt, sim, fine, sched, train_seeds, table, lr=lr, epochs=epochs,
+                          omega_m=omega_m, filters=fl, log=log)
+        sim.set_force_filters(None)
+        res["train_s_" + base + "_net"] = time.perf_counter() - t0
+        res["loss_first_" + base + "_net"] = float(np.mean(h3[:10]))
+        res["loss_last_" + base + "_net"] = float(np.mean(h3[-10:]))
+        nets_on.append((base + "_net", sim, fl, nt))
 
     lib = _lib.load()
     nst = _lib.NSTAGES
@@ -417,6 +431,7 @@ def evaluate(nc, boxsize, sched, net, train_seeds, eval_seeds, table, *, omega_m
             if net2 is not None:
                 runs.append(("filtered_net", coarse, filters, net2))
         runs += [(name, sim, fl, None) for name, sim, fl in extra]
+        runs += nets_on
         for name, sim, fl, nt in runs:
             sim.set_particles(p, sched.a_init, sched.a_init)
             s_x, t_x, w_x = timed_run(sim, sim.forces if fl is None else
@@ -435,9 +450,68 @@ def evaluate(nc, boxsize, sched, net, train_seeds, eval_seeds, table, *, omega_m
     for _, sim, _ in extra:
         sim.close()
     if "mf_fine" in res:
-        for name in ["coarse", "learned", "filtered", "filtered_net"] + [e[0] for e in extra]:
+        for name in (["coarse", "learned", "filtered", "filtered_net"] + [e[0] for e in extra] +
+                     [e[0] for e in nets_on]):
             if "mf_" + name in res:
                 res["mf_err_" + name] = mf_ratio_error(res["mf_" + name], res["mf_fine"])
         for key in [k for k in res if k.startswith("mf_") and not k.startswith("mf_err")]:
             res[key] = [int(c) for c in res[key]]
+    return res
+
+
+def evaluate_large(nc, boxsize, sched, coarse_ngrid, fine_factor, train_seeds, eval_seeds, table,
+                   *, nk=32, kernel=(0, 0, 2), iters=8, omega_m=0.273, log=None):
+    """The large-run comparison: a coarse mesh with the calibrated Fourier
+    correction (the CIC window divided out `kernel`[2] times and T(|n|) of
+    nk knots calibrated on the final P(k) of the training seeds) against
+    the plain run on the fine_factor mesh, which is the truth here, with
+    the plain coarse run beside it.  Per held-out seed: the device time of
+    each realization's time loop and the P(k) error up to half the particle
+    Nyquist wavenumber.  Returns a dict of per-seed rows and the fit."""
+    import time
+
+    from .sim import Simulation
+    fine = Simulation(nc, fine_factor * nc, boxsize, omega_m)
+    sim = Simulation(nc, coarse_ngrid, boxsize, omega_m)
+    sim.set_force_kernel(*kernel)
+    t0 = time.perf_counter()
+    fl, hist = calibrate_force_filter(sim, fine, sched, train_seeds, table, nk=nk, iters=iters,
+                                      omega_m=omega_m, log=log)
+    res = {"calibration_s": time.perf_counter() - t0, "calibration_train_err": hist,
+           "filters_last_step": fl[-1].tolist(), "seeds": []}
+    plain = Simulation(nc, coarse_ngrid, boxsize, omega_m)
+    lib = _lib.load()
+    nst = _lib.NSTAGES
+    kmax = 0.5 * np.pi * nc / boxsize
+    aout = output_scale_factors((0.0,))
+
+    def timed(s, force):
+        s.sync()
+        _lib.check(lib.cg_prof_begin(64 * sched.nloop), "cg_prof_begin")
+        run_time_loop(sched, aout, move=s.move, force=force, kick=s.kick, drift=s.drift,
+                      snapshot=lambda a, i: None, kick_drift=s.kick_drift)
+        ms = (ctypes.c_double * nst)()
+        cnt = (ctypes.c_int * nst)()
+        lib.cg_prof_end(ms, cnt, nst)
+        return s.snapshot(aout[0]), sum(ms) / 1e3
+
+    for seed in eval_seeds:
+        p = _lpt_particles(nc, boxsize, seed, omega_m, sched.a_init, table)
+        fine.set_particles(p, sched.a_init, sched.a_init)
+        s_f, t_f = timed(fine, fine.forces)
+        plain.set_particles(p, sched.a_init, sched.a_init)
+        s_c, t_c = timed(plain, plain.forces)
+        sim.set_particles(p, sched.a_init, sched.a_init)
+        s_l, t_l = timed(sim, filtered_force(sim, fl))
+        sim.set_force_filters(None)
+        k, pf, _ = power_spectrum_on(fine, s_f["x"], 1.0)
+        _, pc, _ = power_spectrum_on(fine, s_c["x"], 1.0)
+        _, pl, _ = power_spectrum_on(fine, s_l["x"], 1.0)
+        row = {"seed": seed, "fine_s": t_f, "coarse_s": t_c, "learned_s": t_l,
+               "err_coarse": pk_error(k, pc, pf, kmax), "err_learned": pk_error(k, pl, pf, kmax)}
+        res["seeds"].append(row)
+        if log:
+            log(str(row))
+    for s in (fine, sim, plain):
+        s.close()
     return res

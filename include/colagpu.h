@@ -203,6 +203,10 @@ int cg_net_set_params(cg_net* h, const float* params);
 int cg_net_set_scales(cg_net* h, float in_delta, float in_phi, float out_scale);
 /* 1: tcgen05 convolutions (default); 0: CUDA-core convolutions. */
 int cg_net_set_tensor_cores(cg_net* h, int on);
+/* Pipeline of the tensor-core convolutions, for every net: -1 by mesh size
+ * (the default), 0 two stages, 1 one stage, 2 the line ring that reuses
+ * input lines along y (128^3 meshes).  All give bit-identical outputs. */
+int cg_net_set_conv_variant(int variant);
 /* Host-array forward / backward (checks): in2 [v][2] scaled features,
  * out3 [v][3] raw outputs, grad3 = dLoss/dout3, grads [num_params]. */
 int cg_net_forward_host(cg_net* h, const float* in2, float* out3);
@@ -339,9 +343,10 @@ int cg_set_z_gather(int mode);
  * atomics only).  cg_sim_tune_deposit times every variant on the handle's
  * current particles (best of 3 CUDA-event timings), installs the fastest
  * for the handle's mesh size and returns it (or a negative CG_E* code); ms
- * (may be NULL) receives each variant's time.  It leaves a deposit of the
- * current positions in the density mesh.  All variants give the same
- * density to float rounding. */
+ * (may be NULL) receives each variant's time.  It wraps the positions into
+ * the box first (move_particles2's wrap) and leaves a deposit of them in
+ * the density mesh.  All variants give the same density to float
+ * rounding. */
 int cg_deposit_variants(void);
 int cg_get_deposit_variant(int ngrid);
 int cg_set_deposit_variant(int ngrid, int variant);

@@ -130,3 +130,29 @@ def test_training_on_pm_pairs_reduces_force_error(gpu_lib, bbks_table):
     for s in test:
         e_plain, e_learned = errs(s)
         assert e_learned < 0.9 * e_plain, (e_plain, e_learned)
+
+
+def test_line_ring_conv_bit_identical(gpu_lib):
+    """At 128^3 the tensor-core convolutions reuse input lines along y (the
+    line ring); its MMAs and operands are those of the one-stage kernel,
+    so forward outputs are bit-identical.  The parameter gradients agree to
+    the rounding of the weight gradient's float atomics, whose order varies
+    from run to run."""
+    from cola_halo_b200.learned import ConvNet
+    n = 128
+    rng = np.random.default_rng(5)
+    x = rng.normal(0, 1, (n, n, n, 2)).astype(np.float32)
+    g = rng.normal(0, 1, (n, n, n, 3)).astype(np.float32)
+    net = ConvNet(n, seed=3)
+    out, grads = [], []
+    try:
+        for v in (1, 2):
+            assert gpu_lib.cg_net_set_conv_variant(v) == 0
+            out.append(net.forward_host(x))
+            grads.append(net.backward_host(x, g))
+    finally:
+        gpu_lib.cg_net_set_conv_variant(-1)
+    np.testing.assert_array_equal(out[0], out[1])
+    np.testing.assert_allclose(grads[0], grads[1], rtol=1e-4, atol=1e-6 * np.abs(grads[0]).max())
+    assert gpu_lib.cg_net_set_conv_variant(5) != 0
+    net.close()
