@@ -603,6 +603,7 @@ def run_b200(args, cfg):
                             "%d force evaluations per realization, bytes averaged per "
                             "step" % sched.nloop},
             "gpu_launches": int(launches),
+            "gpu_launches_before_timed": int(launches0),
             "clocks": clk,
             "stages_ms": {k: round(v["ms"] / args.steps, 4) for k, v in stages.items()},
             "lpt_ms": lpt_s * 1e3,

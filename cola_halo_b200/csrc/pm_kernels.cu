@@ -273,12 +273,24 @@ __global__ void __launch_bounds__(T) k_deposit_box(const float* __restrict__ x0,
     }
   }
   __syncthreads();
-  for (int v = tid; v < vol; v += T) {
-    const float w = box[v];
-    if (w == 0.0f) continue;
-    const int kk = v % (int)nz, jj = (v / (int)nz) % (int)ny, ii = v / (int)(ny * nz);
-    const int gi = lo[0] + ii, gj = lo[1] + jj, gk = lo[2] + kk;
-    if (gi < N && gj < N && gk < N) atomicAdd(dens + cell(gi, gj, gk, N), w);
+  if (!use_box) return;
+  // flush: one 16-byte atomic per touched group of four z cells, aligned in
+  // the mesh (N is a multiple of 4, and every box cell lies inside the mesh:
+  // eligible clouds neither wrap nor leave it)
+  const int q0 = lo[2] >> 2;
+  const int nq = ((lo[2] + (int)nz - 1) >> 2) - q0 + 1;
+  const int nvec = (int)(nx * ny) * nq;
+  for (int v = tid; v < nvec; v += T) {
+    const int q = v % nq, jj = (v / nq) % (int)ny, ii = v / (nq * (int)ny);
+    const int k0 = 4 * (q0 + q) - lo[2];          // box z index of the group's first cell
+    const float* row = box + (ii * (int)ny + jj) * (int)nz;
+    float4 w;
+    w.x = (k0 >= 0 && k0 < nz) ? row[k0] : 0.0f;
+    w.y = (k0 + 1 >= 0 && k0 + 1 < nz) ? row[k0 + 1] : 0.0f;
+    w.z = (k0 + 2 >= 0 && k0 + 2 < nz) ? row[k0 + 2] : 0.0f;
+    w.w = (k0 + 3 >= 0 && k0 + 3 < nz) ? row[k0 + 3] : 0.0f;
+    if (w.x == 0.0f && w.y == 0.0f && w.z == 0.0f && w.w == 0.0f) continue;
+    atomicAdd(reinterpret_cast<float4*>(dens + cell(lo[0] + ii, lo[1] + jj, 4 * (q0 + q), N)), w);
   }
 }
 
@@ -364,7 +376,7 @@ __host__ __device__ constexpr int n_green_variants(int N) {
 struct FxCfg { int tk, rm; };
 struct GreenCfg { int byg, rm, minb; };
 constexpr FxCfg kFxCfg[PM_NUM_FX_VARIANTS] = {{8, 0}, {8, -1}, {16, 16}};
-constexpr GreenCfg kGreenCfg[PM_NUM_GREEN_VARIANTS] = {{4, 16, 3}, {8, 8, 2}, {8, 16, 2}};
+constexpr GreenCfg kGreenCfg[PM_NUM_GREEN_VARIANTS] = {{4, 16, 3}, {8, 8, 2}, {8, 16, 2}, {4, 16, 4}};
 __host__ __device__ constexpr int rm_x_default(int N) { return N >= 768 ? 8 : 16; }
 __host__ __device__ constexpr int fx_rm(int N, int v) {
   return kFxCfg[v].rm == 0 ? rm_x_default(N)
@@ -1080,6 +1092,7 @@ MeshKernels make_kernels(MeshSched s) {
     switch (s.green) {
       case 1: set_green<N, 1>(&k); break;
       case 2: set_green<N, 2>(&k); break;
+      case 3: set_green<N, 3>(&k); break;
       default: set_green<N, 0>(&k);
     }
   } else {
