@@ -928,10 +928,12 @@ def run_learned(args):
     net = ConvNet(nc, seed=7)
     net2 = ConvNet(nc, seed=8)
     net3 = ConvNet(nc, seed=9)
+    net4 = ConvNet(nc, seed=10)
     res = evaluate(nc, L, sched, net, list(range(1, args.train_seeds + 1)),
                    list(range(1001, 1001 + args.eval_seeds)), table, epochs=args.epochs,
                    filter_nk=16, net2=net2, variants=LEARNED_VARIANTS,
                    net_variants=((HEADLINE_VARIANT, net3),),
+                   net_first=(("net_calibrated_128", 128, (0, 0, 2), 32, net4),),
                    log=lambda s: print(s, file=sys.stderr, flush=True))
     seeds = res["seeds"]
     fine_s = float(np.mean([r["fine_s"] for r in seeds]))
@@ -980,7 +982,7 @@ def run_learned(args):
     # the coarse force (16 knots, least squares on 4 training seeds), alone
     # and with a second net trained on the filtered force
     for name in (["filtered", "filtered_net"] + [v[0] for v in LEARNED_VARIANTS] +
-                 [HEADLINE_VARIANT + "_net"]):
+                 [HEADLINE_VARIANT + "_net", "net_calibrated_128"]):
         if "err_" + name in seeds[0]:
             t = float(np.mean([r[name + "_s"] for r in seeds]))
             out[name] = {"s": t, "speedup_vs_plain_fine": fine_s / t,
@@ -1007,6 +1009,16 @@ def run_learned(args):
     if "train2_s" in res:
         out["filtered_net"]["train_s"] = res["train2_s"]
         out["filtered_net"]["loss_last"] = res["loss2_last"]
+    if "net_calibrated_128" in out:
+        out["net_calibrated_128"].update({
+            "what": "the conv net trained first on the window-corrected 128^3 force, then a "
+                    "transfer function T(|n|) of 32 knots calibrated on the final P(k) of runs "
+                    "with the net's correction in",
+            "train_s": res["train_s_net_calibrated_128"],
+            "loss_first": res["loss_first_net_calibrated_128"],
+            "loss_last": res["loss_last_net_calibrated_128"],
+            "fit_s": res["fit_s_net_calibrated_128"],
+            "calibration_train_err": [round(h, 4) for h in res["cal_hist_net_calibrated_128"]]})
     hn = HEADLINE_VARIANT + "_net"
     if hn in out:
         out[hn].update({"what": "the headline correction plus the conv net trained on what it "

@@ -191,7 +191,7 @@ def _final_positions(sim, sched, force):
 
 
 def calibrate_force_filter(sim, fine, sched, seeds, table, *, nk=16, base=None, iters=10,
-                           gamma=0.5, kmax=None, omega_m=0.273, log=None):
+                           gamma=0.5, kmax=None, omega_m=0.273, net=None, log=None):
     """Calibrate the transfer function of `sim`'s force on its final P(k):
     T_s(|n|) = base_s(|n|) C(|n|) with one C shared by all steps, updated
     multiplicatively from the ratio of the a = 1 power spectra of `sim` and
@@ -202,9 +202,11 @@ def calibrate_force_filter(sim, fine, sched, seeds, table, *, nk=16, base=None, 
     particle Nyquist wavenumber), held at its last value beyond.  An update
     that does not lower the training error (max over k <= kmax / 2 of
     |P/P_fine - 1|, mean over seeds) is discarded and retried with g
-    halved (g starts at `gamma`).  Returns the best iterate as an
-    (nsteps, nk) float32 array, with the error history of the `iters`
-    evaluations."""
+    halved (g starts at `gamma`).  With `net`, the runs add the conv net's
+    correction to the filtered force (the net trained first, the transfer
+    function calibrated on what the two give together).  Returns the best
+    iterate as an (nsteps, nk) float32 array, with the error history of the
+    `iters` evaluations."""
     nc, L, ng = fine.nc, fine.boxsize, sim.ngrid
     kmax = kmax or np.pi * nc / L
     if base is None:
@@ -225,7 +227,7 @@ def calibrate_force_filter(sim, fine, sched, seeds, table, *, nk=16, base=None, 
         ratios, errs = [], []
         for p, pf in truth:
             sim.set_particles(p, sched.a_init, sched.a_init)
-            x = _final_positions(sim, sched, filtered_force(sim, filt))
+            x = _final_positions(sim, sched, filtered_force(sim, filt, net))
             sim.set_force_filters(None)
             _, pc, _ = power_spectrum_on(fine, x, 1.0)
             ratios.append(pc / np.where(pf > 0, pf, 1.0))
@@ -309,7 +311,7 @@ def pk_error(k, p, p_ref, kmax):
 
 def evaluate(nc, boxsize, sched, net, train_seeds, eval_seeds, table, *, omega_m=0.273,
              epochs=1, lr=2e-3, filter_nk=16, filter_seeds=4, net2=None, variants=(),
-             net_variants=(), log=None):
+             net_variants=(), net_first=(), log=None):
     """Train on PM pairs, then judge plain-coarse and learned-coarse runs
     against the plain factor-3 run on held-out seeds: P(k) error up to half
     the particle Nyquist wavenumber, and the device time of each run's time
@@ -328,7 +330,12 @@ def evaluate(nc, boxsize, sched, net, train_seeds, eval_seeds, table, *, omega_m
     coarse and the fine mesh.  Each (variant name, net) in `net_variants`
     trains that net on the named variant's corrected force (its kernel and
     transfer functions) over all training seeds, and judges the variant
-    with the net's correction added as "<name>_net"."""
+    with the net's correction added as "<name>_net".  Each (name, ngrid,
+    kernel, nk, net) in `net_first` trains the net on that mesh's force
+    with the Green-step options `kernel`, then calibrates transfer functions
+    of nk knots on the final P(k) of the coarse runs with the net's
+    correction in (calibrate_force_filter with net), and judges the two
+    together as `name`."""
     import time
 
     from .sim import Simulation
@@ -373,6 +380,24 @@ def evaluate(nc, boxsize, sched, net, train_seeds, eval_seeds, table, *, omega_m
             res["filters_" + name] = fl.tolist()
         extra.append((name, sim, fl))
     nets_on = []               # (name, realization, filters, net)
+    extra_sims = []
+    for name, ng, kernel, nk, nt in net_first:
+        sim = Simulation(nc, ng, boxsize, omega_m)
+        sim.set_force_kernel(*kernel)
+        t0 = time.perf_counter()
+        h4 = train_online(nt, sim, fine, sched, train_seeds, table, lr=lr, epochs=epochs,
+                          omega_m=omega_m, log=log)
+        res["train_s_" + name] = time.perf_counter() - t0
+        res["loss_first_" + name] = float(np.mean(h4[:10]))
+        res["loss_last_" + name] = float(np.mean(h4[-10:]))
+        t0 = time.perf_counter()
+        fl, hist = calibrate_force_filter(sim, fine, sched, train_seeds[:filter_seeds], table,
+                                          nk=nk, omega_m=omega_m, net=nt, log=log)
+        res["fit_s_" + name] = time.perf_counter() - t0
+        res["cal_hist_" + name] = hist
+        res["filters_" + name] = fl.tolist()
+        nets_on.append((name, sim, fl, nt))
+        extra_sims.append(sim)
     for base, nt in net_variants:
         _, sim, fl = next(e for e in extra if e[0] == base)
         t0 = time.perf_counter()
@@ -434,7 +459,8 @@ def evaluate(nc, boxsize, sched, net, train_seeds, eval_seeds, table, *, omega_m
         runs += nets_on
         for name, sim, fl, nt in runs:
             sim.set_particles(p, sched.a_init, sched.a_init)
-            s_x, t_x, w_x = timed_run(sim, sim.forces if fl is None else
+            s_x, t_x, w_x = timed_run(sim, sim.forces if fl is None and nt is None else
+                                      (lambda s=sim, n=nt: n.forces(s)) if fl is None else
                                       filtered_force(sim, fl, nt))
             sim.set_force_filters(None)
             _, px, _ = power_spectrum_on(fine, s_x["x"], 1.0)
@@ -448,6 +474,8 @@ def evaluate(nc, boxsize, sched, net, train_seeds, eval_seeds, table, *, omega_m
     fine.close()
     coarse.close()
     for _, sim, _ in extra:
+        sim.close()
+    for sim in extra_sims:
         sim.close()
     if "mf_fine" in res:
         for name in (["coarse", "learned", "filtered", "filtered_net"] + [e[0] for e in extra] +

@@ -76,8 +76,9 @@ def test_autotune_times_installs_and_caches(gpu_lib, tmp_path):
     old = os.environ.get("COLAGPU_TUNE_CACHE")
     os.environ["COLAGPU_TUNE_CACHE"] = str(cache)
     try:
-        mg = (ctypes.c_float * 3)()
-        mf = (ctypes.c_float * 3)()
+        ng, nf = _variants(gpu_lib, 384)
+        mg = (ctypes.c_float * ng)()
+        mf = (ctypes.c_float * nf)()
         assert gpu_lib.cg_autotune(384, 1, mg, mf) == 0, gpu_lib.cg_last_error()
         g, f = _schedule(gpu_lib, 384)
         assert all(t > 0 for t in mg) and all(t > 0 for t in mf)
