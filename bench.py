@@ -448,8 +448,12 @@ def run_b200(args, cfg):
     # interval over whole realizations; then the warm-up again, so the timed
     # steps continue the schedule from the same point
     from cola_halo_b200.tune import tune_deposit, tune_sort_interval
-    dep_best, dep_ms = tune_deposit(sim)
-    sort_best, sort_ms = tune_sort_interval(sim, reset, sched)
+    # COLAGPU_RUN_TUNE_CACHE=file keeps these choices for later runs, as
+    # COLAGPU_TUNE_CACHE keeps the FFT schedule (a profiled rerun then
+    # launches what the plain run chose)
+    run_cache = os.environ.get("COLAGPU_RUN_TUNE_CACHE")
+    dep_best, dep_ms = tune_deposit(sim, cache=run_cache)
+    sort_best, sort_ms = tune_sort_interval(sim, reset, sched, cache=run_cache)
     os.environ["COLAGPU_SORT_EVERY"] = str(sort_best)      # the drop-in run below too
     for i in range(args.warmup):
         step(i)

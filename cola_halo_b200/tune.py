@@ -13,10 +13,32 @@ so they are tuned on a running realization:
   interpolation over a whole realization.
 """
 import ctypes
+import json
+import os
 
 import numpy as np
 
 from . import _lib
+
+
+def _cache_get(cache, key):
+    """A choice stored by an earlier run in the JSON file `cache` (or None)."""
+    if not cache or not os.path.exists(cache):
+        return None
+    with open(cache) as f:
+        return json.load(f).get(key)
+
+
+def _cache_put(cache, key, value):
+    if not cache:
+        return
+    d = {}
+    if os.path.exists(cache):
+        with open(cache) as f:
+            d = json.load(f)
+    d[key] = value
+    with open(cache, "w") as f:
+        json.dump(d, f)
 
 
 def _device_ms(lib, fn, max_marks):
@@ -29,29 +51,45 @@ def _device_ms(lib, fn, max_marks):
     return float(np.sum(np.frombuffer(ms, dtype=np.float64)))
 
 
-def tune_deposit(sim):
+def tune_deposit(sim, cache=None):
     """Time every deposit shape on sim's current particles; installs the
-    fastest for sim's mesh size.  Returns (variant, ms per variant)."""
+    fastest for sim's mesh size.  Returns (variant, ms per variant).  With
+    `cache` (a JSON file), a choice stored there by an earlier run for this
+    mesh size is installed without timing, and a new one is stored."""
     lib = sim.lib
+    key = "deposit_%d" % sim.ngrid
+    got = _cache_get(cache, key)
+    if got is not None:
+        _lib.check(lib.cg_set_deposit_variant(sim.ngrid, int(got)), "cg_set_deposit_variant")
+        return int(got), []
     nv = lib.cg_deposit_variants()
     ms = (ctypes.c_float * nv)()
     best = lib.cg_sim_tune_deposit(sim.h, ms)
     if best < 0:
         raise RuntimeError("cg_sim_tune_deposit: %s" % lib.cg_last_error().decode())
+    _cache_put(cache, key, best)
     return best, [float(t) for t in ms]
 
 
-def tune_sort_interval(sim, reset, sched, candidates=(0, 2, 3, 4, 6, 8, 10), reps=3):
+def tune_sort_interval(sim, reset, sched, candidates=(0, 2, 3, 4, 6, 8, 10), reps=3,
+                       cache=None):
     """Run whole realizations per candidate sort interval and keep the
     fastest.  reset() puts the initial particles back; sched is the
     realization's Schedule.  Steps are move, force, fused kick + drift (the
     loop of main.c:162-206 without outputs).  Each candidate is timed as
     the best of `reps` realizations (the differences between intervals are
     a few per cent, close to the spread of single runs).  Returns (interval,
-    ms per candidate); the fastest is installed on sim."""
+    ms per candidate); the fastest is installed on sim.  `cache` as for
+    tune_deposit (keyed by particle count and mesh size)."""
     lib = sim.lib
     nsteps = sched.nloop - 1
     times = {}
+    key = "sort_%d_%d" % (sim.nc, sim.ngrid)
+    got = _cache_get(cache, key)
+    if got is not None:
+        sim.set_sort_interval(int(got))
+        reset()
+        return int(got), times
 
     def realization():
         for j in range(nsteps):
@@ -73,4 +111,5 @@ def tune_sort_interval(sim, reset, sched, candidates=(0, 2, 3, 4, 6, 8, 10), rep
     best = min(times, key=times.get)
     sim.set_sort_interval(best)
     reset()
+    _cache_put(cache, key, best)
     return best, times
