@@ -368,13 +368,10 @@ def run_b200(args, cfg):
         if dist:
             dist.barrier()
 
+    from cola_halo_b200 import replicas
+
     def allmax(v):
-        if not dist:
-            return v
-        import torch
-        t = torch.tensor([v], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return replicas.allmax(v, dist)
 
     from cola_halo_b200 import Simulation, _lib
     from cola_halo_b200.bbks import write_bbks_table
@@ -388,7 +385,7 @@ def run_b200(args, cfg):
     N = nc * factor
     npart = nc ** 3
     sched = Schedule.linear(cfg["a_init"], 1.0, cfg["nsteps"])
-    seed = cfg["seed"] + rank
+    seed = replicas.replica_seed(cfg["seed"], rank)
     table = write_bbks_table(os.path.join(tempfile.mkdtemp(), "bbks.dat"))
 
     # ---- 2LPT initial conditions on the GPU through the drop-in API,
@@ -483,7 +480,7 @@ def run_b200(args, cfg):
     sim.sync()
     barrier()
     ms_max = allmax(ms)
-    value = world * npart * args.steps / (ms_max / 1e3)
+    value = replicas.whole_job_rate(npart, args.steps, ms_max, world)
 
     stages = {}
     for s in range(_lib.NSTAGES):

@@ -931,7 +931,7 @@ __global__ void __launch_bounds__(T, N >= 1024 ? 3 : 4) k_zi_sw(const __grid_con
 //   1  TMA into a landing area, copied into the padded tile (k_zi_tma)
 //   2  TMA into the swizzled dense tile itself (k_zi_sw)
 // All three give bit-identical output.  Default: 2, the fastest at 384^3
-// (0.313 ms per launch against 0.344 and 0.373 for 1 and 0) and at 768^3
+// (0.104 ms per launch against 0.115 and 0.124 for 1 and 0) and at 768^3
 // (0.81 ms against 1.15 and 0.97), per launch inside the 10-step runs;
 // cg_set_z_gather, or COLAGPU_ZI=0/1/2, selects one.
 std::atomic<int> g_zmode{-1};

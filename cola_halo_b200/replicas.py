@@ -15,6 +15,20 @@ def rank_world():
             int(os.environ.get("LOCAL_RANK", "0")))
 
 
+def replica_seed(base_seed, rank):
+    """The seed of rank `rank`'s realization: base + rank, as the reference
+    numbers its realizations (main.c:117-121, random_seed + irealization)."""
+    return int(base_seed) + int(rank)
+
+
+def whole_job_rate(units_per_rank, steps, ms_max, world):
+    """Throughput of the whole job: every rank processed units_per_rank x
+    steps units, and the job took the slowest rank's device time ms_max."""
+    if ms_max <= 0:
+        raise ValueError("device time must be positive")
+    return world * float(units_per_rank) * steps / (ms_max / 1e3)
+
+
 def shard(items, rank, world):
     """Round-robin share of `items` for `rank` of `world` (seed i -> rank i % world)."""
     if world < 1 or not (0 <= rank < world):
