@@ -94,10 +94,15 @@ PmPlan view(const PmPlan& bufs, const MeshFFT& tab, int N, int factor, float L) 
   p.twH = tab.twH;
   p.mesh_bytes = sizeof(float) * (size_t)N * N * N;
   p.spec_bytes = sizeof(float2) * (size_t)(N / 2 + 1) * N * N;
-  p.ztm_ok = false;    // the stream's TMA maps describe its largest mesh, not this one
-  p.zsw_ok = false;
-  p.xsw_ok = false;
-  p.keep_dens = true;  // meshes of several sizes share the buffer: fill every step
+  if (N != bufs.N) {
+    // the stream's TMA maps describe its largest mesh, not this one
+    p.ztm_ok = false;
+    p.zsw_ok = false;
+    p.xsw_ok = false;
+  }
+  // the realization's first deposit fills the shared buffer (dens_reset
+  // false); from then on each z r2c leaves -1 behind for the next one
+  p.keep_dens = false;
   p.dens_reset = false;
   return p;
 }
