@@ -164,16 +164,22 @@ cudaError_t record_realization(cg_batch* b, Real& r, StreamBufs& sb) {
     }
     float dda, q1, q2;
     b->ct->kick(a_v, a_x, (float)avel1, &dda, &q1, &q2);
-    if ((e = dev_kick(r.ps.v, cf, c1, c2, r.ps.n, b->ct->om32, dda, q1, q2, st)) != cudaSuccess)
-      return e;
-    a_v = (float)avel1;
     if (apos0 < aout && aout <= avel1) {
+      // the output falls between the kick and the drift
+      if ((e = dev_kick(r.ps.v, cf, c1, c2, r.ps.n, b->ct->om32, dda, q1, q2, st)) != cudaSuccess)
+        return e;
+      a_v = (float)avel1;
       if ((e = snapshot()) != cudaSuccess) return e;
       break;
     }
+    // kick, then drift with the kicked velocity, in one pass (bit-identical
+    // to the two kernels, as cg_sim_kick_drift)
+    a_v = (float)avel1;
     float dyyy, da1, da2;
     b->ct->drift(a_x, a_v, (float)apos1, &dyyy, &da1, &da2);
-    if ((e = dev_drift(r.ps.x, cv, c1, c2, r.ps.n, dyyy, da1, da2, st)) != cudaSuccess) return e;
+    if ((e = dev_kick_drift(r.ps.x, r.ps.v, cf, c1, c2, r.ps.n, b->ct->om32, dda, q1, q2, dyyy,
+                            da1, da2, st)) != cudaSuccess)
+      return e;
     a_x = (float)apos1;
   }
   r.nforce = iforce;

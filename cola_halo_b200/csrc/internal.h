@@ -49,10 +49,6 @@ struct PmPlan {
   float2* twH;              // exp(-2 pi i k/(N/2)), k < N/2
   double* dsum;             // device: sum of the density mesh (check)
   double* pk_acc;           // device: 3 N doubles of power-spectrum bin sums
-  unsigned* keys;           // cell-sorted deposit: per-particle bin key
-  float4* sorted;           //   positions in bin order
-  unsigned* bins;           //   counts, offsets, cursors, scan block sums
-  long long sort_cap;       //   particles the two arrays above hold
   unsigned* err;            // device: error word
   size_t mesh_bytes;        // bytes of one real mesh
   size_t spec_bytes;        // bytes of one half spectrum
@@ -144,9 +140,6 @@ cudaError_t pm_deposit(PmPlan* p, const float* const x[3], long long n, cudaStre
 // (may be NULL).  Does not install it; leaves a deposit in the mesh.
 cudaError_t pm_tune_deposit(PmPlan* p, const float* const x[3], long long n, cudaStream_t st,
                             int* best, float* ms);
-// deposit_tiled.cu: the same density mesh, each cell written once by the CTA
-// owning its 16^3 tile (particles binned by tile, warp-aggregated counts).
-cudaError_t pm_deposit_tiled(PmPlan* p, const float* const x[3], long long n, cudaStream_t st);
 // dens -> spec transformed along z and x (+ density sum into dsum)
 cudaError_t pm_r2c(PmPlan* p, cudaStream_t st);
 // spec -> y transform, Green/gradient -> three force meshes fmesh[a]

@@ -1524,25 +1524,11 @@ void pm_plan_free(PmPlan* p) {
   cudaFree(p->twH);
   cudaFree(p->dsum);
   cudaFree(p->pk_acc);
-  cudaFree(p->keys);
-  cudaFree(p->sorted);
-  cudaFree(p->bins);
   cudaFree(p->err);
   memset(p, 0, sizeof(*p));
 }
 
 cudaError_t pm_deposit(PmPlan* p, const float* const x[3], long long n, cudaStream_t st) {
-  // COLAGPU_DEPOSIT=tiled selects the cell-sorted deposit (deposit_tiled.cu);
-  // the default global-atomic scatter measured faster at 256^3 / 768^3.
-  static const bool tiled_deposit =
-      getenv("COLAGPU_DEPOSIT") && getenv("COLAGPU_DEPOSIT")[0] == 't';
-  if (tiled_deposit) {
-    cudaError_t e = pm_deposit_tiled(p, x, n, st);
-    if (e != cudaErrorNotSupported) {
-      p->dens_reset = false;
-      return e;
-    }
-  }
   // scatter with global float atomics into a mesh filled with -1
   const size_t n4 = (size_t)p->N * p->N * p->N / 4;
   if (!p->dens_reset) {   // else the last z r2c left the mesh at -1 already

@@ -57,8 +57,12 @@ def test_handle_api_run_matches_reference(gpu_lib, ref, bbks_table, nc, factor, 
         assert a_r == a_g
         dx = periodic_diff(s_g["x"], s_r["x"], L)
         assert dx.max() <= 1e-5 * L, dx.max() / L
-        dv = np.abs(s_g["v"] - s_r["v"])
-        assert dv.max() <= 1e-3 * np.abs(s_r["v"]).max()
+        dv = np.abs(s_g["v"].astype(np.float64) - s_r["v"])
+        vmax = np.abs(s_r["v"]).max()
+        # rms over all particles at the position bar's level; the largest
+        # single difference (a particle in a halo core) within 1e-3
+        assert np.sqrt(np.mean(dv ** 2)) <= 1e-5 * vmax
+        assert dv.max() <= 1e-3 * vmax
         np.testing.assert_array_equal(s_g["id"], s_r["id"])
 
 
