@@ -180,7 +180,11 @@ struct SmemLine {
   cplx* s;
   __device__ __forceinline__ cplx ld(int b, int n) const { return s[b * SB + n + (n >> 4)]; }
   __device__ __forceinline__ void st(int b, int n, cplx v) const { s[b * SB + n + (n >> 4)] = v; }
+  // element n of line b sits at line(b) + n + n/16: a stage whose legs are
+  // a multiple of 16 apart reaches them at constant offsets from one base
+  __device__ __forceinline__ cplx* line(int b) const { return s + b * SB; }
   static constexpr bool kShared = true;
+  static constexpr bool kPad16 = true;
 };
 // Line pitch >= the padded length, rounded to 1 (mod 16) elements: when
 // consecutive threads walk across lines (same n, consecutive b), the 8-byte
@@ -240,6 +244,7 @@ struct Gmem {
   float2* p;
   size_t ls;
   size_t es;
+  static constexpr bool kPad16 = false;
   __device__ __forceinline__ cplx ld(int b, int n) const {
     const float2 v = __ldg(p + b * ls + (size_t)n * es);
     return cplx{v.x, v.y};
@@ -249,6 +254,14 @@ struct Gmem {
   }
   static constexpr bool kShared = false;
 };
+
+// Accessors that declare kPad16 = true (SmemLine) take the constant-offset
+// paths of stage_io; every other accessor goes through ld / st.
+template <class A, class = void> struct HasPad16 { static constexpr bool v = false; };
+template <class A> struct HasPad16<A, decltype((void)A::kPad16)> {
+  static constexpr bool v = A::kPad16;
+};
+template <class A> __host__ __device__ constexpr bool has_pad16() { return HasPad16<A>::v; }
 
 // T = 32: the tile belongs to one warp (thread = lane, barriers are warp
 // barriers), so warps of a CTA run their tiles independently.  Otherwise the
@@ -275,8 +288,15 @@ __device__ __forceinline__ void stage_io(const In& in, const Out& out,
     if (TOTAL % T == 0 || idx < TOTAL) {
       const int b = LINE_MAJOR ? idx / NBF : idx % B;
       const int j = LINE_MAJOR ? idx % NBF : idx / B;
+      if constexpr (has_pad16<In>() && NBF % 16 == 0) {
+        // legs j + r NBF, r NBF a multiple of 16: padded offsets r NBF 17/16
+        const cplx* p = in.line(b) + j + (j >> 4);
 #pragma unroll
-      for (int r = 0; r < R; r++) v[q][r] = in.ld(b, j + r * NBF);
+        for (int r = 0; r < R; r++) v[q][r] = p[r * (NBF + NBF / 16)];
+      } else {
+#pragma unroll
+        for (int r = 0; r < R; r++) v[q][r] = in.ld(b, j + r * NBF);
+      }
     }
   }
   if (inplace) tile_sync<T>();
@@ -294,8 +314,25 @@ __device__ __forceinline__ void stage_io(const In& in, const Out& out,
       }
       dft<R, DIR>(v[q]);
       const int base = (j / NS) * NS * R + jm;
+      if constexpr (has_pad16<Out>() && NS % 16 == 0) {
+        // outputs base + r NS, r NS a multiple of 16
+        cplx* p = out.line(b) + base + (base >> 4);
 #pragma unroll
-      for (int r = 0; r < R; r++) out.st(b, base + r * NS, v[q][r]);
+        for (int r = 0; r < R; r++) p[r * (NS + NS / 16)] = v[q][r];
+      } else if constexpr (has_pad16<Out>() && NS == 1 && R == 16) {
+        // outputs 16 j + r, r < 16: padded 17 j + r
+        cplx* p = out.line(b) + 17 * j;
+#pragma unroll
+        for (int r = 0; r < R; r++) p[r] = v[q][r];
+      } else if constexpr (has_pad16<Out>() && NS == 1 && R == 8) {
+        // outputs 8 j + r, r < 8: padded 8 j + j/2 + r
+        cplx* p = out.line(b) + 8 * j + (j >> 1);
+#pragma unroll
+        for (int r = 0; r < R; r++) p[r] = v[q][r];
+      } else {
+#pragma unroll
+        for (int r = 0; r < R; r++) out.st(b, base + r * NS, v[q][r]);
+      }
     }
   }
 }
