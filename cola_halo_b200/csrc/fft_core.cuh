@@ -167,6 +167,41 @@ __host__ __device__ constexpr bool supported_length(int L, int RM = 16) {
   return prod == L && L >= 2;
 }
 
+// ------------------------------------------------ per-stage twiddle rows
+// The twiddle table of length L is followed by one block per distinct stage
+// (NS, R), NS > 1, of the radix-16 and the radix-8 schedules of L: NS rows
+// of stage_rp(R) entries, row jm holding W_L^{jm r STEP} for r = 1 .. R-1
+// (STEP = L / (NS R); the same values as entries jm r STEP of the table)
+// and a zero pad to an even count.  A butterfly's R-1 twiddles are then one
+// contiguous, 16-byte-aligned run read by float4 loads at constant offsets.
+__host__ __device__ constexpr int stage_rp(int R) { return (R - 1 + 1) / 2 * 2; }
+
+// Offset of stage (NS, R)'s block in a table for length L, or -1; with
+// NS = 0 the table's total length.
+__host__ __device__ constexpr int stage_tw_offset(int L, int NS, int R) {
+  int off = L;
+  for (int pass = 0; pass < 2; pass++) {
+    const int rm = pass == 0 ? 16 : 8;
+    if (!supported_length(L, rm)) continue;
+    for (int st = 1; st < num_stages(L, rm); st++) {
+      const int ns = ns_before(L, st, rm), r = radix_at(L, st, rm);
+      bool seen = false;      // the same (ns, r) earlier in the walk
+      for (int p2 = 0; p2 <= pass && !seen; p2++) {
+        const int rm2 = p2 == 0 ? 16 : 8;
+        if (!supported_length(L, rm2)) continue;
+        const int last = p2 < pass ? num_stages(L, rm2) : st;
+        for (int s2 = 1; s2 < last; s2++)
+          if (ns_before(L, s2, rm2) == ns && radix_at(L, s2, rm2) == r) seen = true;
+      }
+      if (seen) continue;
+      if (NS > 0 && ns == NS && r == R) return off;
+      off += ns * stage_rp(r);
+    }
+  }
+  return NS > 0 ? -1 : off;
+}
+__host__ __device__ constexpr int twiddle_table_len(int L) { return stage_tw_offset(L, 0, 0); }
+
 // ------------------------------------------------------------ tile access
 // The first stage reads its legs j + r L/R and the last writes its outputs
 // (j/NS) NS R + (j mod NS) + r NS; with consecutive threads on consecutive
@@ -239,6 +274,22 @@ struct SmemSw8 {
   static constexpr bool kShared = true;
 };
 
+// Global lines with compile-time strides: element n of line b at
+// p[b * LS + n * ES] (a stage's legs then sit at constant offsets).
+template <size_t LS, size_t ES>
+struct GmemC {
+  float2* p;
+  __device__ __forceinline__ cplx ld(int b, int n) const {
+    const float2 v = __ldg(p + (size_t)b * LS + (size_t)n * ES);
+    return cplx{v.x, v.y};
+  }
+  __device__ __forceinline__ void st(int b, int n, cplx v) const {
+    p[(size_t)b * LS + (size_t)n * ES] = make_float2(v.x, v.y);
+  }
+  static constexpr bool kShared = false;
+  static constexpr bool kPad16 = false;
+};
+
 // Global lines: element n of line b at p[b * ls + n * es].
 struct Gmem {
   float2* p;
@@ -307,10 +358,23 @@ __device__ __forceinline__ void stage_io(const In& in, const Out& out,
       const int b = LINE_MAJOR ? idx / NBF : idx % B;
       const int j = LINE_MAJOR ? idx % NBF : idx / B;
       const int jm = NS == 1 ? 0 : j % NS;
-      if (NS > 1) {
-        constexpr int STEP = L / (NS * R);
+      if constexpr (NS > 1) {
+        constexpr int OFF = stage_tw_offset(L, NS, R);
+        if constexpr (OFF >= 0) {
+          // the stage's row jm: R-1 twiddles, two per 16-byte load
+          const float4* t4 = reinterpret_cast<const float4*>(tw + OFF + jm * stage_rp(R));
 #pragma unroll
-        for (int r = 1; r < R; r++) v[q][r] = cmul(v[q][r], twiddle<DIR>(tw, jm * r * STEP));
+          for (int i = 0; i < stage_rp(R) / 2; i++) {
+            const float4 w = __ldg(t4 + i);
+            const int r1 = 2 * i + 1, r2 = 2 * i + 2;
+            v[q][r1] = cmul(v[q][r1], DIR < 0 ? cplx{w.x, w.y} : cplx{w.x, -w.y});
+            if (r2 < R) v[q][r2] = cmul(v[q][r2], DIR < 0 ? cplx{w.z, w.w} : cplx{w.z, -w.w});
+          }
+        } else {
+          constexpr int STEP = L / (NS * R);
+#pragma unroll
+          for (int r = 1; r < R; r++) v[q][r] = cmul(v[q][r], twiddle<DIR>(tw, jm * r * STEP));
+        }
       }
       dft<R, DIR>(v[q]);
       const int base = (j / NS) * NS * R + jm;

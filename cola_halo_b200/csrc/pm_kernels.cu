@@ -407,8 +407,8 @@ __global__ void __launch_bounds__(T) k_fz(DensPtr<RESET> dens,
   const SmemLine<cgfft::line_pitch<H>()> mid{reinterpret_cast<cplx*>(smraw)};
   const int x = blockIdx.y;
   const int y0 = blockIdx.x * TY;
-  const Gmem gin{reinterpret_cast<float2*>(const_cast<float*>(dens)) + ((size_t)x * N + y0) * H,
-                 (size_t)H, 1};
+  const cgfft::GmemC<H, 1> gin{reinterpret_cast<float2*>(const_cast<float*>(dens)) +
+                              ((size_t)x * N + y0) * H};
   cgfft::fft_io<H, TY, T, true, -1>(gin, mid, mid, twH);
   if constexpr (RESET) {
     __syncthreads();    // every thread's loads of the lines are done
@@ -439,7 +439,7 @@ __global__ void __launch_bounds__(T) k_fy(float2* __restrict__ spec,
                                           const float2* __restrict__ twN) {
   extern __shared__ __align__(16) unsigned char smraw[];
   const SmemLine<cgfft::line_pitch<N>()> mid{reinterpret_cast<cplx*>(smraw)};
-  const Gmem g{spec + (size_t)blockIdx.x * BY * N, (size_t)N, 1};
+  const cgfft::GmemC<N, 1> g{spec + (size_t)blockIdx.x * BY * N};
   cgfft::fft_io<N, BY, T, true, DIR>(g, mid, g, twN);
 }
 
@@ -475,9 +475,9 @@ __global__ void __launch_bounds__(T) k_fx(const float2* in, float2* out,
   extern __shared__ __align__(16) unsigned char smraw[];
   const SmemCol<TKV> mid{reinterpret_cast<cplx*>(smraw)};
   const size_t off = (size_t)blockIdx.y * N * N + blockIdx.x * TKV;
-  const Gmem go{out + off, 1, (size_t)N};
+  const cgfft::GmemC<1, N> go{out + off};
   if constexpr (SCALE == 0) {
-    const Gmem gi{const_cast<float2*>(in) + off, 1, (size_t)N};
+    const cgfft::GmemC<1, N> gi{const_cast<float2*>(in) + off};
     cgfft::fft_io<N, TKV, T, false, DIR, RMX>(gi, mid, go, twN);
   } else {
     const float fz = SCALE == 2 && gtab ? __ldg(gtab + blockIdx.y) : (float)blockIdx.y;
@@ -564,7 +564,7 @@ __global__ void __launch_bounds__(T) k_fx_sw(const __grid_constant__ CUtensorMap
     return;
   }
   const size_t off = (size_t)blockIdx.y * N * N + blockIdx.x * TKV;
-  const Gmem go{out + off, 1, (size_t)N};
+  const cgfft::GmemC<1, N> go{out + off};
   if constexpr (SCALE == 0) {
     cgfft::fft_io<N, TKV, T, false, DIR, RMX>(t, t, go, twN);
   } else {
@@ -678,15 +678,15 @@ __global__ void __launch_bounds__(T, MINB) k_green(const float2* __restrict__ sp
   const int kz = (int)(l0 / N);
   const int kx0 = (int)(l0 % N);
   const size_t off = l0 * N;
-  const Gmem gin{const_cast<float2*>(spec) + off, (size_t)N, 1};
+  const cgfft::GmemC<N, 1> gin{const_cast<float2*>(spec) + off};
   const SmemLine<P> d{D}, w{W};
   fft_tile_y<N, BG, RMG, -1>(gin, d, d, twN);
   // the y component's load also leaves the shared x/z value in D
   const GreenLoad<P, 2, MODS> gy{D, kz, kx0, N, f1, gm};
-  const Gmem oy{g1 + off, (size_t)N, 1};
+  const cgfft::GmemC<N, 1> oy{g1 + off};
   fft_tile_y<N, BG, RMG, 1>(gy, w, oy, twN);
   __syncthreads();
-  const Gmem os{g2 + off, (size_t)N, 1};
+  const cgfft::GmemC<N, 1> os{g2 + off};
   fft_tile_y<N, BG, RMG, 1>(d, d, os, twN);
 }
 
@@ -738,7 +738,7 @@ __global__ void __launch_bounds__(T) k_zi(const float2* __restrict__ gsp,
     }
   }
   __syncthreads();
-  const Gmem gout{reinterpret_cast<float2*>(out) + ((size_t)x * N + y0) * H, (size_t)H, 1};
+  const cgfft::GmemC<H, 1> gout{reinterpret_cast<float2*>(out) + ((size_t)x * N + y0) * H};
   cgfft::fft_io<H, TY, T, true, 1>(mid, mid, gout, twH);
 }
 
@@ -830,7 +830,7 @@ __global__ void __launch_bounds__(T, 2) k_zi_tma(const __grid_constant__ CUtenso
     }
   }
   __syncthreads();
-  const Gmem gout{reinterpret_cast<float2*>(out) + ((size_t)x * N + y0) * H, (size_t)H, 1};
+  const cgfft::GmemC<H, 1> gout{reinterpret_cast<float2*>(out) + ((size_t)x * N + y0) * H};
   cgfft::fft_io<H, TY, T, true, 1>(mid, mid, gout, twH);
 }
 
@@ -922,7 +922,7 @@ __global__ void __launch_bounds__(T, N >= 1024 ? 3 : 4) k_zi_sw(const __grid_con
     }
   }
   __syncthreads();
-  const Gmem gout{reinterpret_cast<float2*>(out) + ((size_t)x * N + y0) * H, (size_t)H, 1};
+  const cgfft::GmemC<H, 1> gout{reinterpret_cast<float2*>(out) + ((size_t)x * N + y0) * H};
   cgfft::fft_io<H, TY, T, false, 1, 16, true>(t, t, gout, twH);
 }
 
@@ -1159,10 +1159,26 @@ cudaError_t set_all_smem(int N) {
   return e;
 }
 
+// The twiddle table of length L (W_L^k rounded once from double) and the
+// per-stage rows after it (cgfft::stage_tw_offset), which copy its entries.
+size_t twiddle_table_len(int L) { return (size_t)cgfft::twiddle_table_len(L); }
+
 void twiddle_table(float2* h, int L) {
   for (int k = 0; k < L; k++) {
     const double a = -2.0 * 3.14159265358979323846264338327950288 * (double)k / (double)L;
     h[k] = make_float2((float)cos(a), (float)sin(a));
+  }
+  for (int pass = 0; pass < 2; pass++) {
+    const int rm = pass == 0 ? 16 : 8;
+    if (!cgfft::supported_length(L, rm)) continue;
+    for (int st = 1; st < cgfft::num_stages(L, rm); st++) {
+      const int ns = cgfft::ns_before(L, st, rm), r = cgfft::radix_at(L, st, rm);
+      const int off = cgfft::stage_tw_offset(L, ns, r);
+      const int rp = cgfft::stage_rp(r), step = L / (ns * r);
+      for (int jm = 0; jm < ns; jm++)
+        for (int i = 0; i < rp; i++)
+          h[off + jm * rp + i] = i + 1 < r ? h[jm * (i + 1) * step] : make_float2(0.0f, 0.0f);
+    }
   }
 }
 
@@ -1358,17 +1374,18 @@ cudaError_t pm_plan_alloc(PmPlan* p, int N, int factor, float L) {
     CG_TRY(cudaMalloc(&p->gsp[a], p->spec_bytes));
     CG_TRY(cudaMalloc(&p->fmesh[a], p->mesh_bytes));
   }
-  CG_TRY(cudaMalloc(&p->twN, sizeof(float2) * N));
-  CG_TRY(cudaMalloc(&p->twH, sizeof(float2) * (N / 2)));
+  const size_t lenN = twiddle_table_len(N), lenH = twiddle_table_len(N / 2);
+  CG_TRY(cudaMalloc(&p->twN, sizeof(float2) * lenN));
+  CG_TRY(cudaMalloc(&p->twH, sizeof(float2) * lenH));
   CG_TRY(cudaMalloc(&p->dsum, sizeof(double)));
   CG_TRY(cudaMalloc(&p->pk_acc, sizeof(double) * 3 * N));
   CG_TRY(cudaMalloc(&p->err, sizeof(unsigned)));
   {
-    float2* h = (float2*)malloc(sizeof(float2) * N);
+    float2* h = (float2*)malloc(sizeof(float2) * (lenN > lenH ? lenN : lenH));
     twiddle_table(h, N);
-    CG_TRY(cudaMemcpy(p->twN, h, sizeof(float2) * N, cudaMemcpyHostToDevice));
+    CG_TRY(cudaMemcpy(p->twN, h, sizeof(float2) * lenN, cudaMemcpyHostToDevice));
     twiddle_table(h, N / 2);
-    CG_TRY(cudaMemcpy(p->twH, h, sizeof(float2) * (N / 2), cudaMemcpyHostToDevice));
+    CG_TRY(cudaMemcpy(p->twH, h, sizeof(float2) * lenH, cudaMemcpyHostToDevice));
     free(h);
   }
   CG_TRY(cudaMemset(p->dsum, 0, sizeof(double)));
@@ -1399,15 +1416,16 @@ cudaError_t mesh_fft_alloc(MeshFFT* f, int N) {
   MeshKernels k;
   if (!get_kernels(N, &k)) return cudaErrorInvalidValue;
   f->N = N;
-  cudaError_t e = cudaMalloc(&f->twN, sizeof(float2) * N);
-  if (e == cudaSuccess) e = cudaMalloc(&f->twH, sizeof(float2) * (N / 2));
+  const size_t lenN = twiddle_table_len(N), lenH = twiddle_table_len(N / 2);
+  cudaError_t e = cudaMalloc(&f->twN, sizeof(float2) * lenN);
+  if (e == cudaSuccess) e = cudaMalloc(&f->twH, sizeof(float2) * lenH);
   if (e == cudaSuccess) e = cudaMalloc(&f->dsum, sizeof(double));
   if (e == cudaSuccess) {
-    float2* h = (float2*)malloc(sizeof(float2) * N);
+    float2* h = (float2*)malloc(sizeof(float2) * (lenN > lenH ? lenN : lenH));
     twiddle_table(h, N);
-    e = cudaMemcpy(f->twN, h, sizeof(float2) * N, cudaMemcpyHostToDevice);
+    e = cudaMemcpy(f->twN, h, sizeof(float2) * lenN, cudaMemcpyHostToDevice);
     twiddle_table(h, N / 2);
-    if (e == cudaSuccess) e = cudaMemcpy(f->twH, h, sizeof(float2) * (N / 2), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(f->twH, h, sizeof(float2) * lenH, cudaMemcpyHostToDevice);
     free(h);
   }
   if (e == cudaSuccess) e = set_all_smem(N);
