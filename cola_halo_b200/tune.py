@@ -72,15 +72,18 @@ def tune_deposit(sim, cache=None):
 
 
 def tune_sort_interval(sim, reset, sched, candidates=(0, 2, 3, 4, 6, 8, 10), reps=3,
-                       cache=None):
+                       cache=None, margin=0.01):
     """Run whole realizations per candidate sort interval and keep the
     fastest.  reset() puts the initial particles back; sched is the
     realization's Schedule.  Steps are move, force, fused kick + drift (the
     loop of main.c:162-206 without outputs).  Each candidate is timed as
     the best of `reps` realizations (the differences between intervals are
-    a few per cent, close to the spread of single runs).  Returns (interval,
-    ms per candidate); the fastest is installed on sim.  `cache` as for
-    tune_deposit (keyed by particle count and mesh size)."""
+    a few per cent, close to the spread of single runs).  The library's
+    default interval for this particle count (every sixth move from 2^23
+    particles, else never) is kept unless another candidate is faster by
+    more than `margin`.  Returns (interval, ms per candidate); the choice is
+    installed on sim.  `cache` as for tune_deposit (keyed by particle count
+    and mesh size)."""
     lib = sim.lib
     nsteps = sched.nloop - 1
     times = {}
@@ -108,7 +111,10 @@ def tune_sort_interval(sim, reset, sched, candidates=(0, 2, 3, 4, 6, 8, 10), rep
             t = _device_ms(lib, realization, 64 * nsteps)
             best = t if best is None else min(best, t)
         times[every] = best
+    default = 6 if sim.nc ** 3 >= (1 << 23) else 0
     best = min(times, key=times.get)
+    if default in times and times[best] > (1.0 - margin) * times[default]:
+        best = default
     sim.set_sort_interval(best)
     reset()
     _cache_put(cache, key, best)
