@@ -412,9 +412,15 @@ def run_b200(args, cfg):
 
     # ---- FFT schedule for this mesh size (untimed; cached across runs when
     # COLAGPU_TUNE_CACHE names a file)
-    _lib.check(lib.cg_autotune(N, 0, None, None), "cg_autotune")
+    ms_green = (ctypes.c_float * 8)(*([-1.0] * 8))
+    ms_fx = (ctypes.c_float * 8)(*([-1.0] * 8))
+    _lib.check(lib.cg_autotune(N, 0, ms_green, ms_fx), "cg_autotune")
     sg, sf = ctypes.c_int(), ctypes.c_int()
     _lib.check(lib.cg_get_schedule(N, ctypes.byref(sg), ctypes.byref(sf)), "cg_get_schedule")
+    ng_v, nf_v = ctypes.c_int(), ctypes.c_int()
+    lib.cg_schedule_variants(N, ctypes.byref(ng_v), ctypes.byref(nf_v))
+    tuned_ms = {"green": [round(ms_green[v], 4) for v in range(ng_v.value) if ms_green[v] >= 0],
+                "x": [round(ms_fx[v], 4) for v in range(nf_v.value) if ms_fx[v] >= 0]}
 
     # ---- device-resident step loop (value)
     sim = Simulation(nc, N, L, om)
@@ -583,7 +589,8 @@ def run_b200(args, cfg):
                        "parallelism": "replicas x%d (one realization per GPU)" % world,
                        "l2": "inputs larger than L2 (%.2f GB per mesh)" % (4.0 * N ** 3 / 1e9),
                        "fft_schedule": {"green_variant": sg.value, "x_variant": sf.value,
-                                        "chosen_by": "cg_autotune"},
+                                        "chosen_by": "cg_autotune",
+                                        "ms": tuned_ms},
                        "deposit_variant": {"chosen": dep_best,
                                            "ms": [round(t, 4) for t in dep_ms],
                                            "chosen_by": "cg_sim_tune_deposit"},

@@ -520,8 +520,9 @@ extern "C" int cg_sim_keep_density(cg_sim* s, int keep) {
 
 extern "C" int cg_sim_get_mesh(cg_sim* s, int which, float* out) {
   if (!s || !out || which < 0 || which > 3) return set_err(CG_EINVAL, "cg_sim_get_mesh: bad args");
-  if (which == 0 && s->pm.dens_reset) {
-    // the force step consumed the density: deposit the current positions again
+  if (which == 0 && (s->pm.dens_reset || s->pm.dens_stale)) {
+    // the force step consumed the density, or built it in shared memory
+    // only: deposit the current positions again
     const float* x[3] = {s->ps.x[0], s->ps.x[1], s->ps.x[2]};
     CG_CHECK(pm_deposit(&s->pm, x, s->ps.n, s->st), "deposit");
   }

@@ -70,6 +70,17 @@ struct PmPlan {
   CUtensorMap xtm[3];       // TMA maps of spec, gsp[1], gsp[2] for the x pass's gather
   bool xsw_ok;              //   valid (else the x pass loads directly)
   int xtm_tk;               //   the columns per CTA the maps were encoded for
+  bool dens_stale;          // dens does not hold the last force step's density (the
+                            //   column-binned deposit built it in shared memory only)
+  // Column bins of the force step's clouds (pm_colbins_reserve): per key
+  // (lower-corner column) a count, then its start; per particle the rank of
+  // its cloud and of its buffer copy; one 16-byte entry per cloud.
+  long long cb_cap;         //   particles the rank / entry arrays hold
+  long long cb_keys;        //   keys the count array holds (+1 for the total)
+  unsigned* cb_cnt;
+  unsigned* cb_bsum;        //   prefix-sum scratch
+  unsigned* cb_rank;        //   2 cb_cap
+  float4* cb_ent;           //   2 cb_cap
 };
 
 // Plain 3-D real transforms on the mesh layouts above (unnormalised, FFTW
@@ -131,8 +142,20 @@ cudaError_t pm_set_force_kernel(PmPlan* p, int gradient, int laplacian, int deco
 void pm_plan_free(PmPlan* p);
 // Full PM force: deposit -> r2c -> Green/gradient -> 3 c2r -> interpolation.
 // Positions and forces are SoA device arrays of n floats per component.
+// With the column-binned deposit selected (pm_set_force_deposit(1)) and a
+// plan that does not keep its density (keep_dens), the deposit and the r2c
+// along z run as k_dfz, which needs the plan's column bins for n particles
+// (allocated here on first use; pm_colbins_reserve beforehand for a stream
+// capture).
 cudaError_t pm_forces(PmPlan* p, const float* const x[3], long long n,
                       float* const f[3], cudaStream_t st);
+// Deposit of the force step for the plans' next pm_forces calls: 0 (the
+// default) the mesh deposit + k_fz, 1 column bins + k_dfz.  -1 on a bad mode.
+int pm_set_force_deposit(int mode);
+// The column-binned deposit is selected.
+bool pm_force_deposit_binned();
+// Column bins for up to n particles on the plan's mesh (no-op when held).
+cudaError_t pm_colbins_reserve(PmPlan* p, long long n);
 // Individual stages (exposed for tests and timing).
 cudaError_t pm_deposit(PmPlan* p, const float* const x[3], long long n, cudaStream_t st);
 // Time every deposit variant on these positions (best of 3, each after a

@@ -336,6 +336,18 @@ int cg_set_schedule(int ngrid, int green_variant, int fx_variant);
  * into the transform's own swizzled tile, -1 (the default) by mesh size.
  * The three give bit-identical forces; COLAGPU_ZI=0/1/2 overrides. */
 int cg_set_z_gather(int mode);
+/* Deposit of the force step (PtoMesh + the r2c along z, pm.c:229-301), for
+ * every handle from the next force step on: 0 (the default, also -1)
+ * deposits into the mesh and then transforms it; 1 bins the particles'
+ * clouds by mesh column with warp-aggregated atomics, and each CTA of the z
+ * transform builds its own density lines in shared memory from its
+ * columns' clouds, so the density mesh never goes through HBM.  The two
+ * agree to float rounding (only the order of the deposit's float additions
+ * differs); 1 adds them in an order that changes from run to run, so its
+ * forces are not bit-reproducible.  A handle that keeps its density
+ * (cg_sim_keep_density) always takes 0.  COLAGPU_FUSED_DEPOSIT=0/1
+ * overrides. */
+int cg_set_force_deposit(int mode);
 /* Shape of the CIC deposit per mesh size (no reference counterpart; the
  * reference's PtoMesh is pm.c:209-279): variant v of cg_deposit_variants()
  * sets the particles per CTA and the shared-memory box (512 / 3,072 cells,
