@@ -91,6 +91,7 @@ SIGNATURES = {
     "cg_set_z_gather": (i32, [i32]),
     "cg_set_x_gather": (i32, [i32]),
     "cg_set_force_deposit": (i32, [i32]),
+    "cg_set_force_interp": (i32, [i32]),
     "cg_deposit_variants": (i32, []),
     "cg_get_deposit_variant": (i32, [i32]),
     "cg_set_deposit_variant": (i32, [i32, i32]),

@@ -143,6 +143,12 @@ extern "C" int cg_set_force_deposit(int mode) {
   return CG_OK;
 }
 
+extern "C" int cg_set_force_interp(int mode) {
+  if (pm_set_force_interp(mode) != 0)
+    return cg_set_error_from_lpt(CG_EINVAL, "cg_set_force_interp: mode must be -1, 0 or 1");
+  return CG_OK;
+}
+
 extern "C" int cg_set_x_gather(int mode) {
   if (pm_set_x_gather(mode) != 0)
     return cg_set_error_from_lpt(CG_EINVAL, "cg_set_x_gather: mode must be -1, 0 or 1");

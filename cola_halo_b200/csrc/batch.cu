@@ -334,10 +334,11 @@ extern "C" int cg_batch_run(cg_batch* b) {
       if (b->sort_every > 0 && (e = particle_order_reserve(&r.order, r.ps.cap)) != cudaSuccess)
         return fail(e == cudaErrorMemoryAllocation ? CG_ENOMEM : CG_ECUDA,
                     "cg_batch_run: sort scratch", e);
-    // the column bins of the force step's deposit, per stream for its
-    // largest realization (the views of the stream's plan share them)
+    // the column bins of the force step's deposit and interpolation, per
+    // stream for its largest realization (the views of the stream's plan
+    // share them)
     for (auto& r : b->reals)
-      if (pm_force_deposit_binned() &&
+      if ((pm_force_deposit_binned() || pm_force_interp_binned()) &&
           (e = pm_colbins_reserve(&b->streams[r.stream].plan, r.ps.cap)) != cudaSuccess)
         return fail(e == cudaErrorMemoryAllocation ? CG_ENOMEM : CG_ECUDA,
                     "cg_batch_run: column bins", e);

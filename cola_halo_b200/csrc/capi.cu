@@ -526,6 +526,10 @@ extern "C" int cg_sim_get_mesh(cg_sim* s, int which, float* out) {
     const float* x[3] = {s->ps.x[0], s->ps.x[1], s->ps.x[2]};
     CG_CHECK(pm_deposit(&s->pm, x, s->ps.n, s->st), "deposit");
   }
+  if (which > 0) {
+    // the interpolation from the z c2r's tiles wrote no force mesh
+    CG_CHECK(pm_force_mesh(&s->pm, which - 1, s->st), "force mesh");
+  }
   const float* src = which == 0 ? s->pm.dens : s->pm.fmesh[which - 1];
   CG_CHECK(cudaMemcpyAsync(out, src, s->pm.mesh_bytes, cudaMemcpyDeviceToHost, s->st), "get mesh");
   CG_CHECK(cudaStreamSynchronize(s->st), "sync");

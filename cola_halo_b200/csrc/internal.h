@@ -81,6 +81,10 @@ struct PmPlan {
   unsigned* cb_bsum;        //   prefix-sum scratch
   unsigned* cb_rank;        //   2 cb_cap
   float4* cb_ent;           //   2 cb_cap
+  float* cb_part;           //   interpolation partials: 6 x 2 cb_cap (slots i0 / i1 of
+                            //   the x, y, z components)
+  bool fmesh_stale;         // fmesh does not hold the last force step's force meshes (the
+                            //   interpolation read them from shared memory only)
 };
 
 // Plain 3-D real transforms on the mesh layouts above (unnormalised, FFTW
@@ -154,6 +158,16 @@ cudaError_t pm_forces(PmPlan* p, const float* const x[3], long long n,
 int pm_set_force_deposit(int mode);
 // The column-binned deposit is selected.
 bool pm_force_deposit_binned();
+// Interpolation of the force step for the plans' next pm_forces calls: 0
+// (the default) from the force meshes (k_zi + k_interp), 1 from the z c2r's
+// shared tiles through the column bins (k_zi_interp).  The forces are the
+// same bit for bit.  -1 on a bad mode.
+int pm_set_force_interp(int mode);
+// The interpolation from the column bins is selected.
+bool pm_force_interp_binned();
+// The force mesh of component a (0..2) of the last force step in fmesh[a]
+// (a z c2r of its spectrum when the interpolation did not write it).
+cudaError_t pm_force_mesh(PmPlan* p, int a, cudaStream_t st);
 // Column bins for up to n particles on the plan's mesh (no-op when held).
 cudaError_t pm_colbins_reserve(PmPlan* p, long long n);
 // Individual stages (exposed for tests and timing).

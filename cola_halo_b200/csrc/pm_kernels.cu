@@ -376,9 +376,13 @@ __host__ __device__ constexpr int n_green_variants(int N) {
   return N >= MIN_TUNED_N && N <= 768 ? PM_NUM_GREEN_VARIANTS : 1;
 }
 struct FxCfg { int tk, rm; };
-struct GreenCfg { int byg, rm, minb; };
+struct GreenCfg { int byg, rm, minb, thr; };
 constexpr FxCfg kFxCfg[PM_NUM_FX_VARIANTS] = {{8, 0}, {8, -1}, {16, 16}};
-constexpr GreenCfg kGreenCfg[PM_NUM_GREEN_VARIANTS] = {{4, 16, 3}, {8, 8, 2}, {8, 16, 2}, {4, 16, 4}};
+// (lines per CTA, maximum radix, CTAs per SM, threads): at 768 a radix-16
+// stage has 48 butterflies per line, so 8 lines fill 384 threads and 4
+// lines 192 once each.
+constexpr GreenCfg kGreenCfg[PM_NUM_GREEN_VARIANTS] = {
+    {4, 16, 3, 256}, {8, 8, 2, 256}, {8, 16, 2, 384}, {4, 16, 4, 192}};
 __host__ __device__ constexpr int rm_x_default(int N) { return N >= 768 ? 8 : 16; }
 __host__ __device__ constexpr int fx_rm(int N, int v) {
   return kFxCfg[v].rm == 0 ? rm_x_default(N)
@@ -487,7 +491,9 @@ __global__ void __launch_bounds__(T) k_col_count(const float* __restrict__ x0,
                                                  int N, float scale, float x_right, float shiftx,
                                                  unsigned* __restrict__ cnt,
                                                  unsigned* __restrict__ rank, long long cap,
-                                                 unsigned* __restrict__ err) {
+                                                 unsigned* __restrict__ err,
+                                                 float* __restrict__ f0, float* __restrict__ f1,
+                                                 float* __restrict__ f2) {
   const int lane = threadIdx.x & 31;
   const long long stride = (long long)gridDim.x * T;
   // warp-uniform trip count: every lane takes part in the warp's match
@@ -508,9 +514,19 @@ __global__ void __launch_bounds__(T) k_col_count(const float* __restrict__ x0,
     }
     const unsigned r0 = warp_rank(cnt, k0, lane);
     if (k0 != COL_NONE) rank[i] = r0;
+    // the interpolation from the bins writes the forces of the primary
+    // clouds only; a particle without one (its cell index not finite or x
+    // rounded to L) has the force 0 of interp_one, plus its buffer copy's
+    if (f0 && k0 == COL_NONE && i < n) f0[i] = f1[i] = f2[i] = 0.0f;
     if (__any_sync(0xffffffffu, k1 != COL_NONE)) {
       const unsigned r1 = warp_rank(cnt, k1, lane);
-      if (k1 != COL_NONE) rank[cap + i] = r1;
+      if (k1 != COL_NONE) {
+        rank[cap + i] = r1;
+        // a copy outside key row 0 (x = L exactly after the wrap, or a
+        // position never wrapped): counted past the keys, so that the
+        // interpolation's copy pass looks at every entry
+        if (k1 >= (unsigned)N) atomicAdd(cnt + (size_t)(N + 1) * N + 1, 1u);
+      }
     }
   }
 }
@@ -874,10 +890,10 @@ struct GreenLoad {
 // The three transforms of the fused pass as separate (not inlined) calls:
 // each keeps its own register live range, so the kernel fits MINB CTAs per
 // SM without spilling.
-template <int N, int BG, int RMG, int DIR, class First, class Mid, class Last>
+template <int N, int BG, int RMG, int TG, int DIR, class First, class Mid, class Last>
 __device__ __noinline__ void fft_tile_y(const First f, const Mid m, const Last l,
                                         const float2* __restrict__ tw) {
-  cgfft::fft_io<N, BG, T, true, DIR, RMG>(f, m, l, tw);
+  cgfft::fft_io<N, BG, TG, true, DIR, RMG>(f, m, l, tw);
 }
 
 // GREEN: forward c2c along ky, Green/gradient, inverse c2c along ky:
@@ -886,9 +902,9 @@ __device__ __noinline__ void fft_tile_y(const First f, const Mid m, const Last l
 // their factor n_x / n_z, which is constant along a y line and is applied
 // by the inverse x pass as it loads g2 (k_fx, SCALE 1 and 2): one inverse
 // transform serves both components.  BG lines (kz, kx0 .. kx0+BG-1) per
-// CTA; N is a multiple of BG so the lines of a CTA share kz.
-template <int N, int BG, int RMG, int MINB, bool MODS>
-__global__ void __launch_bounds__(T, MINB) k_green(const float2* __restrict__ spec,
+// CTA of TG threads; N is a multiple of BG so the lines of a CTA share kz.
+template <int N, int BG, int RMG, int MINB, int TG, bool MODS>
+__global__ void __launch_bounds__(TG, MINB) k_green(const float2* __restrict__ spec,
                                                          float2* __restrict__ g1,
                                                          float2* __restrict__ g2,
                                                          const float2* __restrict__ twN,
@@ -903,14 +919,14 @@ __global__ void __launch_bounds__(T, MINB) k_green(const float2* __restrict__ sp
   const size_t off = l0 * N;
   const cgfft::GmemC<N, 1> gin{const_cast<float2*>(spec) + off};
   const SmemLine<P> d{D}, w{W};
-  fft_tile_y<N, BG, RMG, -1>(gin, d, d, twN);
+  fft_tile_y<N, BG, RMG, TG, -1>(gin, d, d, twN);
   // the y component's load also leaves the shared x/z value in D
   const GreenLoad<P, 2, MODS> gy{D, kz, kx0, N, f1, gm};
   const cgfft::GmemC<N, 1> oy{g1 + off};
-  fft_tile_y<N, BG, RMG, 1>(gy, w, oy, twN);
+  fft_tile_y<N, BG, RMG, TG, 1>(gy, w, oy, twN);
   __syncthreads();
   const cgfft::GmemC<N, 1> os{g2 + off};
-  fft_tile_y<N, BG, RMG, 1>(d, d, os, twN);
+  fft_tile_y<N, BG, RMG, TG, 1>(d, d, os, twN);
 }
 
 // ZI: c2r along z of S (lines (x, y0..y0+TY-1) per CTA) into R.  The
@@ -1077,6 +1093,73 @@ template <int N> __host__ __device__ constexpr size_t zsw_smem() {
   return (size_t)128 * zsw_nbox<N>() * zsw_krows<N>() + 1024 + 16;   // + alignment, mbarrier
 }
 
+// The swizzled tile's gather: thread 0 issues the NB tensor loads of the
+// (N/2+1) kz rows of the lines (x, y0 .. y0+15) of the spectrum behind `tm`
+// (mbarrier `bar`, already initialised, phase `parity`); every thread then
+// waits, bounded.  False (for every thread) when the loads did not complete.
+struct NoWork {
+  __device__ __forceinline__ void operator()() const {}
+};
+
+// `during` runs on every thread after the loads are issued, before the wait.
+template <int N, class F = NoWork>
+__device__ __forceinline__ bool zsw_gather(const CUtensorMap& tm, unsigned char* base,
+                                           unsigned bar, unsigned parity, int x, int y0,
+                                           F during = F()) {
+  constexpr int KR = zsw_krows<N>(), NB = zsw_nbox<N>();
+  constexpr unsigned kBytes = 128u * NB * KR;
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar),
+                 "r"(kBytes) : "memory");
+    const unsigned dst0 = (unsigned)__cvta_generic_to_shared(base);
+#pragma unroll
+    for (int h = 0; h < NB; h++) {
+      asm volatile(
+          "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
+          " [%0], [%1, {%2, %3, %4}], [%5];\n" ::"r"(dst0 + 128u * KR * h),
+          "l"(reinterpret_cast<unsigned long long>(&tm)), "r"(2 * y0), "r"(x), "r"(h * KR),
+          "r"(bar)
+          : "memory");
+    }
+  }
+  during();
+  unsigned done = 0;
+  for (int it = 0; it < (1 << 22) && !done; it++) {
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done) : "r"(bar), "r"(parity) : "memory");
+  }
+  return !__syncthreads_or(!done);
+}
+
+// Half-complex combination of k_zi (rows k and H - k of every line), in
+// place on the swizzled tile.
+template <int N>
+__device__ __forceinline__ void zsw_halfcomplex(const cgfft::SmemSw16& t,
+                                                const float2* __restrict__ twN) {
+  constexpr int H = N / 2;
+  for (int idx = threadIdx.x; idx < (H / 2 + 1) * TY; idx += T) {
+    const int b = idx % TY, k = idx / TY;
+    if (k == 0) {
+      const float x0 = t.ld(b, 0).x, xh = t.ld(b, H).x;
+      t.st(b, 0, cplx{x0 + xh, x0 - xh});
+    } else {
+      const int k2 = H - k;
+      const cplx a = t.ld(b, k), c = t.ld(b, k2);
+      const float2 wa = __ldg(twN + k), wc = __ldg(twN + k2);
+      const cplx sa = {a.x + c.x, a.y - c.y}, da = {a.x - c.x, a.y + c.y};
+      const cplx ra = {da.x * wa.x + da.y * wa.y, da.y * wa.x - da.x * wa.y};
+      const cplx za = {sa.x - ra.y, sa.y + ra.x};
+      const cplx sc = {c.x + a.x, c.y - a.y}, dc = {c.x - a.x, c.y + a.y};
+      const cplx rc = {dc.x * wc.x + dc.y * wc.y, dc.y * wc.x - dc.x * wc.y};
+      const cplx zc = {sc.x - rc.y, sc.y + rc.x};
+      t.st(b, k, za);
+      if (k2 != k) t.st(b, k2, zc);
+    }
+  }
+}
+
 template <int N>
 __global__ void __launch_bounds__(T, N >= 1024 ? 3 : 4) k_zi_sw(const __grid_constant__ CUtensorMap tm,
                                              float* __restrict__ out,
@@ -1099,54 +1182,169 @@ __global__ void __launch_bounds__(T, N >= 1024 ? 3 : 4) k_zi_sw(const __grid_con
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
   __syncthreads();
-  if (threadIdx.x == 0) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar),
-                 "r"(kBytes) : "memory");
-    const unsigned dst0 = (unsigned)__cvta_generic_to_shared(base);
-#pragma unroll
-    for (int h = 0; h < NB; h++) {
-      asm volatile(
-          "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
-          " [%0], [%1, {%2, %3, %4}], [%5];\n" ::"r"(dst0 + 128u * KR * h),
-          "l"(reinterpret_cast<unsigned long long>(&tm)), "r"(2 * y0), "r"(x), "r"(h * KR),
-          "r"(bar)
-          : "memory");
-    }
-  }
-  unsigned done = 0;
-  for (int it = 0; it < (1 << 22) && !done; it++) {
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n"
-        " selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(done) : "r"(bar) : "memory");
-  }
-  if (!done) {
+  if (!zsw_gather<N>(tm, base, bar, 0, x, y0)) {
     if (threadIdx.x == 0) atomicOr(err, (unsigned)CG_ERR_TMA_WAIT);
     return;
   }
-  // half-complex combination, rows k and H - k of every line, in place
-  for (int idx = threadIdx.x; idx < (H / 2 + 1) * TY; idx += T) {
-    const int b = idx % TY, k = idx / TY;
-    if (k == 0) {
-      const float x0 = t.ld(b, 0).x, xh = t.ld(b, H).x;
-      t.st(b, 0, cplx{x0 + xh, x0 - xh});
-    } else {
-      const int k2 = H - k;
-      const cplx a = t.ld(b, k), c = t.ld(b, k2);
-      const float2 wa = __ldg(twN + k), wc = __ldg(twN + k2);
-      const cplx sa = {a.x + c.x, a.y - c.y}, da = {a.x - c.x, a.y + c.y};
-      const cplx ra = {da.x * wa.x + da.y * wa.y, da.y * wa.x - da.x * wa.y};
-      const cplx za = {sa.x - ra.y, sa.y + ra.x};
-      const cplx sc = {c.x + a.x, c.y - a.y}, dc = {c.x - a.x, c.y + a.y};
-      const cplx rc = {dc.x * wc.x + dc.y * wc.y, dc.y * wc.x - dc.x * wc.y};
-      const cplx zc = {sc.x - rc.y, sc.y + rc.x};
-      t.st(b, k, za);
-      if (k2 != k) t.st(b, k2, zc);
-    }
-  }
+  zsw_halfcomplex<N>(t, twN);
   __syncthreads();
   const cgfft::GmemC<H, 1> gout{reinterpret_cast<float2*>(out) + ((size_t)x * N + y0) * H};
   cgfft::fft_io<H, TY, T, false, 1, 16, true>(t, t, gout, twH);
+}
+
+// ------------------------------------------ z c2r fused with interpolation
+// ZIP: the z c2r of one force component with the CIC interpolation of its
+// plane (force_at_particle_locations, pm.c:370-411) done from the
+// transformed lines in shared memory, so the force mesh is never written to
+// or read from HBM.  A CTA computes the 16 lines (x, y0 .. y0+15), y0 = 14 t
+// (tiles overlap by two lines: a cloud with lower corner column j0 needs
+// lines j0 and j0 + 1), and interpolates the clouds of the column bins
+// (k_col_count) with i0 = x (plane x is the cloud's i0) or i0 = x - 1 (its
+// i1) and j0 in y0 .. y0+13.  Tiles that reach past line N - 1 hold the
+// lines (y0 + b) mod N, gathered by plain loads (line 0 follows line N - 1);
+// the others take k_zi_sw's tensor loads (y0 = 14 t keeps the box's x
+// coordinate 2 y0 floats on a 16-byte boundary).  Each cloud's gather4
+// partial goes to its slot: p0[e] (plane i0) or p1[e] (plane i1).  The
+// lines are bit for bit k_zi's, and the partials are gather4 of
+// interp_one, so k_interp_sum reproduces k_interp's forces exactly.
+constexpr int ZIP_S = 14;
+__host__ __device__ constexpr int zip_tiles(int N) { return (N + ZIP_S - 1) / ZIP_S; }
+
+__device__ __forceinline__ float zsw_real(const cgfft::SmemSw16& t, int b, int k) {
+  const cplx z = t.ld(b, k >> 1);
+  return (k & 1) ? z.y : z.x;
+}
+
+template <int N>
+__global__ void __launch_bounds__(T, N >= 1024 ? 3 : 4) k_zi_interp(
+    const __grid_constant__ CUtensorMap tm, const float2* __restrict__ gsp,
+    const float4* __restrict__ ent, const unsigned* __restrict__ start,
+    float* __restrict__ p0, float* __restrict__ p1, const float2* __restrict__ twH,
+    const float2* __restrict__ twN, float scale, unsigned* __restrict__ err) {
+  static_assert(TY == 16, "the swizzled tile holds 16 lines per 128-byte row");
+  constexpr int H = N / 2;
+  constexpr int KR = zsw_krows<N>(), NB = zsw_nbox<N>();
+  constexpr unsigned kBytes = 128u * NB * KR;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  __shared__ unsigned beg[2], pre[3];
+  unsigned char* base =
+      smraw + ((1024u - ((unsigned)__cvta_generic_to_shared(smraw) & 1023u)) & 1023u);
+  const cgfft::SmemSw16 t{reinterpret_cast<cplx*>(base)};
+  const unsigned bar = (unsigned)__cvta_generic_to_shared(base + kBytes);
+  const int x = blockIdx.y;
+  const int y0 = blockIdx.x * ZIP_S;
+  const bool wrap = y0 + TY > N;
+  if (!wrap) {
+    if (threadIdx.x == 0) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(bar) : "memory");
+      asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    __syncthreads();
+  }
+  // the tensor loads go out first; the entry ranges are read while they land
+  // (key rows x (i0 = x - 1) and x + 1 (i0 = x), columns y0 .. min(y0+14, N) - 1)
+  const auto ranges = [&] {
+    if (threadIdx.x == 0) {
+      const unsigned c0 = (unsigned)y0, c1 = (unsigned)min(y0 + ZIP_S, N);
+      const unsigned k0 = (unsigned)x * N, k1 = k0 + N;
+      const unsigned s00 = start[k0 + c0], s01 = start[k0 + c1];
+      const unsigned s10 = start[k1 + c0], s11 = start[k1 + c1];
+      beg[0] = s00;
+      beg[1] = s10;
+      pre[0] = 0;
+      pre[1] = s01 - s00;
+      pre[2] = pre[1] + (s11 - s10);
+    }
+  };
+  if (!wrap) {
+    if (!zsw_gather<N>(tm, base, bar, 0, x, y0, ranges)) {
+      if (threadIdx.x == 0) atomicOr(err, (unsigned)CG_ERR_TMA_WAIT);
+      return;
+    }
+  } else {
+    ranges();
+    for (int idx = threadIdx.x; idx < (H + 1) * TY; idx += T) {
+      const int b = idx % TY, k = idx / TY;
+      const int y = y0 + b < N ? y0 + b : y0 + b - N;
+      const float2 v = __ldg(gsp + ((size_t)k * N + x) * N + y);
+      t.st(b, k, cplx{v.x, v.y});
+    }
+    __syncthreads();
+  }
+  zsw_halfcomplex<N>(t, twN);
+  __syncthreads();
+  cgfft::fft_io<H, TY, T, false, 1>(t, t, t, twH);
+  const unsigned total = pre[2];
+  for (unsigned e = threadIdx.x; e < total; e += T) {
+    const int q = e < pre[1] ? 0 : 1;
+    const unsigned ei = beg[q] + (e - pre[q]);
+    const float4 w = __ldg(ent + ei);
+    const Cic c = cic_index(w.x, w.y, w.z, N, scale);
+    const bool at_i0 = c.i0 == x;
+    const float wi = at_i0 ? c.t1 : c.d1;
+    const int b0 = c.j0 - y0;            // line j1 = j0 + 1 (mod N) sits at b0 + 1
+    // gather4: ((m*T3)*Ti)*T2 + ((m*D3)*Ti)*T2 + ((m*T3)*Ti)*D2 + ((m*D3)*Ti)*D2
+    const float a = __fmul_rn(__fmul_rn(__fmul_rn(zsw_real(t, b0, c.k0), c.t3), wi), c.t2);
+    const float b = __fmul_rn(__fmul_rn(__fmul_rn(zsw_real(t, b0, c.k1), c.d3), wi), c.t2);
+    const float d = __fmul_rn(__fmul_rn(__fmul_rn(zsw_real(t, b0 + 1, c.k0), c.t3), wi), c.d2);
+    const float g = __fmul_rn(__fmul_rn(__fmul_rn(zsw_real(t, b0 + 1, c.k1), c.d3), wi), c.d2);
+    (at_i0 ? p0 : p1)[ei] = __fadd_rn(__fadd_rn(__fadd_rn(a, b), d), g);
+  }
+}
+
+// The forces of the primary clouds, in interp_one's order:
+// f = (0 + gather4(i0)) + gather4(i1), each term for a plane inside the mesh.
+// part holds the slots p0, p1 of the x, y and z components, stride cap2.
+__global__ void __launch_bounds__(T) k_interp_sum(const float4* __restrict__ ent,
+                                                  const unsigned* __restrict__ start, int N,
+                                                  float scale, const float* __restrict__ part,
+                                                  long long cap2, float* __restrict__ f0,
+                                                  float* __restrict__ f1, float* __restrict__ f2) {
+  const unsigned hi = start[(size_t)(N + 1) * N];
+  float* const f[3] = {f0, f1, f2};
+  for (unsigned e = blockIdx.x * T + threadIdx.x; e < hi; e += gridDim.x * T) {
+    const float4 w = __ldg(ent + e);
+    const unsigned i = __float_as_uint(w.w);
+    if (i & COL_COPY) continue;
+    const Cic c = cic_index(w.x, w.y, w.z, N, scale);
+    const bool in0 = 0 <= c.i0 && c.i0 < N, in1 = 0 <= c.i1 && c.i1 < N;
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      float s = 0.0f;
+      if (in0) s = __fadd_rn(s, __ldg(part + (2 * a) * cap2 + e));
+      if (in1) s = __fadd_rn(s, __ldg(part + (2 * a + 1) * cap2 + e));
+      f[a][i] = s;
+    }
+  }
+}
+
+// The buffer copies' forces added to their particles' (add_buffer_forces,
+// pm.c:526-531, of interp_one for the copy).  After the wrap every copy
+// sits in key row 0 (i0 = -1, i1 = 0), the entries before start[N]; when
+// k_col_count counted copies elsewhere, every entry is looked at.
+__global__ void __launch_bounds__(T) k_interp_copies(const float4* __restrict__ ent,
+                                                     const unsigned* __restrict__ start, int N,
+                                                     float scale, const float* __restrict__ part,
+                                                     long long cap2, float* __restrict__ f0,
+                                                     float* __restrict__ f1,
+                                                     float* __restrict__ f2) {
+  const size_t keys = (size_t)(N + 1) * N;
+  const unsigned hi = start[keys + 1] ? start[keys] : start[N];
+  float* const f[3] = {f0, f1, f2};
+  for (unsigned e = blockIdx.x * T + threadIdx.x; e < hi; e += gridDim.x * T) {
+    const float4 w = __ldg(ent + e);
+    const unsigned i = __float_as_uint(w.w);
+    if (!(i & COL_COPY)) continue;
+    const Cic c = cic_index(w.x, w.y, w.z, N, scale);
+    const bool in0 = 0 <= c.i0 && c.i0 < N, in1 = 0 <= c.i1 && c.i1 < N;
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      float s = 0.0f;
+      if (in0) s = __fadd_rn(s, __ldg(part + (2 * a) * cap2 + e));
+      if (in1) s = __fadd_rn(s, __ldg(part + (2 * a + 1) * cap2 + e));
+      f[a][i & ~COL_COPY] = __fadd_rn(f[a][i & ~COL_COPY], s);
+    }
+  }
 }
 
 // Gather of the z c2r by mesh size (the plans created afterwards):
@@ -1278,9 +1476,12 @@ struct MeshKernels {
   void (*zi)(const float2*, float*, const float2*, const float2*);
   void (*zi_tma)(CUtensorMap, float*, const float2*, const float2*, unsigned*);
   void (*zi_sw)(CUtensorMap, float*, const float2*, const float2*, unsigned*);
+  void (*zip)(CUtensorMap, const float2*, const float4*, const unsigned*, float*, float*,
+              const float2*, const float2*, float, unsigned*);
   size_t sm_fz, sm_fy, sm_fx, sm_green, sm_zi, sm_zi_tma, sm_zi_sw;
   int tk;    // ky columns per CTA of the x pass
   int byg;   // lines per CTA of the Green pass
+  int tg;    // threads per CTA of the Green pass
 };
 
 template <int N, int V>
@@ -1302,8 +1503,9 @@ void set_fx(MeshKernels* k) {
 template <int N, int V>
 void set_green(MeshKernels* k) {
   constexpr GreenCfg c = kGreenCfg[V];
-  k->green = k_green<N, c.byg, c.rm, c.minb, false>;
-  k->green_mods = k_green<N, c.byg, c.rm, c.minb, true>;
+  k->green = k_green<N, c.byg, c.rm, c.minb, c.thr, false>;
+  k->green_mods = k_green<N, c.byg, c.rm, c.minb, c.thr, true>;
+  k->tg = c.thr;
   k->sm_green = sizeof(cplx) * 2 * c.byg * cgfft::line_pitch<N>();
   k->byg = c.byg;
 }
@@ -1321,6 +1523,7 @@ MeshKernels make_kernels(MeshSched s) {
   k.sm_zi_tma = zi_tma_smem<N>();
   k.zi_sw = k_zi_sw<N>;
   k.sm_zi_sw = zsw_smem<N>();
+  k.zip = k_zi_interp<N>;
   k.sm_fz = sizeof(cplx) * TY * cgfft::line_pitch<N / 2>();
   k.sm_fy = sizeof(cplx) * BY * cgfft::line_pitch<N>();
   k.sm_zi = sizeof(cplx) * TY * cgfft::line_pitch<N / 2 + 1>();
@@ -1401,6 +1604,7 @@ cudaError_t set_all_smem(int N) {
     if (e == cudaSuccess) e = set_smem((const void*)k.zi, k.sm_zi);
     if (e == cudaSuccess) e = set_smem((const void*)k.zi_tma, k.sm_zi_tma);
     if (e == cudaSuccess) e = set_smem((const void*)k.zi_sw, k.sm_zi_sw);
+    if (e == cudaSuccess) e = set_smem((const void*)k.zip, k.sm_zi_sw);
   }
   return e;
 }
@@ -1444,6 +1648,30 @@ int pm_set_x_gather(int mode) {
 
 bool pm_force_deposit_binned() { return fused_deposit(); }
 
+// Interpolation of the force step: 0 from the force meshes (the default), 1
+// from the z c2r's shared tiles.  COLAGPU_FUSED_INTERP=0/1 overrides.  The
+// default stays the force meshes: at 768^3 the fused form measured 1.04 ms
+// per component (the tiles overlap by two lines, 14 % more transform work,
+// and the gathers from shared memory add issue slots) plus 0.35 ms of
+// binning and 0.42 ms of sums, against 0.81 ms per k_zi_sw and 1.05 ms for
+// k_interp: 10.76 against 10.50 ms per step.
+std::atomic<int> g_fint{-1};
+
+bool pm_force_interp_binned() {
+  static const int forced = [] {
+    const char* e = getenv("COLAGPU_FUSED_INTERP");
+    return e ? atoi(e) : -1;
+  }();
+  const int m = forced >= 0 ? forced : g_fint.load();
+  return m == 1;
+}
+
+int pm_set_force_interp(int mode) {
+  if (mode < -1 || mode > 1) return -1;
+  g_fint.store(mode);
+  return 0;
+}
+
 int pm_set_force_deposit(int mode) {
   if (mode < -1 || mode > 1) return -1;
   g_fdep.store(mode);
@@ -1459,7 +1687,7 @@ cudaError_t pm_colbins_reserve(PmPlan* p, long long n) {
     p->cb_cnt = nullptr;
     p->cb_bsum = nullptr;
     p->cb_keys = 0;
-    e = cudaMalloc(&p->cb_cnt, sizeof(unsigned) * keys);
+    e = cudaMalloc(&p->cb_cnt, sizeof(unsigned) * (keys + 1));
     if (e == cudaSuccess)
       e = cudaMalloc(&p->cb_bsum, sizeof(unsigned) * (cgscan::scratch_entries(keys) + 1));
     if (e != cudaSuccess) return e;
@@ -1471,8 +1699,11 @@ cudaError_t pm_colbins_reserve(PmPlan* p, long long n) {
     p->cb_rank = nullptr;
     p->cb_ent = nullptr;
     p->cb_cap = 0;
+    cudaFree(p->cb_part);
+    p->cb_part = nullptr;
     e = cudaMalloc(&p->cb_rank, sizeof(unsigned) * 2 * (size_t)n);
     if (e == cudaSuccess) e = cudaMalloc(&p->cb_ent, sizeof(float4) * 2 * (size_t)n);
+    if (e == cudaSuccess) e = cudaMalloc(&p->cb_part, sizeof(float) * 12 * (size_t)n);
     if (e != cudaSuccess) return e;
     p->cb_cap = n;
   }
@@ -1603,7 +1834,7 @@ cudaError_t pm_autotune(PmPlan* p, cudaStream_t st, MeshSched* best, float* ms_g
   e = interleaved_best(st, ng, kRounds, [&](int v) {
     const MeshKernels& k = kg[v];
     prof_mark(st, CG_ST_OTHER);
-    k.green<<<(N / 2 + 1) * N / k.byg, T, k.sm_green, st>>>(p->spec, p->gsp[1], p->gsp[2],
+    k.green<<<(N / 2 + 1) * N / k.byg, k.tg, k.sm_green, st>>>(p->spec, p->gsp[1], p->gsp[2],
                                                              p->twN, p->f1, GreenMods{});
   }, tg);
   // time the gather the plan uses (its TMA maps, kernel parameters, are
@@ -1842,6 +2073,7 @@ void pm_plan_free(PmPlan* p) {
   cudaFree(p->cb_bsum);
   cudaFree(p->cb_rank);
   cudaFree(p->cb_ent);
+  cudaFree(p->cb_part);
   memset(p, 0, sizeof(*p));
 }
 
@@ -1887,22 +2119,25 @@ cudaError_t pm_r2c(PmPlan* p, cudaStream_t st) {
   return cudaGetLastError();
 }
 
-// The force step's deposit and r2c through the column bins: counts with
-// warp-aggregated ranks, their prefix sum, the entries, then k_dfz (deposit
-// in shared memory + r2c along z) and the forward x pass.  The density mesh
-// is left untouched (dens_stale).
-cudaError_t pm_binned_r2c(PmPlan* p, const float* const x[3], long long n, cudaStream_t st) {
-  MeshKernels k;
-  get_kernels(p->N, &k);
+void launch_zi(const PmPlan* p, const MeshKernels& k, int a, cudaStream_t st);
+
+// The column bins of the particles' clouds for this force step: counts with
+// warp-aggregated ranks, their prefix sum, the entries.  With f, the
+// forces of particles without a primary cloud are set to 0 (the
+// interpolation from the bins writes the others).
+cudaError_t pm_build_bins(PmPlan* p, const float* const x[3], long long n, float* const* f,
+                          cudaStream_t st) {
   const int N = p->N;
   const long long keys = (long long)(N + 1) * N + 1;
   if (n > p->cb_cap || keys > p->cb_keys) return cudaErrorInvalidValue;
-  cudaMemsetAsync(p->cb_cnt, 0, sizeof(unsigned) * keys, st);
-  cudaMemsetAsync(p->dsum, 0, sizeof(double), st);
+  // the counts, and past them the count of buffer copies outside key row 0
+  cudaMemsetAsync(p->cb_cnt, 0, sizeof(unsigned) * (keys + 1), st);
   if (n > 0) {
     prof_mark(st, CG_ST_DEPOSIT);
     k_col_count<<<grid_for(n), T, 0, st>>>(x[0], x[1], x[2], n, N, p->scale, p->x_right,
-                                           p->shiftx, p->cb_cnt, p->cb_rank, p->cb_cap, p->err);
+                                           p->shiftx, p->cb_cnt, p->cb_rank, p->cb_cap, p->err,
+                                           f ? f[0] : nullptr, f ? f[1] : nullptr,
+                                           f ? f[2] : nullptr);
   }
   cgscan::exclusive(p->cb_cnt, p->cb_cnt, keys, p->cb_bsum, nullptr, CG_ST_DEPOSIT, st);
   if (n > 0) {
@@ -1911,13 +2146,58 @@ cudaError_t pm_binned_r2c(PmPlan* p, const float* const x[3], long long n, cudaS
                                              p->shiftx, p->cb_cnt, p->cb_rank, p->cb_cap,
                                              p->cb_ent);
   }
+  return cudaGetLastError();
+}
+
+// The force step's deposit and r2c through the column bins (built): k_dfz
+// (deposit in shared memory + r2c along z) and the forward x pass.  The
+// density mesh is left untouched (dens_stale).
+cudaError_t pm_binned_r2c(PmPlan* p, cudaStream_t st) {
+  MeshKernels k;
+  get_kernels(p->N, &k);
+  const int N = p->N;
+  cudaMemsetAsync(p->dsum, 0, sizeof(double), st);
   prof_mark(st, CG_ST_FZ);
-  // persistent: as many CTAs as fit on the device at once
   k.dfz<<<dim3(N / TY, N), T, k.sm_fz, st>>>(p->cb_ent, p->cb_cnt, p->spec, p->twH, p->twN,
                                              p->dsum, p->scale, p->wpar);
   p->dens_reset = false;
   p->dens_stale = true;
   launch_fx_fwd(p, k, st);
+  return cudaGetLastError();
+}
+
+// The z c2r of the three components fused with the interpolation (bins
+// built, spectra gsp[0..2] inverse-transformed along x), then the sums.
+cudaError_t pm_zi_interp(PmPlan* p, long long n, float* const f[3], cudaStream_t st) {
+  MeshKernels k;
+  get_kernels(p->N, &k);
+  const int N = p->N;
+  const long long cap2 = 2 * p->cb_cap;
+  for (int a = 0; a < 3; a++) {
+    prof_mark(st, CG_ST_ZI);
+    k.zip<<<dim3(zip_tiles(N), N), T, k.sm_zi_sw, st>>>(
+        p->ztm[a], p->gsp[a], p->cb_ent, p->cb_cnt, p->cb_part + 2 * a * cap2,
+        p->cb_part + (2 * a + 1) * cap2, p->twH, p->twN, p->scale, p->err);
+  }
+  if (n > 0) {
+    prof_mark(st, CG_ST_INTERP);
+    k_interp_sum<<<grid_for(n), T, 0, st>>>(p->cb_ent, p->cb_cnt, N, p->scale, p->cb_part, cap2,
+                                            f[0], f[1], f[2]);
+    prof_mark(st, CG_ST_INTERP);
+    k_interp_copies<<<cg_grid((long long)N * N, 4), T, 0, st>>>(p->cb_ent, p->cb_cnt, N,
+                                                                p->scale, p->cb_part, cap2,
+                                                                f[0], f[1], f[2]);
+  }
+  p->fmesh_stale = true;
+  return cudaGetLastError();
+}
+
+cudaError_t pm_force_mesh(PmPlan* p, int a, cudaStream_t st) {
+  if (!p->fmesh_stale) return cudaSuccess;
+  MeshKernels k;
+  get_kernels(p->N, &k);
+  prof_mark(st, CG_ST_ZI);
+  launch_zi(p, k, a, st);
   return cudaGetLastError();
 }
 
@@ -2011,7 +2291,9 @@ bool x_maps_for(PmPlan* p, int tk) {
   return true;
 }
 
-cudaError_t pm_green_c2r(PmPlan* p, cudaStream_t st) {
+// The Green pass and the inverse x passes; with zi, each component's z c2r
+// into its force mesh after its x pass.
+static cudaError_t green_x_zi(PmPlan* p, cudaStream_t st, bool zi) {
   MeshKernels k;
   get_kernels(p->N, &k);
   const int N = p->N;
@@ -2019,7 +2301,7 @@ cudaError_t pm_green_c2r(PmPlan* p, cudaStream_t st) {
   prof_mark(st, CG_ST_GREEN);
   const GreenMods gm{p->kfilt_cur >= 0 ? p->kfilt + (size_t)p->kfilt_cur * p->kfilt_n : nullptr,
                      p->kfilt_n, p->kfilt_inv_dn, p->ktab};
-  (gm.t || gm.tab ? k.green_mods : k.green)<<<(N / 2 + 1) * N / k.byg, T, k.sm_green, st>>>(
+  (gm.t || gm.tab ? k.green_mods : k.green)<<<(N / 2 + 1) * N / k.byg, k.tg, k.sm_green, st>>>(
       p->spec, p->gsp[1], p->gsp[2], p->twN, p->f1, gm);
   const dim3 gx(N / k.tk, N / 2 + 1);
   const bool xsw = x_maps_for(p, k.tk);
@@ -2029,25 +2311,36 @@ cudaError_t pm_green_c2r(PmPlan* p, cudaStream_t st) {
     k.fxi_x_sw<<<gx, T, k.sm_fx_sw, st>>>(p->xtm[2], p->gsp[0], p->twN, p->ktab, p->err);
   else
     k.fxi_x<<<gx, T, k.sm_fx, st>>>(p->gsp[2], p->gsp[0], p->twN, p->ktab);
-  prof_mark(st, CG_ST_ZI);
-  launch_zi(p, k, 0, st);
+  if (zi) {
+    prof_mark(st, CG_ST_ZI);
+    launch_zi(p, k, 0, st);
+  }
   // y: in place
   prof_mark(st, CG_ST_FX_INV);
   if (xsw)
     k.fxi_sw<<<gx, T, k.sm_fx_sw, st>>>(p->xtm[1], p->gsp[1], p->twN, nullptr, p->err);
   else
     k.fxi<<<gx, T, k.sm_fx, st>>>(p->gsp[1], p->gsp[1], p->twN, nullptr);
-  prof_mark(st, CG_ST_ZI);
-  launch_zi(p, k, 1, st);
+  if (zi) {
+    prof_mark(st, CG_ST_ZI);
+    launch_zi(p, k, 1, st);
+  }
   // z: n_z * gsp[2], in place
   prof_mark(st, CG_ST_FX_INV);
   if (xsw)
     k.fxi_z_sw<<<gx, T, k.sm_fx_sw, st>>>(p->xtm[2], p->gsp[2], p->twN, p->ktab, p->err);
   else
     k.fxi_z<<<gx, T, k.sm_fx, st>>>(p->gsp[2], p->gsp[2], p->twN, p->ktab);
-  prof_mark(st, CG_ST_ZI);
-  launch_zi(p, k, 2, st);
+  if (zi) {
+    prof_mark(st, CG_ST_ZI);
+    launch_zi(p, k, 2, st);
+  }
   return cudaGetLastError();
+}
+
+cudaError_t pm_green_c2r(PmPlan* p, cudaStream_t st) {
+  p->fmesh_stale = false;
+  return green_x_zi(p, st, true);
 }
 
 cudaError_t pm_interp(PmPlan* p, const float* const x[3], long long n, float* const f[3],
@@ -2064,12 +2357,23 @@ cudaError_t pm_interp(PmPlan* p, const float* const x[3], long long n, float* co
 cudaError_t pm_forces(PmPlan* p, const float* const x[3], long long n, float* const f[3],
                       cudaStream_t st) {
   cudaError_t e;
-  if (!p->keep_dens && fused_deposit()) {
+  // the column bins serve the binned deposit and the interpolation from the
+  // z c2r's tiles (which needs the swizzled tiles' tensor maps)
+  const bool bdep = !p->keep_dens && fused_deposit();
+  const bool bint = pm_force_interp_binned() && p->zsw_ok;
+  if (bdep || bint) {
     if ((e = pm_colbins_reserve(p, n)) != cudaSuccess) return e;
-    if ((e = pm_binned_r2c(p, x, n, st)) != cudaSuccess) return e;
+    if ((e = pm_build_bins(p, x, n, bint ? f : nullptr, st)) != cudaSuccess) return e;
+  }
+  if (bdep) {
+    if ((e = pm_binned_r2c(p, st)) != cudaSuccess) return e;
   } else {
     if ((e = pm_deposit(p, x, n, st)) != cudaSuccess) return e;
     if ((e = pm_r2c(p, st)) != cudaSuccess) return e;
+  }
+  if (bint) {
+    if ((e = green_x_zi(p, st, false)) != cudaSuccess) return e;
+    return pm_zi_interp(p, n, f, st);
   }
   if ((e = pm_green_c2r(p, st)) != cudaSuccess) return e;
   return pm_interp(p, x, n, f, st);

@@ -348,6 +348,16 @@ int cg_set_z_gather(int mode);
  * (cg_sim_keep_density) always takes 0.  COLAGPU_FUSED_DEPOSIT=0/1
  * overrides. */
 int cg_set_force_deposit(int mode);
+/* Interpolation of the force step (force_at_particle_locations ×3 + the
+ * buffer copies' forces, pm.c:359-412, 505-532), for every handle from the
+ * next force step on: 0 (the default, also -1) writes the force meshes and
+ * interpolates from them; 1 bins the particles' clouds by mesh column, and
+ * each CTA of the z c2r interpolates the clouds of its plane from the force
+ * lines it has just transformed in shared memory, so the three force
+ * meshes never go through HBM.  The forces are the same bit for bit.  After
+ * a step with 1, cg_sim_get_mesh(s, 1..3, ..) transforms the requested
+ * force mesh from its spectrum first.  COLAGPU_FUSED_INTERP=0/1 overrides. */
+int cg_set_force_interp(int mode);
 /* Shape of the CIC deposit per mesh size (no reference counterpart; the
  * reference's PtoMesh is pm.c:209-279): variant v of cg_deposit_variants()
  * sets the particles per CTA and the shared-memory box (512 / 3,072 cells,
