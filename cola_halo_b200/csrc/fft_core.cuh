@@ -200,7 +200,34 @@ __host__ __device__ constexpr int stage_tw_offset(int L, int NS, int R) {
   }
   return NS > 0 ? -1 : off;
 }
-__host__ __device__ constexpr int twiddle_table_len(int L) { return stage_tw_offset(L, 0, 0); }
+// The same stages' twiddles once more, transposed, after the row blocks:
+// R-1 runs of NS entries, run r-1 holding W_L^{jm r STEP} for jm = 0 ..
+// NS-1.  Along a line consecutive threads take consecutive jm, so a warp's
+// loads of one r fall on one contiguous run.  Offset of stage (NS, R)'s
+// block, or -1; with NS = 0 the table's total length.
+__host__ __device__ constexpr int stage_twt_offset(int L, int NS, int R) {
+  int off = stage_tw_offset(L, 0, 0);
+  for (int pass = 0; pass < 2; pass++) {
+    const int rm = pass == 0 ? 16 : 8;
+    if (!supported_length(L, rm)) continue;
+    for (int st = 1; st < num_stages(L, rm); st++) {
+      const int ns = ns_before(L, st, rm), r = radix_at(L, st, rm);
+      bool seen = false;
+      for (int p2 = 0; p2 <= pass && !seen; p2++) {
+        const int rm2 = p2 == 0 ? 16 : 8;
+        if (!supported_length(L, rm2)) continue;
+        const int last = p2 < pass ? num_stages(L, rm2) : st;
+        for (int s2 = 1; s2 < last; s2++)
+          if (ns_before(L, s2, rm2) == ns && radix_at(L, s2, rm2) == r) seen = true;
+      }
+      if (seen) continue;
+      if (NS > 0 && ns == NS && r == R) return off;
+      off += ns * (r - 1);
+    }
+  }
+  return NS > 0 ? -1 : off;
+}
+__host__ __device__ constexpr int twiddle_table_len(int L) { return stage_twt_offset(L, 0, 0); }
 
 // ------------------------------------------------------------ tile access
 // The first stage reads its legs j + r L/R and the last writes its outputs
@@ -362,11 +389,19 @@ __device__ __forceinline__ void stage_io(const In& in, const Out& out,
         // per-stage rows where consecutive threads share a row (the same
         // butterfly of consecutive lines): one broadcast 16-byte load per
         // pair of twiddles.  Along a line consecutive threads would read
-        // consecutive rows, R-1 entries apart, and the strided table
-        // reads of nearby entries take fewer sectors (768-point Green pass:
-        // 1.85 ms with table reads against 2.61 ms with rows).
+        // consecutive rows, R-1 entries apart (768-point Green pass: 2.61
+        // ms with rows against 1.85 ms with strided table reads); there they
+        // read the transposed runs instead.
         constexpr int OFF = LINE_MAJOR ? -1 : stage_tw_offset(L, NS, R);
-        if constexpr (OFF >= 0) {
+        constexpr int OFFT = LINE_MAJOR ? stage_twt_offset(L, NS, R) : -1;
+        if constexpr (OFFT >= 0) {
+          // along a line: the transposed runs, one contiguous run per r
+#pragma unroll
+          for (int r = 1; r < R; r++) {
+            const float2 w = __ldg(tw + OFFT + (r - 1) * NS + jm);
+            v[q][r] = cmul(v[q][r], DIR < 0 ? cplx{w.x, w.y} : cplx{w.x, -w.y});
+          }
+        } else if constexpr (OFF >= 0) {
           // the stage's row jm: R-1 twiddles, two per 16-byte load
           const float4* t4 = reinterpret_cast<const float4*>(tw + OFF + jm * stage_rp(R));
 #pragma unroll

@@ -1609,8 +1609,9 @@ cudaError_t set_all_smem(int N) {
   return e;
 }
 
-// The twiddle table of length L (W_L^k rounded once from double) and the
-// per-stage rows after it (cgfft::stage_tw_offset), which copy its entries.
+// The twiddle table of length L (W_L^k rounded once from double), the
+// per-stage rows after it (cgfft::stage_tw_offset) and the same stages'
+// transposed runs (cgfft::stage_twt_offset), which copy its entries.
 size_t twiddle_table_len(int L) { return (size_t)cgfft::twiddle_table_len(L); }
 
 void twiddle_table(float2* h, int L) {
@@ -1628,6 +1629,9 @@ void twiddle_table(float2* h, int L) {
       for (int jm = 0; jm < ns; jm++)
         for (int i = 0; i < rp; i++)
           h[off + jm * rp + i] = i + 1 < r ? h[jm * (i + 1) * step] : make_float2(0.0f, 0.0f);
+      const int offt = cgfft::stage_twt_offset(L, ns, r);
+      for (int i = 1; i < r; i++)
+        for (int jm = 0; jm < ns; jm++) h[offt + (i - 1) * ns + jm] = h[jm * i * step];
     }
   }
 }
