@@ -642,6 +642,8 @@ def main():
                     help="the mesh r2c / c2r transforms beside cuFFT's at 384^3 and 768^3")
     ap.add_argument("--fof", action="store_true",
                     help="friends-of-friends halo finding on the z = 0 snapshot (b = 0.2)")
+    ap.add_argument("--batch-streams", type=int, default=4,
+                    help="streams the batch graph spreads its realizations over")
     ap.add_argument("--batch", action="store_true",
                     help="batched realizations: 32 x 128^3 particles / 384^3 meshes, uneven "
                          "boxes and step counts, one CUDA graph per run")
@@ -848,7 +850,7 @@ def run_batch(args):
     """Throughput of batched realizations: 32 realizations of 128^3
     particles on 384^3 meshes with box sizes L ~ U[250, 400] Mpc/h and step
     counts ~ U[5, 20] drawn from a fixed meta-seed, 2LPT at z = 49, recorded
-    into one CUDA graph over 4 streams; a particle-step is one COLA step of
+    into one CUDA graph over --batch-streams streams; a particle-step is one COLA step of
     one particle.  Device time from CUDA events around each graph launch."""
     rank, world, local = dist_setup(args)
     if rank != 0:
@@ -879,7 +881,7 @@ def run_batch(args):
     lib.cg_dropin_set_abort(0)
     lib.power_init(table.encode(), a_init, 0.81, om, 1 - om)
     lib.lpt_init(nc, None, 0)
-    b = Batch(specs, om, nstreams=4)
+    b = Batch(specs, om, nstreams=args.batch_streams)
     dep = None
     for i, sp in enumerate(specs):
         rc = lib.lpt_set_displacement(a_init, om, 1000 + i, sp["boxsize"], ctypes.byref(P))
@@ -920,7 +922,7 @@ def run_batch(args):
            "config": {"workload": "batch: 32 x 128^3 particles, 384^3 meshes, L ~ U[250,400] "
                                   "Mpc/h, nsteps ~ U[5,20] (meta-seed 2024), one CUDA graph",
                       "realizations": nreal, "particle_steps_per_launch": psteps,
-                      "graph_nodes": b.num_nodes(), "streams": 4,
+                      "graph_nodes": b.num_nodes(), "streams": args.batch_streams,
                       "deposit_variant": {"chosen": dep, "chosen_by": "cg_sim_tune_deposit"},
                       "l2": "inputs larger than L2 (0.23 GB per mesh, 32 realizations)"},
            "ms_per_launch": [round(t, 3) for t in times],
