@@ -92,6 +92,12 @@ SIGNATURES = {
     "cg_set_x_gather": (i32, [i32]),
     "cg_set_force_deposit": (i32, [i32]),
     "cg_set_force_interp": (i32, [i32]),
+    "cg_sim_state_ptrs": (i32, [P, ctypes.POINTER(P), ctypes.POINTER(P)]),
+    "cg_sim_spectrum_ptr": (i32, [P, i32, ctypes.POINTER(P)]),
+    "cg_sim_slab_density": (i32, [P, i32, i32, P, i64, dptr]),
+    "cg_sim_slab_kspace": (i32, [P, i32, i32]),
+    "cg_sim_slab_c2r": (i32, [P, i32, i32]),
+    "cg_sim_slab_interp": (i32, [P, i32, i32, P, i64, P]),
     "cg_deposit_variants": (i32, []),
     "cg_get_deposit_variant": (i32, [i32]),
     "cg_set_deposit_variant": (i32, [i32, i32]),

@@ -512,6 +512,72 @@ extern "C" int cg_sim_tune_deposit(cg_sim* s, float* ms) {
   return best;
 }
 
+// ------------------------------------------------ slab decomposition
+// The per-rank stages of a force split over x slabs (pm_slab_* in
+// pm_kernels.cu); the caller moves the spectra and the buffer copies
+// between ranks.  bx / bf: SoA device arrays of nb floats per component.
+
+extern "C" int cg_sim_state_ptrs(cg_sim* s, float** x, float** f) {
+  if (!s || !x || !f) return set_err(CG_EINVAL, "cg_sim_state_ptrs: NULL");
+  for (int a = 0; a < 3; a++) {
+    x[a] = s->ps.x[a];
+    f[a] = s->ps.f[a];
+  }
+  return CG_OK;
+}
+
+extern "C" int cg_sim_spectrum_ptr(cg_sim* s, int which, void** ptr) {
+  if (!s || !ptr || which < 0 || which > 3)
+    return set_err(CG_EINVAL, "cg_sim_spectrum_ptr: bad arguments");
+  *ptr = which == 0 ? (void*)s->pm.spec : (void*)s->pm.gsp[which - 1];
+  return CG_OK;
+}
+
+static void soa3(const float* base, long long n, const float* out[3]) {
+  for (int a = 0; a < 3; a++) out[a] = base ? base + a * n : nullptr;
+}
+
+extern "C" int cg_sim_slab_density(cg_sim* s, int x0, int nx, const float* bx, long long nb,
+                                   double* density_sum) {
+  if (!s || nb < 0 || (nb > 0 && !bx)) return set_err(CG_EINVAL, "cg_sim_slab_density: bad arguments");
+  const float* x[3] = {s->ps.x[0], s->ps.x[1], s->ps.x[2]};
+  const float* b[3];
+  soa3(bx, nb, b);
+  CG_CHECK(pm_slab_density(&s->pm, x0, nx, x, s->ps.n, b, nb, s->st), "slab density");
+  if (density_sum) {
+    CG_CHECK(cudaMemcpyAsync(density_sum, s->pm.dsum, sizeof(double), cudaMemcpyDeviceToHost,
+                             s->st), "read density sum");
+    int rc = check_err_word(s);
+    if (rc) return rc;
+  }
+  return CG_OK;
+}
+
+extern "C" int cg_sim_slab_kspace(cg_sim* s, int kz0, int nkz) {
+  if (!s) return set_err(CG_EINVAL, "cg_sim_slab_kspace: NULL");
+  CG_CHECK(pm_slab_kspace(&s->pm, kz0, nkz, s->st), "slab kspace");
+  return CG_OK;
+}
+
+extern "C" int cg_sim_slab_c2r(cg_sim* s, int x0, int nx) {
+  if (!s) return set_err(CG_EINVAL, "cg_sim_slab_c2r: NULL");
+  CG_CHECK(pm_slab_c2r(&s->pm, x0, nx, s->st), "slab c2r");
+  return CG_OK;
+}
+
+extern "C" int cg_sim_slab_interp(cg_sim* s, int x0, int nx, const float* bx, long long nb,
+                                  float* bf) {
+  if (!s || nb < 0 || (nb > 0 && (!bx || !bf)))
+    return set_err(CG_EINVAL, "cg_sim_slab_interp: bad arguments");
+  const float* x[3] = {s->ps.x[0], s->ps.x[1], s->ps.x[2]};
+  const float* b[3];
+  soa3(bx, nb, b);
+  float* fb[3] = {bf, bf ? bf + nb : nullptr, bf ? bf + 2 * nb : nullptr};
+  CG_CHECK(pm_slab_interp(&s->pm, x0, nx, x, s->ps.n, s->ps.f, b, nb, fb, s->st),
+           "slab interp");
+  return CG_OK;
+}
+
 extern "C" int cg_sim_keep_density(cg_sim* s, int keep) {
   if (!s) return set_err(CG_EINVAL, "cg_sim_keep_density: null handle");
   s->pm.keep_dens = keep != 0;

@@ -170,6 +170,20 @@ bool pm_force_interp_binned();
 cudaError_t pm_force_mesh(PmPlan* p, int a, cudaStream_t st);
 // Column bins for up to n particles on the plan's mesh (no-op when held).
 cudaError_t pm_colbins_reserve(PmPlan* p, long long n);
+// Slab decomposition of the force over ranks (pm_kernels.cu): the density
+// and r2c along z of planes [x0, x0+nx) from the rank's particles and the
+// buffer copies it received (bx, nb: SoA device positions); the x, Green
+// and inverse x passes of kz planes [kz0, kz0+nkz); the three z c2r of
+// planes [x0, x0+nx); the interpolation of the rank's particles and buffer
+// copies from its own planes.  The spectra move between the x and the kz
+// slabs in between (the caller's exchange).
+cudaError_t pm_slab_density(PmPlan* p, int x0, int nx, const float* const x[3], long long n,
+                            const float* const bx[3], long long nb, cudaStream_t st);
+cudaError_t pm_slab_kspace(PmPlan* p, int kz0, int nkz, cudaStream_t st);
+cudaError_t pm_slab_c2r(PmPlan* p, int x0, int nx, cudaStream_t st);
+cudaError_t pm_slab_interp(PmPlan* p, int x0, int nx, const float* const x[3], long long n,
+                           float* const f[3], const float* const bx[3], long long nb,
+                           float* const bf[3], cudaStream_t st);
 // Individual stages (exposed for tests and timing).
 cudaError_t pm_deposit(PmPlan* p, const float* const x[3], long long n, cudaStream_t st);
 // Time every deposit variant on these positions (best of 3, each after a

@@ -308,10 +308,13 @@ __device__ __forceinline__ float gather4(const float* __restrict__ m, int i, con
   return __fadd_rn(__fadd_rn(__fadd_rn(a, b), d), e);
 }
 
-__device__ __forceinline__ float interp_one(const float* __restrict__ m, const Cic& c, int N) {
+// Planes lo <= i < hi take part (the whole mesh: 0, N; a slab of a
+// decomposed mesh: its own planes, pm.c:379-405's local_nx test).
+__device__ __forceinline__ float interp_one(const float* __restrict__ m, const Cic& c, int N,
+                                            int lo, int hi) {
   float f = 0.0f;
-  if (0 <= c.i0 && c.i0 < N) f = __fadd_rn(f, gather4(m, c.i0, c, N, c.t1));
-  if (0 <= c.i1 && c.i1 < N) f = __fadd_rn(f, gather4(m, c.i1, c, N, c.d1));
+  if (lo <= c.i0 && c.i0 < hi) f = __fadd_rn(f, gather4(m, c.i0, c, N, c.t1));
+  if (lo <= c.i1 && c.i1 < hi) f = __fadd_rn(f, gather4(m, c.i1, c, N, c.d1));
   return f;
 }
 
@@ -323,7 +326,7 @@ __global__ void __launch_bounds__(T) k_interp(const float* __restrict__ x0,
                                               const float* __restrict__ m2,
                                               float* __restrict__ f0, float* __restrict__ f1,
                                               float* __restrict__ f2, int N, float scale,
-                                              float x_right, float shiftx) {
+                                              float x_right, float shiftx, int xlo, int xhi) {
   long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long stride = (long long)gridDim.x * blockDim.x;
   for (; i < n; i += stride) {
@@ -331,15 +334,15 @@ __global__ void __launch_bounds__(T) k_interp(const float* __restrict__ x0,
     Cic c = cic_index(px, py, pz, N, scale);
     float a = 0.0f, b = 0.0f, d = 0.0f;
     if (c.ok) {
-      a = interp_one(m0, c, N);
-      b = interp_one(m1, c, N);
-      d = interp_one(m2, c, N);
+      a = interp_one(m0, c, N, xlo, xhi);
+      b = interp_one(m1, c, N, xlo, xhi);
+      d = interp_one(m2, c, N, xlo, xhi);
       if (px > x_right) {
         Cic g = cic_index(__fadd_rn(px, shiftx), py, pz, N, scale);
         if (g.ok) {
-          a = __fadd_rn(a, interp_one(m0, g, N));
-          b = __fadd_rn(b, interp_one(m1, g, N));
-          d = __fadd_rn(d, interp_one(m2, g, N));
+          a = __fadd_rn(a, interp_one(m0, g, N, xlo, xhi));
+          b = __fadd_rn(b, interp_one(m1, g, N, xlo, xhi));
+          d = __fadd_rn(d, interp_one(m2, g, N, xlo, xhi));
         }
       }
     }
@@ -829,6 +832,7 @@ struct GreenMods {
   int n;
   float inv_dn;
   const float* tab;
+  int kz0;          // kz of the first plane the launch sees (a kz slab; 0: the whole spectrum)
   __device__ __forceinline__ float at(int den) const {
     const float r = __fmul_rn(sqrtf((float)den), inv_dn);
     const int i = (int)r;
@@ -914,7 +918,7 @@ __global__ void __launch_bounds__(TG, MINB) k_green(const float2* __restrict__ s
   cplx* D = reinterpret_cast<cplx*>(smraw);
   cplx* W = D + BG * P;
   const size_t l0 = (size_t)blockIdx.x * BG;
-  const int kz = (int)(l0 / N);
+  const int kz = (int)(l0 / N) + gm.kz0;
   const int kx0 = (int)(l0 % N);
   const size_t off = l0 * N;
   const cgfft::GmemC<N, 1> gin{const_cast<float2*>(spec) + off};
@@ -2353,7 +2357,132 @@ cudaError_t pm_interp(PmPlan* p, const float* const x[3], long long n, float* co
     prof_mark(st, CG_ST_INTERP);
     k_interp<<<grid_for(n), T, 0, st>>>(x[0], x[1], x[2], n, p->fmesh[0], p->fmesh[1],
                                         p->fmesh[2], f[0], f[1], f[2], p->N, p->scale,
-                                        p->x_right, p->shiftx);
+                                        p->x_right, p->shiftx, 0, p->N);
+  }
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------ slab decomposition
+// One realization's PM force split over ranks by x slabs of mesh planes,
+// the reference's MPI decomposition (comm.c:35-111, pm.c:416-532) with the
+// exchanges left to the caller.  Every rank holds full-size meshes; rank r
+// works on planes [x0, x0 + nx) in real space and on kz planes
+// [kz0, kz0 + nkz) of the spectra.  Particles within one cell of a slab's
+// upper edge act on the next slab through buffer copies, as in
+// send_buffer_positions / add_buffer_forces: the owner sends their
+// positions (shifted by -L across the periodic face), the next rank deposits
+// them and interpolates their forces, and the owner adds those forces to its
+// particles'.  The copies inside the kernels are switched off
+// (x_right = +inf) and each rank reads only its own planes.
+
+// Signed wavenumber index table (n <= N/2 ? n : n - N), the n_z factor of
+// the z component's inverse x pass from an offset kz.
+static cudaError_t sgn_table(PmPlan* p, const float** out) {
+  static std::mutex mu;
+  static std::map<std::pair<int, int>, float*> tabs;   // (device, N)
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = tabs.find({dev, p->N});
+  if (it == tabs.end()) {
+    std::vector<float> h(p->N);
+    for (int i = 0; i < p->N; i++) h[i] = (float)(i <= p->N / 2 ? i : i - p->N);
+    float* d = nullptr;
+    cudaError_t e = cudaMalloc(&d, sizeof(float) * p->N);
+    if (e == cudaSuccess) e = cudaMemcpy(d, h.data(), sizeof(float) * p->N, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return e;
+    it = tabs.emplace(std::make_pair(dev, p->N), d).first;
+  }
+  *out = it->second;
+  return cudaSuccess;
+}
+
+cudaError_t pm_slab_density(PmPlan* p, int x0, int nx, const float* const x[3], long long n,
+                            const float* const bx[3], long long nb, cudaStream_t st) {
+  MeshKernels k;
+  if (!get_kernels(p->N, &k)) return cudaErrorInvalidValue;
+  const int N = p->N;
+  if (x0 < 0 || nx < 1 || x0 + nx > N) return cudaErrorInvalidValue;
+  const size_t plane = (size_t)N * N;
+  const size_t n4 = plane * nx / 4;
+  prof_mark(st, CG_ST_FILL);
+  k_fill<<<grid_for((long long)n4), T, 0, st>>>(reinterpret_cast<float4*>(p->dens + x0 * plane),
+                                               n4, -1.0f);
+  PmPlan q = *p;
+  q.x_right = INFINITY;      // the buffer copies are deposited by the next rank
+  if (n > 0) launch_deposit(&q, x, n, sched_for(N).dep, st);
+  if (nb > 0) {
+    prof_mark(st, CG_ST_DEPOSIT);
+    k_deposit<<<grid_for(nb), T, 0, st>>>(bx[0], bx[1], bx[2], nb, p->dens, N, p->scale,
+                                          p->wpar, INFINITY, 0.0f, p->err);
+  }
+  cudaMemsetAsync(p->dsum, 0, sizeof(double), st);
+  prof_mark(st, CG_ST_FZ);
+  k.fz<<<dim3(N / TY, nx), T, k.sm_fz, st>>>(p->dens + x0 * plane, p->spec + (size_t)x0 * N,
+                                             p->twH, p->twN, p->dsum);
+  p->dens_reset = false;
+  p->dens_stale = true;       // only this slab's planes hold the density
+  p->fmesh_stale = false;
+  return cudaGetLastError();
+}
+
+cudaError_t pm_slab_kspace(PmPlan* p, int kz0, int nkz, cudaStream_t st) {
+  MeshKernels k;
+  if (!get_kernels(p->N, &k)) return cudaErrorInvalidValue;
+  const int N = p->N;
+  if (kz0 < 0 || nkz < 1 || kz0 + nkz > N / 2 + 1) return cudaErrorInvalidValue;
+  const float* sgn = nullptr;
+  cudaError_t e = sgn_table(p, &sgn);
+  if (e != cudaSuccess) return e;
+  const size_t off = (size_t)kz0 * N * N;
+  const dim3 gx(N / k.tk, nkz);
+  prof_mark(st, CG_ST_FX_FWD);
+  k.fxf<<<gx, T, k.sm_fx, st>>>(p->spec + off, p->spec + off, p->twN, nullptr);
+  prof_mark(st, CG_ST_GREEN);
+  GreenMods gm{p->kfilt_cur >= 0 ? p->kfilt + (size_t)p->kfilt_cur * p->kfilt_n : nullptr,
+               p->kfilt_n, p->kfilt_inv_dn, p->ktab, kz0};
+  (gm.t || gm.tab ? k.green_mods : k.green)<<<nkz * N / k.byg, k.tg, k.sm_green, st>>>(
+      p->spec + off, p->gsp[1] + off, p->gsp[2] + off, p->twN, p->f1, gm);
+  prof_mark(st, CG_ST_FX_INV);
+  k.fxi_x<<<gx, T, k.sm_fx, st>>>(p->gsp[2] + off, p->gsp[0] + off, p->twN, p->ktab);
+  prof_mark(st, CG_ST_FX_INV);
+  k.fxi<<<gx, T, k.sm_fx, st>>>(p->gsp[1] + off, p->gsp[1] + off, p->twN, nullptr);
+  prof_mark(st, CG_ST_FX_INV);
+  k.fxi_z<<<gx, T, k.sm_fx, st>>>(p->gsp[2] + off, p->gsp[2] + off, p->twN,
+                                  (p->ktab ? p->ktab : sgn) + kz0);
+  return cudaGetLastError();
+}
+
+cudaError_t pm_slab_c2r(PmPlan* p, int x0, int nx, cudaStream_t st) {
+  MeshKernels k;
+  if (!get_kernels(p->N, &k)) return cudaErrorInvalidValue;
+  const int N = p->N;
+  if (x0 < 0 || nx < 1 || x0 + nx > N) return cudaErrorInvalidValue;
+  for (int a = 0; a < 3; a++) {
+    prof_mark(st, CG_ST_ZI);
+    k.zi<<<dim3(N / TY, nx), T, k.sm_zi, st>>>(p->gsp[a] + (size_t)x0 * N,
+                                               p->fmesh[a] + (size_t)x0 * N * N, p->twH,
+                                               p->twN);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t pm_slab_interp(PmPlan* p, int x0, int nx, const float* const x[3], long long n,
+                           float* const f[3], const float* const bx[3], long long nb,
+                           float* const bf[3], cudaStream_t st) {
+  const int N = p->N;
+  if (x0 < 0 || nx < 1 || x0 + nx > N) return cudaErrorInvalidValue;
+  if (n > 0) {
+    prof_mark(st, CG_ST_INTERP);
+    k_interp<<<grid_for(n), T, 0, st>>>(x[0], x[1], x[2], n, p->fmesh[0], p->fmesh[1],
+                                        p->fmesh[2], f[0], f[1], f[2], N, p->scale, INFINITY,
+                                        0.0f, x0, x0 + nx);
+  }
+  if (nb > 0) {
+    prof_mark(st, CG_ST_INTERP);
+    k_interp<<<grid_for(nb), T, 0, st>>>(bx[0], bx[1], bx[2], nb, p->fmesh[0], p->fmesh[1],
+                                         p->fmesh[2], bf[0], bf[1], bf[2], N, p->scale,
+                                         INFINITY, 0.0f, x0, x0 + nx);
   }
   return cudaGetLastError();
 }

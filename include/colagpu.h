@@ -358,6 +358,39 @@ int cg_set_force_deposit(int mode);
  * a step with 1, cg_sim_get_mesh(s, 1..3, ..) transforms the requested
  * force mesh from its spectrum first.  COLAGPU_FUSED_INTERP=0/1 overrides. */
 int cg_set_force_interp(int mode);
+
+/* Slab decomposition of one realization's PM force over ranks (one GPU per
+ * rank).  It replaces the reference's MPI slabs: comm_init's x slabs
+ * (comm.c:35-111), the FFTW-MPI transposes inside pm.c:282-355, the buffer
+ * particles of send_buffer_positions / add_buffer_forces (pm.c:416-532) and
+ * move_particles2's exchange (move.c:15-175).  Every rank's handle holds full-size
+ * meshes; rank r owns mesh planes [x0, x0 + nx) and kz planes [kz0, kz0 +
+ * nkz) of the spectra.  Per force evaluation:
+ *   cg_sim_slab_density  density of the rank's particles and of the buffer
+ *                        copies it received (bx: 3 x nb floats, SoA, device;
+ *                        copies keep their own weights, shifted by -L across
+ *                        the periodic face), its r2c along z for planes
+ *                        [x0, x0+nx); density_sum (may be NULL) receives the
+ *                        slab's part of check_total_density's sum;
+ *   (caller)             spectrum x slabs -> kz slabs (cg_sim_spectrum_ptr 0);
+ *   cg_sim_slab_kspace   x, Green and inverse x passes of kz planes [kz0,
+ *                        kz0+nkz) into the three force spectra;
+ *   (caller)             force spectra kz slabs -> x slabs (ptr 1..3);
+ *   cg_sim_slab_c2r      the three z c2r of planes [x0, x0+nx);
+ *   cg_sim_slab_interp   forces of the rank's particles and of the buffer
+ *                        copies (bf: 3 x nb floats) from planes [x0, x0+nx);
+ *   (caller)             buffer forces back to their owners, added to theirs.
+ * cg_sim_state_ptrs gives the device arrays of positions and forces (three
+ * each); cg_sim_spectrum_ptr the half spectrum (0) or the force spectra
+ * (1..3), laid out [kz][kx][ky].  cola_halo_b200/slab.py drives them over
+ * torch.distributed. */
+int cg_sim_state_ptrs(cg_sim* s, float** x, float** f);
+int cg_sim_spectrum_ptr(cg_sim* s, int which, void** ptr);
+int cg_sim_slab_density(cg_sim* s, int x0, int nx, const float* bx, long long nb,
+                        double* density_sum);
+int cg_sim_slab_kspace(cg_sim* s, int kz0, int nkz);
+int cg_sim_slab_c2r(cg_sim* s, int x0, int nx);
+int cg_sim_slab_interp(cg_sim* s, int x0, int nx, const float* bx, long long nb, float* bf);
 /* Shape of the CIC deposit per mesh size (no reference counterpart; the
  * reference's PtoMesh is pm.c:209-279): variant v of cg_deposit_variants()
  * sets the particles per CTA and the shared-memory box (512 / 3,072 cells,
