@@ -647,6 +647,9 @@ def main():
     ap.add_argument("--batch", action="store_true",
                     help="batched realizations: 32 x 128^3 particles / 384^3 meshes, uneven "
                          "boxes and step counts, one CUDA graph per run")
+    ap.add_argument("--slab", action="store_true",
+                    help="one realization split over the ranks by x slabs (cola_halo_b200.slab; "
+                         "NCCL between the ranks of a torchrun job)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "b200":
         args.warmup = 3
@@ -665,7 +668,110 @@ def main():
         cfg["nc"], cfg["nc"] * cfg["factor"], cfg["L"])
     if args.impl == "reference":
         return run_reference(args, cfg)
+    if args.slab:
+        return run_slab(args, cfg)
     return run_b200(args, cfg)
+
+
+def run_slab(args, cfg):
+    """One realization split over the job's ranks by x slabs of the mesh
+    (the reference's MPI decomposition, cola_halo_b200.slab): per step the
+    wrap, the particles' moves to their slabs, the slab-decomposed force and
+    the kick + drift.  Strong scaling: the realization is the same for every
+    N.  Device time from CUDA events around the steps, max over ranks."""
+    rank, world, local = dist_setup(args)
+    import torch
+    from cola_halo_b200 import Simulation, _lib
+    from cola_halo_b200.bbks import write_bbks_table
+    from cola_halo_b200.schedule import Schedule
+    from cola_halo_b200.slab import GpuRank, LocalComm, SlabPM, TorchComm
+    from cola_halo_b200.types import PARTICLE_DTYPE, Particles
+    lib = _lib.load()
+    _lib.check(lib.cg_set_device(local), "cg_set_device")
+    torch.cuda.set_device(local)
+    td = None
+    if world > 1:
+        import datetime
+        import torch.distributed as td
+        td.init_process_group("nccl", device_id=torch.device("cuda", local),
+                              timeout=datetime.timedelta(seconds=600))
+    nc, factor, L, om = cfg["nc"], cfg["factor"], cfg["L"], cfg["om"]
+    N, npart = nc * factor, nc ** 3
+    sched = Schedule.linear(cfg["a_init"], 1.0, cfg["nsteps"])
+    table = write_bbks_table(os.path.join(tempfile.mkdtemp(), "bbks.dat"))
+    # the same 2LPT initial conditions on every rank (the GPU lpt of the
+    # drop-in layer); each rank keeps the particles of its slab
+    nbytes = 56 * npart
+    hp = lib.cg_host_alloc(nbytes)
+    host = np.ctypeslib.as_array((ctypes.c_uint8 * nbytes).from_address(hp)).view(PARTICLE_DTYPE)
+    P = Particles()
+    P.p, P.force, P.np_allocated, P.np_total, P.np_average = hp, None, npart, npart, float(npart)
+    lib.cg_dropin_set_abort(0)
+    lib.power_init(table.encode(), sched.a_init, 0.81, om, 1 - om)
+    lib.lpt_init(nc, None, 0)
+    assert lib.lpt_set_displacement(sched.a_init, om, cfg["seed"], L, ctypes.byref(P)) == 0
+    rows = torch.from_numpy(np.ascontiguousarray(host).view(np.float32).reshape(npart, 14).copy())
+    lib.cg_dropin_finalize()
+    comm = TorchComm(device="cuda") if world > 1 else LocalComm(1)
+    cap = int(2.0 * npart / world) + 1024
+    sim = Simulation(nc, N, L, om, np_capacity=cap)
+    rk = GpuRank(sim)
+    pm = SlabPM([rk], comm, "cuda")
+    x0 = pm.xs[rank][0] * np.float32(L) / N
+    x1 = (pm.xs[rank][0] + pm.xs[rank][1]) * np.float32(L) / N
+    xw = torch.remainder(rows[:, 0], L)
+    mine = rows[(xw >= x0) & (xw < x1)].cuda()
+    nsteps_run = sched.nloop - 1
+
+    def step(i):
+        j = i % nsteps_run
+        if j == 0:       # a realization restarts from the initial conditions
+            sim.set_particles_ptr(mine.data_ptr(), mine.shape[0], sched.a_init, sched.a_init)
+        _, _, avel1, apos1 = sched.times(j + 1)
+        sim.move()
+        pm.exchange_particles()
+        pm.forces()
+        sim.kick_drift(avel1, apos1)
+
+    def barrier():
+        if td:
+            td.barrier()
+    steps = args.steps
+    for i in range(args.warmup):
+        step(i)
+    sim.sync()
+    barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    for i in range(steps):
+        step(args.warmup + i)
+    sim.sync()
+    ev1.record()
+    ev1.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    if td:
+        t = torch.tensor([ms], device="cuda")
+        td.all_reduce(t, op=td.ReduceOp.MAX)
+        ms = float(t.item())
+    barrier()
+    if rank == 0:
+        out = {"metric": METRIC, "value": npart * steps / (ms / 1e3), "unit": "particle-steps/s",
+               "n_gpus": world, "steps": steps, "warmup": args.warmup, "ms_per_step": ms / steps,
+               "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+               "dtype": "f32", "data": "synthetic (seeded 2LPT initial conditions, BBKS P(k))",
+               "config": {"workload": args.config_desc, "particles": npart, "mesh": N,
+                          "boxsize": L, "parallelism": "slab x%d (one realization split by "
+                                                      "x slabs)" % world,
+                          "l2": "inputs larger than L2 (%.2f GB per mesh)" % (4.0 * N ** 3 / 1e9)},
+               "density_sum": pm.density_sum,
+               "note": "the slab-decomposed path (exchanges through torch); the default "
+                       "bench line runs whole realizations per GPU"}
+        print(json.dumps(out))
+    sim.close()
+    lib.cg_host_free(hp)
+    if td:
+        td.destroy_process_group()
+    return 0
 
 
 def _z0_snapshot(lib, cfg, table):

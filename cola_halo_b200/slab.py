@@ -221,6 +221,10 @@ class SlabPM:
                 else:          # my kz slab, s's x slab
                     (x0, nx), (k0, nk) = self.xs[s], self.ks[r]
                     (rx0, rnx), (rk0, rnk) = self.xs[r], self.ks[s]
+                if s == r:     # the block a rank keeps is already in place
+                    row.append(None)
+                    srow.append(None)
+                    continue
                 row.append(t[k0:k0 + nk, x0:x0 + nx].contiguous())
                 srow.append((rnk, rnx, N, 2))
             sends.append(row)
@@ -233,13 +237,16 @@ class SlabPM:
                     (rx0, rnx), (rk0, rnk) = self.xs[s], self.ks[r]
                 else:
                     (rx0, rnx), (rk0, rnk) = self.xs[r], self.ks[s]
-                t[rk0:rk0 + rnk, rx0:rx0 + rnx] = got[i][s]
+                if s != r:
+                    t[rk0:rk0 + rnk, rx0:rx0 + rnx] = got[i][s]
             self.ranks[i].sync()
 
     # -- particles to the rank of their slab (move.c:15-175, after the wrap)
     def exchange_particles(self):
         P, dev = self.size, self.device
         me = self.comm.ranks
+        if P == 1:
+            return [self.ranks[0].n]
         bounds = [self.x_bounds(s) for s in range(P)]
         edges = torch.tensor([float(b[0]) for b in bounds[1:]], dtype=torch.float32, device=dev)
         sends, keep = [], []
