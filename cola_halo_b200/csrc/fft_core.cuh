@@ -25,14 +25,35 @@ namespace cgfft {
 // ------------------------------------------------------------ complex ops
 struct cplx { float x, y; };
 
+// The fused multiply-adds are explicit, so that every kernel built on these
+// butterflies rounds a product the same way (the compiler's own contraction
+// may fuse either product, differently from one kernel to the next).
 __device__ __forceinline__ cplx cmul(cplx a, cplx b) {
-  return {a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x};
+  return {__fmaf_rn(a.x, b.x, -__fmul_rn(a.y, b.y)), __fmaf_rn(a.x, b.y, __fmul_rn(a.y, b.x))};
 }
-__device__ __forceinline__ cplx cadd(cplx a, cplx b) { return {a.x + b.x, a.y + b.y}; }
-__device__ __forceinline__ cplx csub(cplx a, cplx b) { return {a.x - b.x, a.y - b.y}; }
+// Complex sums as paired fp32 instructions (sm_100's two-lane add and fma,
+// through the CUDA float2 intrinsics): one instruction for both components,
+// each rounded exactly as the scalar operation.  fma(b, +-1, a) is a +- b
+// rounded once, so the sign pairs below give mixed-sign sums in one
+// instruction as well.
+__device__ __forceinline__ float2 f2(cplx a) { return make_float2(a.x, a.y); }
+__device__ __forceinline__ cplx c2(float2 a) { return {a.x, a.y}; }
+__device__ __forceinline__ cplx cadd(cplx a, cplx b) { return c2(__fadd2_rn(f2(a), f2(b))); }
+__device__ __forceinline__ cplx csub(cplx a, cplx b) {
+  return c2(__ffma2_rn(f2(b), make_float2(-1.0f, -1.0f), f2(a)));
+}
+// a + (s.x b.x, s.y b.y), one rounding per component
+__device__ __forceinline__ cplx cfma(cplx b, float2 s, cplx a) {
+  return c2(__ffma2_rn(f2(b), s, f2(a)));
+}
 // multiply by -i (forward) or +i (inverse):  DIR = -1 forward, +1 inverse
 template <int DIR> __device__ __forceinline__ cplx mul_i(cplx a) {
   return DIR < 0 ? cplx{a.y, -a.x} : cplx{-a.y, a.x};
+}
+// a +- i_DIR t, given t with its components swapped, ts = (t.y, t.x):
+// i_DIR t = DIR < 0 ? (t.y, -t.x) : (-t.y, t.x) = ts * isgn<DIR>()
+template <int DIR> __device__ __forceinline__ float2 isgn() {
+  return DIR < 0 ? make_float2(1.0f, -1.0f) : make_float2(-1.0f, 1.0f);
 }
 template <int DIR> __device__ __forceinline__ cplx twiddle(const float2* __restrict__ tw, int t) {
   float2 w = __ldg(tw + t);
@@ -51,22 +72,30 @@ template <int DIR> __device__ __forceinline__ void dft3(cplx* v) {
   const float s = 0.866025403784438646763723170753f;
   cplx a = v[0], b = v[1], c = v[2];
   cplx t = cadd(b, c);
-  cplx d = csub(b, c);
-  cplx m = {a.x - 0.5f * t.x, a.y - 0.5f * t.y};
-  // DIR*i*s*d
-  cplx r = DIR < 0 ? cplx{s * d.y, -s * d.x} : cplx{-s * d.y, s * d.x};
+  // d = b - c with its components swapped, for r = DIR i s d = ds * (s isgn)
+  const cplx ds = {b.y - c.y, b.x - c.x};
+  const cplx m = cfma(t, make_float2(-0.5f, -0.5f), a);
+  const float2 sr = DIR < 0 ? make_float2(s, -s) : make_float2(-s, s);
   v[0] = cadd(a, t);
-  v[1] = cadd(m, r);
-  v[2] = csub(m, r);
+  v[1] = cfma(ds, sr, m);
+  v[2] = cfma(ds, make_float2(-sr.x, -sr.y), m);
 }
 
-template <int DIR> __device__ __forceinline__ void dft4(cplx* v) {
+// OUT2 = 0: plain; 1: output 2 multiplied by i_DIR; 2: output 2 with its
+// components swapped (for a following cfma).  Either costs one scalar
+// subtraction more than the plain output.
+template <int DIR, int OUT2 = 0> __device__ __forceinline__ void dft4(cplx* v) {
   cplx s0 = cadd(v[0], v[2]), d0 = csub(v[0], v[2]);
-  cplx s1 = cadd(v[1], v[3]), d1 = mul_i<DIR>(csub(v[1], v[3]));
+  cplx s1 = cadd(v[1], v[3]);
+  // v1 - v3 with its components swapped (two scalar subtractions)
+  const cplx ts = {v[1].y - v[3].y, v[1].x - v[3].x};
+  const float2 sg = isgn<DIR>();
   v[0] = cadd(s0, s1);
-  v[2] = csub(s0, s1);
-  v[1] = cadd(d0, d1);
-  v[3] = csub(d0, d1);
+  if constexpr (OUT2 == 0) v[2] = csub(s0, s1);
+  else if constexpr (OUT2 == 2) v[2] = cplx{s0.y - s1.y, s0.x - s1.x};
+  else v[2] = DIR < 0 ? cplx{s0.y - s1.y, s1.x - s0.x} : cplx{s1.y - s0.y, s0.x - s1.x};
+  v[1] = cfma(ts, sg, d0);
+  v[3] = cfma(ts, make_float2(-sg.x, -sg.y), d0);
 }
 
 // 8-point: two 4-point DFTs on even/odd samples, then the W8 butterflies.
@@ -75,18 +104,24 @@ template <int DIR> __device__ __forceinline__ void dft8(cplx* v) {
   cplx e[4] = {v[0], v[2], v[4], v[6]};
   cplx o[4] = {v[1], v[3], v[5], v[7]};
   dft4<DIR>(e);
-  dft4<DIR>(o);
+  dft4<DIR, 2>(o);    // o[2] comes back swapped
   // o[k] *= W8^{DIR k}: k=1: (h, DIR h), k=2: DIR i, k=3: (-h, DIR h)
   cplx o1 = o[1], o3 = o[3];
   o[1] = DIR < 0 ? cplx{h * (o1.x + o1.y), h * (o1.y - o1.x)}
                  : cplx{h * (o1.x - o1.y), h * (o1.y + o1.x)};
-  o[2] = mul_i<DIR>(o[2]);
   o[3] = DIR < 0 ? cplx{h * (o3.y - o3.x), -h * (o3.x + o3.y)}
                  : cplx{-h * (o3.x + o3.y), h * (o3.x - o3.y)};
+  const float2 sg = isgn<DIR>();
 #pragma unroll
   for (int k = 0; k < 4; k++) {
-    v[k] = cadd(e[k], o[k]);
-    v[k + 4] = csub(e[k], o[k]);
+    if (k == 2) {
+      // e2 +- i_DIR o2, o2 swapped
+      v[2] = cfma(o[2], sg, e[2]);
+      v[6] = cfma(o[2], make_float2(-sg.x, -sg.y), e[2]);
+    } else {
+      v[k] = cadd(e[k], o[k]);
+      v[k + 4] = csub(e[k], o[k]);
+    }
   }
 }
 
@@ -100,7 +135,9 @@ template <int DIR> __device__ __forceinline__ void dft16(cplx* v) {
 #pragma unroll
   for (int n2 = 0; n2 < 4; n2++) {
     cplx t[4] = {v[n2], v[n2 + 4], v[n2 + 8], v[n2 + 12]};
-    dft4<DIR>(t);
+    // a[2][2]'s twiddle W16^{DIR 4} = i_DIR is applied as it is formed
+    if (n2 == 2) dft4<DIR, 1>(t);
+    else dft4<DIR>(t);
 #pragma unroll
     for (int k1 = 0; k1 < 4; k1++) a[n2][k1] = t[k1];
   }
@@ -109,7 +146,7 @@ template <int DIR> __device__ __forceinline__ void dft16(cplx* v) {
   const cplx w1 = {c1, ds * s1}, w2 = {h, ds * h}, w3 = {s1, ds * c1};
   const cplx w6 = {-h, ds * h}, w9 = {-c1, -ds * s1};
   a[1][1] = cmul(a[1][1], w1); a[1][2] = cmul(a[1][2], w2); a[1][3] = cmul(a[1][3], w3);
-  a[2][1] = cmul(a[2][1], w2); a[2][2] = mul_i<DIR>(a[2][2]); a[2][3] = cmul(a[2][3], w6);
+  a[2][1] = cmul(a[2][1], w2); a[2][3] = cmul(a[2][3], w6);
   a[3][1] = cmul(a[3][1], w3); a[3][2] = cmul(a[3][2], w6); a[3][3] = cmul(a[3][3], w9);
 #pragma unroll
   for (int k1 = 0; k1 < 4; k1++) {
@@ -341,6 +378,17 @@ template <class A> struct HasPad16<A, decltype((void)A::kPad16)> {
 };
 template <class A> __host__ __device__ constexpr bool has_pad16() { return HasPad16<A>::v; }
 
+// Accessors that declare kDistinct = true are never the same buffer as the
+// shared tile `mid` of the transform they start or end (the Green pass's
+// loader of the forward-transformed tile, which feeds a second tile), so
+// the first stage (first -> mid) and the last (mid -> last) need no barrier
+// between their loads and their stores.
+template <class A, class = void> struct IsDistinct { static constexpr bool v = false; };
+template <class A> struct IsDistinct<A, decltype((void)A::kDistinct)> {
+  static constexpr bool v = A::kDistinct;
+};
+template <class A> __host__ __device__ constexpr bool distinct() { return IsDistinct<A>::v; }
+
 // T = 32: the tile belongs to one warp (thread = lane, barriers are warp
 // barriers), so warps of a CTA run their tiles independently.  Otherwise the
 // tile belongs to the CTA's T threads.
@@ -458,11 +506,11 @@ __device__ __forceinline__ void fft_io_from(const First& first, const Mid& mid, 
     if constexpr (S == 0)
       stage_io<L, R, NS, B, T, LML, DIR>(first, last, tw, First::kShared && Last::kShared);
     else
-      stage_io<L, R, NS, B, T, LML, DIR>(mid, last, tw, Last::kShared);
+      stage_io<L, R, NS, B, T, LML, DIR>(mid, last, tw, Last::kShared && !distinct<Last>());
     if constexpr (Last::kShared) tile_sync<T>();
   } else {
     if constexpr (S == 0)
-      stage_io<L, R, NS, B, T, LM, DIR>(first, mid, tw, First::kShared);
+      stage_io<L, R, NS, B, T, LM, DIR>(first, mid, tw, First::kShared && !distinct<First>());
     else
       stage_io<L, R, NS, B, T, LM, DIR>(mid, mid, tw, true);
     tile_sync<T>();

@@ -889,6 +889,13 @@ struct GreenLoad {
     return cplx{-__fmul_rn(f2, p.y), __fmul_rn(f2, p.x)};
   }
   static constexpr bool kShared = true;
+  // never the output tile of the stage that reads it (k_green's first
+  // inverse stage reads D and writes W), so that stage needs no barrier
+  // between its loads and its stores; unreferenced where the transform has
+  // one stage
+#pragma nv_diag_suppress 177
+  static constexpr bool kDistinct = true;
+#pragma nv_diag_default 177
 };
 
 // The three transforms of the fused pass as separate (not inlined) calls:
