@@ -382,10 +382,10 @@ struct FxCfg { int tk, rm; };
 struct GreenCfg { int byg, rm, minb, thr; };
 constexpr FxCfg kFxCfg[PM_NUM_FX_VARIANTS] = {{8, 0}, {8, -1}, {16, 16}};
 // (lines per CTA, maximum radix, CTAs per SM, threads): at 768 a radix-16
-// stage has 48 butterflies per line, so 8 lines fill 384 threads and 4
-// lines 192 once each.
+// stage has 48 butterflies per line, so 8 lines fill 384 threads, 4 lines
+// 192 and 2 lines 96 once each.
 constexpr GreenCfg kGreenCfg[PM_NUM_GREEN_VARIANTS] = {
-    {4, 16, 3, 256}, {8, 8, 2, 256}, {8, 16, 2, 384}, {4, 16, 4, 192}};
+    {4, 16, 3, 256}, {8, 8, 2, 256}, {8, 16, 2, 384}, {4, 16, 4, 192}, {2, 16, 8, 96}};
 __host__ __device__ constexpr int rm_x_default(int N) { return N >= 768 ? 8 : 16; }
 __host__ __device__ constexpr int fx_rm(int N, int v) {
   return kFxCfg[v].rm == 0 ? rm_x_default(N)
@@ -1172,7 +1172,7 @@ __device__ __forceinline__ void zsw_halfcomplex(const cgfft::SmemSw16& t,
 }
 
 template <int N>
-__global__ void __launch_bounds__(T, N >= 1024 ? 3 : 4) k_zi_sw(const __grid_constant__ CUtensorMap tm,
+__global__ void __launch_bounds__(T, N >= 768 ? 3 : 4) k_zi_sw(const __grid_constant__ CUtensorMap tm,
                                              float* __restrict__ out,
                                              const float2* __restrict__ twH,
                                              const float2* __restrict__ twN,
@@ -1552,6 +1552,7 @@ MeshKernels make_kernels(MeshSched s) {
       case 1: set_green<N, 1>(&k); break;
       case 2: set_green<N, 2>(&k); break;
       case 3: set_green<N, 3>(&k); break;
+      case 4: set_green<N, 4>(&k); break;
       default: set_green<N, 0>(&k);
     }
   } else {
