@@ -55,8 +55,27 @@ template <int DIR> __device__ __forceinline__ cplx mul_i(cplx a) {
 template <int DIR> __device__ __forceinline__ float2 isgn() {
   return DIR < 0 ? make_float2(1.0f, -1.0f) : make_float2(-1.0f, 1.0f);
 }
-template <int DIR> __device__ __forceinline__ cplx twiddle(const float2* __restrict__ tw, int t) {
-  float2 w = __ldg(tw + t);
+// Twiddle sources: the global table (read through the read-only path), or
+// entries [BASE, BASE + n) of it copied into shared memory by the CTA
+// (TwShared; p points at the copy of entry BASE, 16-byte aligned).
+template <int BASE> struct TwShared { const float2* p; };
+template <class TW> struct IsTwShared { static constexpr bool v = false; };
+template <int BASE> struct IsTwShared<TwShared<BASE>> { static constexpr bool v = true; };
+__device__ __forceinline__ float2 tw_ld(const float2* __restrict__ tw, int i) {
+  return __ldg(tw + i);
+}
+template <int BASE> __device__ __forceinline__ float2 tw_ld(const TwShared<BASE>& tw, int i) {
+  return tw.p[i - BASE];
+}
+// two entries i, i+1 (i even: 16-byte aligned in the table and in the copy)
+__device__ __forceinline__ float4 tw_ld2(const float2* __restrict__ tw, int i) {
+  return __ldg(reinterpret_cast<const float4*>(tw + i));
+}
+template <int BASE> __device__ __forceinline__ float4 tw_ld2(const TwShared<BASE>& tw, int i) {
+  return *reinterpret_cast<const float4*>(tw.p + (i - BASE));
+}
+template <int DIR, class TW> __device__ __forceinline__ cplx twiddle(const TW& tw, int t) {
+  float2 w = tw_ld(tw, t);
   return DIR < 0 ? cplx{w.x, w.y} : cplx{w.x, -w.y};
 }
 
@@ -266,6 +285,36 @@ __host__ __device__ constexpr int stage_twt_offset(int L, int NS, int R) {
 }
 __host__ __device__ constexpr int twiddle_table_len(int L) { return stage_twt_offset(L, 0, 0); }
 
+// The table entries an L-point transform (maximum radix RM, stage mappings
+// LM and LML as in fft_io) reads: [tw_copy_lo, tw_copy_hi), both even, so
+// that a copy of them keeps the stage rows 16-byte aligned.
+__host__ __device__ constexpr int tw_copy_bound(int L, int RM, bool LM, bool LML, bool hi) {
+  int lo_v = 1 << 30, hi_v = 0;
+  const int ns = num_stages(L, RM);
+  for (int st = 1; st < ns; st++) {
+    const int n = ns_before(L, st, RM), r = radix_at(L, st, RM);
+    const bool line = st == ns - 1 ? LML : LM;
+    const int off = line ? stage_twt_offset(L, n, r) : stage_tw_offset(L, n, r);
+    const int end = off + (line ? n * (r - 1) : n * stage_rp(r));
+    lo_v = off < lo_v ? off : lo_v;
+    hi_v = end > hi_v ? end : hi_v;
+  }
+  if (hi_v == 0) return 0;
+  return hi ? (hi_v + 1) / 2 * 2 : lo_v / 2 * 2;
+}
+template <int L, int RM, bool LM, bool LML> struct TwCopy {
+  static constexpr int lo = tw_copy_bound(L, RM, LM, LML, false);
+  static constexpr int hi = tw_copy_bound(L, RM, LM, LML, true);
+  static constexpr int bytes = (hi - lo) * 8;
+  // entries [lo, hi) of the table tw into dst (16-byte aligned), by T threads
+  template <int T>
+  __device__ static __forceinline__ void copy(float2* dst, const float2* __restrict__ tw) {
+    const float4* src = reinterpret_cast<const float4*>(tw + lo);
+    float4* d = reinterpret_cast<float4*>(dst);
+    for (int i = (int)threadIdx.x; i < (hi - lo) / 2; i += T) d[i] = __ldg(src + i);
+  }
+};
+
 // ------------------------------------------------------------ tile access
 // The first stage reads its legs j + r L/R and the last writes its outputs
 // (j/NS) NS R + (j mod NS) + r NS; with consecutive threads on consecutive
@@ -400,9 +449,10 @@ template <int T> __device__ __forceinline__ int tile_tid() {
   return T == 32 ? (int)(threadIdx.x & 31) : (int)threadIdx.x;
 }
 
-template <int L, int R, int NS, int B, int T, bool LINE_MAJOR, int DIR, class In, class Out>
-__device__ __forceinline__ void stage_io(const In& in, const Out& out,
-                                         const float2* __restrict__ tw, bool inplace) {
+template <int L, int R, int NS, int B, int T, bool LINE_MAJOR, int DIR, class In, class Out,
+          class TW>
+__device__ __forceinline__ void stage_io(const In& in, const Out& out, const TW& tw,
+                                         bool inplace) {
   constexpr int NBF = L / R;
   constexpr int TOTAL = NBF * B;
   constexpr int PER = (TOTAL + T - 1) / T;
@@ -446,20 +496,20 @@ __device__ __forceinline__ void stage_io(const In& in, const Out& out,
           // along a line: the transposed runs, one contiguous run per r
 #pragma unroll
           for (int r = 1; r < R; r++) {
-            const float2 w = __ldg(tw + OFFT + (r - 1) * NS + jm);
+            const float2 w = tw_ld(tw, OFFT + (r - 1) * NS + jm);
             v[q][r] = cmul(v[q][r], DIR < 0 ? cplx{w.x, w.y} : cplx{w.x, -w.y});
           }
         } else if constexpr (OFF >= 0) {
           // the stage's row jm: R-1 twiddles, two per 16-byte load
-          const float4* t4 = reinterpret_cast<const float4*>(tw + OFF + jm * stage_rp(R));
 #pragma unroll
           for (int i = 0; i < stage_rp(R) / 2; i++) {
-            const float4 w = __ldg(t4 + i);
+            const float4 w = tw_ld2(tw, OFF + jm * stage_rp(R) + 2 * i);
             const int r1 = 2 * i + 1, r2 = 2 * i + 2;
             v[q][r1] = cmul(v[q][r1], DIR < 0 ? cplx{w.x, w.y} : cplx{w.x, -w.y});
             if (r2 < R) v[q][r2] = cmul(v[q][r2], DIR < 0 ? cplx{w.z, w.w} : cplx{w.z, -w.w});
           }
         } else {
+          static_assert(!IsTwShared<TW>::v, "a shared twiddle copy holds stage rows and runs only");
           constexpr int STEP = L / (NS * R);
 #pragma unroll
           for (int r = 1; r < R; r++) v[q][r] = cmul(v[q][r], twiddle<DIR>(tw, jm * r * STEP));
@@ -496,9 +546,9 @@ __device__ __forceinline__ void stage_io(const In& in, const Out& out,
 // shared tile `mid`.  Every stage that writes `mid` is followed by a barrier.
 // LML: the thread mapping of the last stage (the others use LM).
 template <int L, int S, int B, int T, bool LM, int DIR, int RM, bool LML, class First, class Mid,
-          class Last>
+          class Last, class TW>
 __device__ __forceinline__ void fft_io_from(const First& first, const Mid& mid, const Last& last,
-                                            const float2* __restrict__ tw) {
+                                            const TW& tw) {
   constexpr int NSTAGE = num_stages(L, RM);
   constexpr int R = radix_at(L, S, RM);
   constexpr int NS = ns_before(L, S, RM);
@@ -523,9 +573,9 @@ __device__ __forceinline__ void fft_io_from(const First& first, const Mid& mid, 
 // consecutive lines (false); LML: the same choice for the last stage alone.
 // DIR = -1 forward, +1 inverse (unnormalised).
 template <int L, int B, int T, bool LM, int DIR, int RM = 16, bool LML = LM, class First,
-          class Mid, class Last>
+          class Mid, class Last, class TW>
 __device__ __forceinline__ void fft_io(const First& first, const Mid& mid, const Last& last,
-                                       const float2* __restrict__ tw) {
+                                       const TW& tw) {
   static_assert(supported_length(L, RM), "FFT length must be 2^a 3^b");
   fft_io_from<L, 0, B, T, LM, DIR, RM, LML>(first, mid, last, tw);
 }

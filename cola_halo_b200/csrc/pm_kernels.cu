@@ -737,8 +737,17 @@ __global__ void __launch_bounds__(T) k_fx(const float2* in, float2* out,
 // timeout.  The tensor map views the spectrum as floats (2N, N, N/2+1).
 template <int N> __host__ __device__ constexpr int fx_nbox() { return (N + 255) / 256; }
 template <int N> __host__ __device__ constexpr int fx_krows() { return N / fx_nbox<N>(); }
-template <int N, int TKV> __host__ __device__ constexpr size_t fx_sw_smem() {
-  return sizeof(float2) * (size_t)N * TKV + 1024 + 16;
+// Meshes up to 768^3 keep the twiddle entries of the x pass in shared memory
+// (a few KB, copied while the tensor loads land): the column stages' loads
+// then wait on shared memory instead of L1 (768^3: 0.57 against 0.72 ms
+// per launch).  Larger meshes read the table (their copies would cost a
+// resident CTA per SM).  The z c2r measured slower with its copy (2.36
+// against 2.24-2.29 ms per step at 768^3) and reads the table.
+template <int N> __host__ __device__ constexpr bool tw_in_smem() { return N <= 768; }
+
+template <int N, int TKV, int RMX> __host__ __device__ constexpr size_t fx_sw_smem() {
+  return sizeof(float2) * (size_t)N * TKV + 1024 + 16 +
+         (tw_in_smem<N>() ? (size_t)cgfft::TwCopy<N, RMX, false, false>::bytes : 0);
 }
 template <int TKV> struct SwTile;
 template <> struct SwTile<8> { using type = cgfft::SmemSw8; };
@@ -794,6 +803,17 @@ __global__ void __launch_bounds__(T) k_fx_sw(const __grid_constant__ CUtensorMap
           : "memory");
     }
   }
+  // the stages' twiddles into shared memory while the tensor loads land
+  using TC = cgfft::TwCopy<N, RMX, false, false>;
+  float2* tws = reinterpret_cast<float2*>(base + kBytes + 16);
+  if constexpr (tw_in_smem<N>()) {
+    TC::template copy<T>(tws, twN);
+    __syncthreads();
+  }
+  const auto tw = [&] {
+    if constexpr (tw_in_smem<N>()) return cgfft::TwShared<TC::lo>{tws};
+    else return twN;
+  }();
   unsigned done = 0;
   for (int it = 0; it < (1 << 22) && !done; it++) {
     asm volatile(
@@ -808,11 +828,11 @@ __global__ void __launch_bounds__(T) k_fx_sw(const __grid_constant__ CUtensorMap
   const size_t off = (size_t)blockIdx.y * N * N + blockIdx.x * TKV;
   const cgfft::GmemC<1, N> go{out + off};
   if constexpr (SCALE == 0) {
-    cgfft::fft_io<N, TKV, T, false, DIR, RMX>(t, t, go, twN);
+    cgfft::fft_io<N, TKV, T, false, DIR, RMX>(t, t, go, tw);
   } else {
     const float fz = SCALE == 2 && gtab ? __ldg(gtab + blockIdx.y) : (float)blockIdx.y;
     const SmemScaled<Tile, SCALE> ts{t, N, fz, gtab};
-    cgfft::fft_io<N, TKV, T, false, DIR, RMX>(ts, t, go, twN);
+    cgfft::fft_io<N, TKV, T, false, DIR, RMX>(ts, t, go, tw);
   }
 }
 
@@ -1108,15 +1128,11 @@ template <int N> __host__ __device__ constexpr size_t zsw_smem() {
 // (N/2+1) kz rows of the lines (x, y0 .. y0+15) of the spectrum behind `tm`
 // (mbarrier `bar`, already initialised, phase `parity`); every thread then
 // waits, bounded.  False (for every thread) when the loads did not complete.
-struct NoWork {
-  __device__ __forceinline__ void operator()() const {}
-};
-
 // `during` runs on every thread after the loads are issued, before the wait.
-template <int N, class F = NoWork>
+template <int N, class F>
 __device__ __forceinline__ bool zsw_gather(const CUtensorMap& tm, unsigned char* base,
                                            unsigned bar, unsigned parity, int x, int y0,
-                                           F during = F()) {
+                                           F during) {
   constexpr int KR = zsw_krows<N>(), NB = zsw_nbox<N>();
   constexpr unsigned kBytes = 128u * NB * KR;
   if (threadIdx.x == 0) {
@@ -1193,7 +1209,7 @@ __global__ void __launch_bounds__(T, N >= 768 ? 3 : 4) k_zi_sw(const __grid_cons
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
   __syncthreads();
-  if (!zsw_gather<N>(tm, base, bar, 0, x, y0)) {
+  if (!zsw_gather<N>(tm, base, bar, 0, x, y0, [] {})) {
     if (threadIdx.x == 0) atomicOr(err, (unsigned)CG_ERR_TMA_WAIT);
     return;
   }
@@ -1506,7 +1522,7 @@ void set_fx(MeshKernels* k) {
   k->fxi_sw = k_fx_sw<N, 1, 0, TKV, RMX>;
   k->fxi_x_sw = k_fx_sw<N, 1, 1, TKV, RMX>;
   k->fxi_z_sw = k_fx_sw<N, 1, 2, TKV, RMX>;
-  k->sm_fx_sw = fx_sw_smem<N, TKV>();
+  k->sm_fx_sw = fx_sw_smem<N, TKV, RMX>();
   k->sm_fx = sizeof(cplx) * cgfft::col_tile_elems<N, TKV>();
   k->tk = TKV;
 }
