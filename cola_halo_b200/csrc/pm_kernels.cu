@@ -738,11 +738,13 @@ __global__ void __launch_bounds__(T) k_fx(const float2* in, float2* out,
 template <int N> __host__ __device__ constexpr int fx_nbox() { return (N + 255) / 256; }
 template <int N> __host__ __device__ constexpr int fx_krows() { return N / fx_nbox<N>(); }
 // Meshes up to 768^3 keep the twiddle entries of the x pass in shared memory
-// (a few KB, copied while the tensor loads land): the column stages' loads
-// then wait on shared memory instead of L1 (768^3: 0.57 against 0.72 ms
-// per launch).  Larger meshes read the table (their copies would cost a
-// resident CTA per SM).  The z c2r measured slower with its copy (2.36
-// against 2.24-2.29 ms per step at 768^3) and reads the table.
+// (a few KB, copied while the tensor loads land).  A shared-memory load
+// takes a 32-bit address where a table load took a 64-bit one: the
+// 16-column radix-16 form fell from 186 to 128 registers, fits 2 CTAs per
+// SM instead of 1, and takes 0.57 instead of 0.90 ms per launch at 768^3.
+// Larger meshes read the table (their copies would cost a resident CTA per
+// SM).  The z c2r measured slower with its copy (2.36 against 2.24-2.29 ms
+// per step at 768^3) and reads the table.
 template <int N> __host__ __device__ constexpr bool tw_in_smem() { return N <= 768; }
 
 template <int N, int TKV, int RMX> __host__ __device__ constexpr size_t fx_sw_smem() {
