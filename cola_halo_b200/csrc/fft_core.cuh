@@ -55,26 +55,21 @@ template <int DIR> __device__ __forceinline__ cplx mul_i(cplx a) {
 template <int DIR> __device__ __forceinline__ float2 isgn() {
   return DIR < 0 ? make_float2(1.0f, -1.0f) : make_float2(-1.0f, 1.0f);
 }
-// Twiddle sources: the global table (read through the read-only path), or
-// entries [BASE, BASE + n) of it copied into shared memory by the CTA
-// (TwShared; p points at the copy of entry BASE, 16-byte aligned).
-template <int BASE> struct TwShared { const float2* p; };
-template <class TW> struct IsTwShared { static constexpr bool v = false; };
-template <int BASE> struct IsTwShared<TwShared<BASE>> { static constexpr bool v = true; };
+// Twiddle sources: the global table (read through the read-only path), or a
+// shared-memory pack of the stage blocks one transform reads (TwPack, below).
+// tw_at<B>(tw, i): entry B + i of the table, B the start of a stage block.
+template <int B> __device__ __forceinline__ float2 tw_at(const float2* __restrict__ tw, int i) {
+  return __ldg(tw + B + i);
+}
+// two entries (B + i even: 16-byte aligned in the table and in a pack)
+template <int B> __device__ __forceinline__ float4 tw_at2(const float2* __restrict__ tw, int i) {
+  return __ldg(reinterpret_cast<const float4*>(tw + B + i));
+}
+template <class TW> struct IsTwPack { static constexpr bool v = false; };
 __device__ __forceinline__ float2 tw_ld(const float2* __restrict__ tw, int i) {
   return __ldg(tw + i);
 }
-template <int BASE> __device__ __forceinline__ float2 tw_ld(const TwShared<BASE>& tw, int i) {
-  return tw.p[i - BASE];
-}
-// two entries i, i+1 (i even: 16-byte aligned in the table and in the copy)
-__device__ __forceinline__ float4 tw_ld2(const float2* __restrict__ tw, int i) {
-  return __ldg(reinterpret_cast<const float4*>(tw + i));
-}
-template <int BASE> __device__ __forceinline__ float4 tw_ld2(const TwShared<BASE>& tw, int i) {
-  return *reinterpret_cast<const float4*>(tw.p + (i - BASE));
-}
-template <int DIR, class TW> __device__ __forceinline__ cplx twiddle(const TW& tw, int t) {
+template <int DIR> __device__ __forceinline__ cplx twiddle(const float2* __restrict__ tw, int t) {
   float2 w = tw_ld(tw, t);
   return DIR < 0 ? cplx{w.x, w.y} : cplx{w.x, -w.y};
 }
@@ -285,35 +280,69 @@ __host__ __device__ constexpr int stage_twt_offset(int L, int NS, int R) {
 }
 __host__ __device__ constexpr int twiddle_table_len(int L) { return stage_twt_offset(L, 0, 0); }
 
-// The table entries an L-point transform (maximum radix RM, stage mappings
-// LM and LML as in fft_io) reads: [tw_copy_lo, tw_copy_hi), both even, so
-// that a copy of them keeps the stage rows 16-byte aligned.
-__host__ __device__ constexpr int tw_copy_bound(int L, int RM, bool LM, bool LML, bool hi) {
-  int lo_v = 1 << 30, hi_v = 0;
+// The table blocks an L-point transform (maximum radix RM, stage mappings LM
+// and LML as in fft_io) reads, one per stage after the first: the stage's
+// rows where it is column-mapped, its transposed runs where it is
+// line-major.  TwPack packs them back to back in shared memory, each rounded
+// up to an even count of entries so that the rows stay 16-byte aligned.
+__host__ __device__ constexpr int tw_block(int L, int RM, bool LM, bool LML, int st, bool len) {
   const int ns = num_stages(L, RM);
-  for (int st = 1; st < ns; st++) {
-    const int n = ns_before(L, st, RM), r = radix_at(L, st, RM);
-    const bool line = st == ns - 1 ? LML : LM;
-    const int off = line ? stage_twt_offset(L, n, r) : stage_tw_offset(L, n, r);
-    const int end = off + (line ? n * (r - 1) : n * stage_rp(r));
-    lo_v = off < lo_v ? off : lo_v;
-    hi_v = end > hi_v ? end : hi_v;
-  }
-  if (hi_v == 0) return 0;
-  return hi ? (hi_v + 1) / 2 * 2 : lo_v / 2 * 2;
+  const int n = ns_before(L, st, RM), r = radix_at(L, st, RM);
+  const bool line = st == ns - 1 ? LML : LM;
+  if (!len) return line ? stage_twt_offset(L, n, r) : stage_tw_offset(L, n, r);
+  return ((line ? n * (r - 1) : n * stage_rp(r)) + 1) / 2 * 2;
 }
-template <int L, int RM, bool LM, bool LML> struct TwCopy {
-  static constexpr int lo = tw_copy_bound(L, RM, LM, LML, false);
-  static constexpr int hi = tw_copy_bound(L, RM, LM, LML, true);
-  static constexpr int bytes = (hi - lo) * 8;
-  // entries [lo, hi) of the table tw into dst (16-byte aligned), by T threads
-  template <int T>
+// Position in the pack of the block that starts at table entry B (-1: none);
+// with B < 0 the pack's length.
+__host__ __device__ constexpr int tw_pack_pos(int L, int RM, bool LM, bool LML, int B) {
+  int pos = 0;
+  for (int st = 1; st < num_stages(L, RM); st++) {
+    if (B >= 0 && tw_block(L, RM, LM, LML, st, false) == B) return pos;
+    pos += tw_block(L, RM, LM, LML, st, true);
+  }
+  return B >= 0 ? -1 : pos;
+}
+__host__ __device__ constexpr bool tw_blocks_even(int L, int RM, bool LM, bool LML) {
+  for (int st = 1; st < num_stages(L, RM); st++)
+    if (tw_block(L, RM, LM, LML, st, false) % 2) return false;
+  return true;
+}
+template <int L, int RM, bool LM, bool LML> struct TwPack {
+  static_assert(tw_blocks_even(L, RM, LM, LML), "stage blocks start on even table entries");
+  const float2* p;      // the pack in shared memory, 16-byte aligned
+  static constexpr int entries = tw_pack_pos(L, RM, LM, LML, -1);
+  static constexpr int bytes = entries * 8;
+  static constexpr int kL = L, kRM = RM;
+  static constexpr bool kLM = LM, kLML = LML;
+  // the blocks of the table tw into dst, by T threads (stage ST on)
+  template <int T, int ST = 1>
   __device__ static __forceinline__ void copy(float2* dst, const float2* __restrict__ tw) {
-    const float4* src = reinterpret_cast<const float4*>(tw + lo);
-    float4* d = reinterpret_cast<float4*>(dst);
-    for (int i = (int)threadIdx.x; i < (hi - lo) / 2; i += T) d[i] = __ldg(src + i);
+    if constexpr (ST < num_stages(L, RM)) {
+      constexpr int b = tw_block(L, RM, LM, LML, ST, false);
+      constexpr int n = tw_block(L, RM, LM, LML, ST, true);
+      constexpr int pos = tw_pack_pos(L, RM, LM, LML, b);
+      const float4* src = reinterpret_cast<const float4*>(tw + b);
+      float4* d = reinterpret_cast<float4*>(dst + pos);
+      for (int i = (int)threadIdx.x; i < n / 2; i += T) d[i] = __ldg(src + i);
+      copy<T, ST + 1>(dst, tw);
+    }
   }
 };
+template <int L, int RM, bool LM, bool LML> struct IsTwPack<TwPack<L, RM, LM, LML>> {
+  static constexpr bool v = true;
+};
+template <int B, int L, int RM, bool LM, bool LML>
+__device__ __forceinline__ float2 tw_at(const TwPack<L, RM, LM, LML>& tw, int i) {
+  constexpr int pos = tw_pack_pos(L, RM, LM, LML, B);
+  static_assert(pos >= 0, "the pack does not hold this stage block");
+  return tw.p[pos + i];
+}
+template <int B, int L, int RM, bool LM, bool LML>
+__device__ __forceinline__ float4 tw_at2(const TwPack<L, RM, LM, LML>& tw, int i) {
+  constexpr int pos = tw_pack_pos(L, RM, LM, LML, B);
+  static_assert(pos >= 0, "the pack does not hold this stage block");
+  return *reinterpret_cast<const float4*>(tw.p + pos + i);
+}
 
 // ------------------------------------------------------------ tile access
 // The first stage reads its legs j + r L/R and the last writes its outputs
@@ -496,20 +525,20 @@ __device__ __forceinline__ void stage_io(const In& in, const Out& out, const TW&
           // along a line: the transposed runs, one contiguous run per r
 #pragma unroll
           for (int r = 1; r < R; r++) {
-            const float2 w = tw_ld(tw, OFFT + (r - 1) * NS + jm);
+            const float2 w = tw_at<OFFT>(tw, (r - 1) * NS + jm);
             v[q][r] = cmul(v[q][r], DIR < 0 ? cplx{w.x, w.y} : cplx{w.x, -w.y});
           }
         } else if constexpr (OFF >= 0) {
           // the stage's row jm: R-1 twiddles, two per 16-byte load
 #pragma unroll
           for (int i = 0; i < stage_rp(R) / 2; i++) {
-            const float4 w = tw_ld2(tw, OFF + jm * stage_rp(R) + 2 * i);
+            const float4 w = tw_at2<OFF>(tw, jm * stage_rp(R) + 2 * i);
             const int r1 = 2 * i + 1, r2 = 2 * i + 2;
             v[q][r1] = cmul(v[q][r1], DIR < 0 ? cplx{w.x, w.y} : cplx{w.x, -w.y});
             if (r2 < R) v[q][r2] = cmul(v[q][r2], DIR < 0 ? cplx{w.z, w.w} : cplx{w.z, -w.w});
           }
         } else {
-          static_assert(!IsTwShared<TW>::v, "a shared twiddle copy holds stage rows and runs only");
+          static_assert(!IsTwPack<TW>::v, "a twiddle pack holds stage rows and runs only");
           constexpr int STEP = L / (NS * R);
 #pragma unroll
           for (int r = 1; r < R; r++) v[q][r] = cmul(v[q][r], twiddle<DIR>(tw, jm * r * STEP));

@@ -758,7 +758,7 @@ template <int N> __host__ __device__ constexpr bool tw_in_smem() { return N <= 7
 
 template <int N, int TKV, int RMX> __host__ __device__ constexpr size_t fx_sw_smem() {
   return sizeof(float2) * (size_t)N * TKV + 1024 + 16 +
-         (tw_in_smem<N>() ? (size_t)cgfft::TwCopy<N, RMX, false, false>::bytes : 0);
+         (tw_in_smem<N>() ? (size_t)cgfft::TwPack<N, RMX, false, false>::bytes : 0);
 }
 template <int TKV> struct SwTile;
 template <> struct SwTile<8> { using type = cgfft::SmemSw8; };
@@ -815,14 +815,14 @@ __global__ void __launch_bounds__(T) k_fx_sw(const __grid_constant__ CUtensorMap
     }
   }
   // the stages' twiddles into shared memory while the tensor loads land
-  using TC = cgfft::TwCopy<N, RMX, false, false>;
+  using TP = cgfft::TwPack<N, RMX, false, false>;
   float2* tws = reinterpret_cast<float2*>(base + kBytes + 16);
   if constexpr (tw_in_smem<N>()) {
-    TC::template copy<T>(tws, twN);
+    TP::template copy<T>(tws, twN);
     __syncthreads();
   }
   const auto tw = [&] {
-    if constexpr (tw_in_smem<N>()) return cgfft::TwShared<TC::lo>{tws};
+    if constexpr (tw_in_smem<N>()) return TP{tws};
     else return twN;
   }();
   unsigned done = 0;
@@ -1134,6 +1134,14 @@ template <int N> __host__ __device__ constexpr int zsw_krows() {
 template <int N> __host__ __device__ constexpr size_t zsw_smem() {
   return (size_t)128 * zsw_nbox<N>() * zsw_krows<N>() + 1024 + 16;   // + alignment, mbarrier
 }
+// The z c2r's stage twiddles (its N/2-point transform: column-mapped stages,
+// a line-major last stage), packed in shared memory after the tile from
+// 1024^3 on.  There the 32-bit shared addresses take the kernel from 188 to 4
+// bytes of spill at 3 CTAs per SM (1024^3: 5.72 against 6.76 ms per step).
+// At 384^3 and 768^3 the copy made the pass slower (768^3: 2.34-2.35
+// against 2.25-2.30 ms per step), and it reads the table.
+template <int N> using ZswPack = cgfft::TwPack<N / 2, 16, false, true>;
+template <int N> __host__ __device__ constexpr bool zsw_pack() { return N >= 1024; }
 
 // The swizzled tile's gather: thread 0 issues the NB tensor loads of the
 // (N/2+1) kz rows of the lines (x, y0 .. y0+15) of the spectrum behind `tm`
@@ -1220,14 +1228,23 @@ __global__ void __launch_bounds__(T, N >= 768 ? 3 : 4) k_zi_sw(const __grid_cons
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
   __syncthreads();
-  if (!zsw_gather<N>(tm, base, bar, 0, x, y0, [] {})) {
+  // from 1024^3 on, the transform's stage twiddles (4 KB) into shared
+  // memory while the tensor loads land
+  using TP = ZswPack<N>;
+  float2* tws = reinterpret_cast<float2*>(base + kBytes + 16);
+  if (!zsw_gather<N>(tm, base, bar, 0, x, y0, [&] {
+        if constexpr (zsw_pack<N>()) TP::template copy<T>(tws, twH);
+      })) {
     if (threadIdx.x == 0) atomicOr(err, (unsigned)CG_ERR_TMA_WAIT);
     return;
   }
   zsw_halfcomplex<N>(t, twN);
   __syncthreads();
   const cgfft::GmemC<H, 1> gout{reinterpret_cast<float2*>(out) + ((size_t)x * N + y0) * H};
-  cgfft::fft_io<H, TY, T, false, 1, 16, true>(t, t, gout, twH);
+  if constexpr (zsw_pack<N>())
+    cgfft::fft_io<H, TY, T, false, 1, 16, true>(t, t, gout, TP{tws});
+  else
+    cgfft::fft_io<H, TY, T, false, 1, 16, true>(t, t, gout, twH);
 }
 
 // ------------------------------------------ z c2r fused with interpolation
@@ -1560,7 +1577,7 @@ MeshKernels make_kernels(MeshSched s) {
   k.zi_tma = k_zi_tma<N>;
   k.sm_zi_tma = zi_tma_smem<N>();
   k.zi_sw = k_zi_sw<N>;
-  k.sm_zi_sw = zsw_smem<N>();
+  k.sm_zi_sw = zsw_smem<N>() + (zsw_pack<N>() ? ZswPack<N>::bytes : 0);
   k.zip = k_zi_interp<N>;
   k.sm_fz = sizeof(cplx) * TY * cgfft::line_pitch<N / 2>();
   k.sm_fy = sizeof(cplx) * BY * cgfft::line_pitch<N>();

@@ -27,14 +27,14 @@ def _particles(nc, L):
     return p
 
 
-def _force_run(lib, mode, nc, L, table, meshes, xmode=-1, fx_variant=None):
+def _force_run(lib, mode, nc, L, table, meshes, xmode=-1, fx_variant=None, factor=3):
     from cola_halo_b200 import Simulation
     assert lib.cg_set_z_gather(mode) == 0
     assert lib.cg_set_x_gather(xmode) == 0
     if fx_variant is not None:
-        assert lib.cg_set_schedule(3 * nc, 0, fx_variant) == 0
+        assert lib.cg_set_schedule(factor * nc, 0, fx_variant) == 0
     try:
-        sim = Simulation(nc, 3 * nc, L, OM)
+        sim = Simulation(nc, factor * nc, L, OM)
     finally:
         lib.cg_set_z_gather(-1)
         lib.cg_set_x_gather(-1)
@@ -79,6 +79,16 @@ def test_gathers_bit_identical_768(gpu_lib, bbks_table):
     gathers against the TMA ones."""
     f = [_force_run(gpu_lib, z, 256, 600.0, bbks_table, False, xmode=x)[0]
          for z, x in ((0, 0), (2, 1))]
+    np.testing.assert_array_equal(f[0], f[1])
+
+
+def test_z_gathers_bit_identical_1024(gpu_lib, bbks_table):
+    """The large configuration's 1024^3 mesh, where the swizzled TMA z c2r
+    reads its twiddles from a shared-memory pack: forces of every particle
+    as with the cp.async gather, which reads them from the table.  64^3
+    particles at factor 16: the clouds share no cell."""
+    f = [_force_run(gpu_lib, z, 64, 1200.0, bbks_table, False, factor=16)[0] for z in (0, 2)]
+    assert np.abs(f[0]).max() > 0
     np.testing.assert_array_equal(f[0], f[1])
 
 
