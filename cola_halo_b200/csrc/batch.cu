@@ -183,7 +183,7 @@ cudaError_t record_realization(cg_batch* b, Real& r, StreamBufs& sb) {
     a_x = (float)apos1;
   }
   r.nforce = iforce;
-  // power spectrum of the final positions (the P(k) the batch is judged by);
+  // power spectrum of the final positions (the P(k) the batch is measured by);
   // its density sum goes to the spare slot after the force evaluations
   p.dsum = r.dsum + sp.nsteps + 1;
   return pm_power_spectrum(&p, cx, r.ps.n, sp.ngrid / 2, 0, r.pk, st);

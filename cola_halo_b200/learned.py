@@ -312,15 +312,15 @@ def pk_error(k, p, p_ref, kmax):
 def evaluate(nc, boxsize, sched, net, train_seeds, eval_seeds, table, *, omega_m=0.273,
              epochs=1, lr=2e-3, filter_nk=16, filter_seeds=4, net2=None, variants=(),
              net_variants=(), net_first=(), log=None):
-    """Train on PM pairs, then judge plain-coarse and learned-coarse runs
+    """Train on PM pairs, then evaluate plain-coarse and learned-coarse runs
     against the plain factor-3 run on held-out seeds: P(k) error up to half
     the particle Nyquist wavenumber, and the device time of each run's time
     loop (with the host wall time beside it).
 
     filter_nk > 0 also fits per-step force transfer functions of filter_nk
     knots on the first `filter_seeds` training seeds (fit_force_filter) and
-    judges the filtered coarse run; `net2`, when given, is trained on the
-    filtered coarse force and judged as filter + net.  Each
+    evaluates the filtered coarse run; `net2`, when given, is trained on the
+    filtered coarse force and evaluated as filter + net.  Each
     (name, ngrid, kernel, fit, calibrate, nk) in `variants` adds a run on an
     ngrid mesh with the Green-step options `kernel` = (gradient, laplacian,
     deconvolve), with transfer functions of nk knots: least-squares fitted
@@ -329,12 +329,12 @@ def evaluate(nc, boxsize, sched, net, train_seeds, eval_seeds, table, *, omega_m
     `filter_seeds` training seeds: the error-versus-time curve between the
     coarse and the fine mesh.  Each (variant name, net) in `net_variants`
     trains that net on the named variant's corrected force (its kernel and
-    transfer functions) over all training seeds, and judges the variant
+    transfer functions) over all training seeds, and evaluates the variant
     with the net's correction added as "<name>_net".  Each (name, ngrid,
     kernel, nk, net) in `net_first` trains the net on that mesh's force
     with the Green-step options `kernel`, then calibrates transfer functions
     of nk knots on the final P(k) of the coarse runs with the net's
-    correction in (calibrate_force_filter with net), and judges the two
+    correction in (calibrate_force_filter with net), and evaluates the two
     together as `name`."""
     import time
 

@@ -1,7 +1,7 @@
 """What the trained conv net gains: the learned-correction workload's
 coarse run (128^3 particles on a 128^3 mesh, L = 300 Mpc/h, 10 steps from
 z = 49) with the net's force correction against the same run without it,
-both judged by the P(k) error up to half the particle Nyquist wavenumber
+both measured by the P(k) error up to half the particle Nyquist wavenumber
 against the plain factor-3 (384^3) run on held-out seeds.  The net is
 trained by the library's own forward and backward kernels on pairs made by
 the method itself (factor-3 force minus coarse force along factor-3
