@@ -104,7 +104,7 @@ cudaError_t mesh_c2r(const MeshFFT* f, float2* spec, float* real, cudaStream_t s
 // strided x pass and of the fused Green pass runs (pm_kernels.cu kFxCfg,
 // kGreenCfg).  Variants other than 0 exist from 256 up (Green: up to 768).
 #define PM_NUM_FX_VARIANTS 3
-#define PM_NUM_GREEN_VARIANTS 5
+#define PM_NUM_GREEN_VARIANTS 7
 #define PM_NUM_DEP_VARIANTS 6
 struct MeshSched {
   int green = 0;

@@ -376,8 +376,9 @@ using cgfft::SmemLine;
 // explicitly.  x pass: ky columns per CTA and maximum radix (0: radix 8
 // from 768 up, else 16; -1: the other of the two).  Green pass: lines per
 // CTA, maximum radix and the resident CTAs per SM the kernel is
-// register-limited to.  The defaults are the fastest shapes measured at
-// 384 and 768.
+// register-limited to.  The Green default is the fastest shape measured at
+// 384 and 768; for the x pass the tuner picks 16 columns (variant 2) there,
+// ahead of the 8-column default.
 constexpr int MIN_TUNED_N = 256;
 // Variants compiled at size N.  The 8-line Green variants stop at 768: at
 // 1024 they would spill registers.
@@ -392,9 +393,14 @@ struct GreenCfg { int byg, rm, minb, thr; };
 constexpr FxCfg kFxCfg[PM_NUM_FX_VARIANTS] = {{8, 0}, {8, -1}, {16, 16}};
 // (lines per CTA, maximum radix, CTAs per SM, threads): at 768 a radix-16
 // stage has 48 butterflies per line, so 8 lines fill 384 threads, 4 lines
-// 192 and 2 lines 96 once each.
+// 192 and 2 lines 96 once each; 2 lines on 128 threads split the radix-3
+// stage's 512 butterflies evenly.  The default, 2 lines on 128 threads at 7
+// CTAs per SM, keeps a barrier to 4 warps (768^3: 1.39 ms; 4 lines on 256
+// threads, the earlier default: 1.64 ms; 2 lines on 96 threads: 1.62 ms; 2
+// on 128 at 8 or 6 CTAs per SM: 1.41 and 1.42 ms).
 constexpr GreenCfg kGreenCfg[PM_NUM_GREEN_VARIANTS] = {
-    {4, 16, 3, 256}, {8, 8, 2, 256}, {8, 16, 2, 384}, {4, 16, 4, 192}, {2, 16, 8, 96}};
+    {2, 16, 7, 128}, {8, 8, 2, 256}, {8, 16, 2, 384}, {4, 16, 4, 192}, {2, 16, 8, 96},
+    {2, 16, 8, 128}, {4, 16, 3, 256}};
 __host__ __device__ constexpr int rm_x_default(int N) { return N >= 768 ? 8 : 16; }
 __host__ __device__ constexpr int fx_rm(int N, int v) {
   return kFxCfg[v].rm == 0 ? rm_x_default(N)
@@ -1597,6 +1603,8 @@ MeshKernels make_kernels(MeshSched s) {
       case 2: set_green<N, 2>(&k); break;
       case 3: set_green<N, 3>(&k); break;
       case 4: set_green<N, 4>(&k); break;
+      case 5: set_green<N, 5>(&k); break;
+      case 6: set_green<N, 6>(&k); break;
       default: set_green<N, 0>(&k);
     }
   } else {

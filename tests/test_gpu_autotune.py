@@ -32,7 +32,7 @@ def test_schedule_variants_match_default_and_oracle(gpu_lib, bbks_table):
     nc, factor, L = 64, 4, 256.0
     N = nc * factor
     ng, nf = _variants(gpu_lib, N)
-    assert ng == 5 and nf == 3
+    assert ng == 7 and nf == 3
     p = lattice_particles(nc, L, 31, OM, 0.5, bbks_table)
     sim = Simulation(nc, N, L, OM)
 
@@ -49,7 +49,8 @@ def test_schedule_variants_match_default_and_oracle(gpu_lib, bbks_table):
         _, _, want = R.pm_force_meshes(x, N, L, factor)
         for a in range(3):
             assert np.abs(base[a] - want[a]).max() < 2e-5 * np.abs(want[a]).max()
-        for g, f in [(1, 0), (2, 0), (3, 0), (4, 0), (0, 1), (0, 2), (2, 2), (4, 1)]:
+        for g, f in [(1, 0), (2, 0), (3, 0), (4, 0), (5, 0), (6, 0), (0, 1), (0, 2), (2, 2),
+                     (6, 2)]:
             assert gpu_lib.cg_set_schedule(N, g, f) == 0
             got, fgot = meshes()
             for a in range(3):
@@ -64,7 +65,7 @@ def test_schedule_variants_match_default_and_oracle(gpu_lib, bbks_table):
 def test_schedule_arguments_checked(gpu_lib):
     assert _variants(gpu_lib, 128) == (1, 1)
     assert gpu_lib.cg_set_schedule(128, 1, 0) != 0
-    assert gpu_lib.cg_set_schedule(256, 5, 0) != 0
+    assert gpu_lib.cg_set_schedule(256, 7, 0) != 0
     assert gpu_lib.cg_set_schedule(256, 0, -1) != 0
     assert gpu_lib.cg_set_schedule(100, 0, 0) != 0
     assert _variants(gpu_lib, 1024)[0] == 1      # 8-line Green variants stop at 768
